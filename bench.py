@@ -1,0 +1,391 @@
+"""Benchmark of the bulk SRD fluid hot path: solvent particle-steps per second.
+
+Workload (one "step" = one MPCD interval of the bulk loop of
+test/setup_bulk_decay.f90: simple_mpcd_step -> mpcd_stream_periodic(tau) ->
+random_shift -> sort): a 128 x 128 x 128 periodic box at density 10, i.e.
+20,971,520 solvent particles, Maxwell velocities at kT = 1/3, alpha = pi/2,
+tau = 1.  Inputs are synthetic (seeded placement and velocities); the
+particle arrays (~1 GB in FP32, ~1.5 GB in FP64 per copy) exceed the 126 MB
+L2, so no L2 flush is needed between steps.
+
+The headline `value` is the FP32 form (the production form); the plain FP64
+form, which reproduces the reference arithmetic bit for bit, is reported in
+`fp64_plain`.  `--impl reference` times the CPU restatement of the same loop
+(the reference is Fortran and cannot be built here) on the host cores.
+
+Multi-GPU: the bulk system does not shard without a halo exchange; N GPUs run
+N independent replicas (weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+L_DEFAULT = 128
+RHO = 10
+T_INIT = 1.0 / 3.0
+TAU = 1.0
+SEED = 20241203
+# HBM bytes the fused interval kernel must move per particle and per slot
+# (read + write of the full particle record, the permutation index and the
+# next key; see the traffic table in DESIGN.md)
+BYTES_PER_PARTICLE = {32: 104, 64: 152}
+BYTES_PER_SLOT = 12
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(precision):
+    """dram bytes per particle of the fused kernel from the committed ncu summary, or None."""
+    f = ROOT / "profiles" / "k_bulk_interval.md"
+    if not f.exists():
+        return None
+    key = f"dram_bytes_per_particle_fp{precision}:"
+    for line in f.read_text().splitlines():
+        if line.strip().startswith(key):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out = ""
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5], f[6], f[7], f[8]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[2:]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def make_system(rm, L, precision):
+    from rmpcdmd_b200 import programs
+
+    cells = rm.CellSystem([L, L, L], 1.0)
+    N = RHO * L ** 3
+    p = rm.ParticleSystem(N, 1, None, precision)
+    p.random_placement(cells.edges, seed=SEED)
+    p.maxwell(T_INIT, SEED)
+    p.species = 1
+    rng = rm.Rng(SEED)
+    cells.random_shift(rng)
+    p.sort(cells)
+    rm.synchronize()
+    return p, cells, rng
+
+
+def timed_run(rm, p, cells, rng, steps, warmup):
+    """Device time (ms) of `steps` intervals after `warmup`, plus the average
+    duration of the fused interval kernel from its CUDA events."""
+    from rmpcdmd_b200._capi import call
+    import ctypes as C
+
+    rm.bulk_run(p, cells, rng, TAU, warmup)
+    rm.synchronize()
+    rm.Timers.enable(True)
+    rm.Timers.reset()
+    a, b = C.c_int(), C.c_int()
+    call("rmpcd_mark", C.byref(a))
+    rm.bulk_run(p, cells, rng, TAU, steps)
+    call("rmpcd_mark", C.byref(b))
+    rm.synchronize()
+    ms = C.c_float()
+    call("rmpcd_elapsed_ms", a, b, C.byref(ms))
+    tm = rm.Timers.read()
+    rm.Timers.enable(False)
+    return float(ms.value), tm
+
+
+def roofline(N, S, precision, phase, peak, peak_kind):
+    secs, calls = phase.get("interval_fused", (0.0, 0))
+    if not calls:
+        return None
+    avg = secs / calls
+    alg = N * BYTES_PER_PARTICLE[precision] + S * BYTES_PER_SLOT
+    achieved = alg / avg / 1e9
+    t = profile_traffic(precision)
+    return {"kernel": "k_bulk_interval", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+            "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "traffic": None if t is None else int(t * N), "algorithmic_bytes": int(alg),
+            "avg_launch_ms": round(avg * 1e3, 4), "launches": calls}
+
+
+def e2e_run(rm, p, cells, rng, steps):
+    """The same loop through the public API with host arrays: every step
+    uploads the particle arrays from page-locked host memory in the reference
+    layout, runs one interval and downloads them again."""
+    import ctypes as C
+
+    from rmpcdmd_b200._capi import call
+
+    N = p.Nmax
+    fields = [("pos", 3, np.float64), ("vel", 3, np.float64), ("image", 3, np.int32), ("id", 1, np.int32),
+              ("species", 1, np.int32), ("flags", 1, np.int32)]
+    bufs, ptrs = {}, []
+    for name, k, dt in fields:
+        nbytes = N * k * np.dtype(dt).itemsize
+        ptr = C.c_void_p()
+        call("rmpcd_host_alloc", C.c_size_t(nbytes), C.byref(ptr))
+        ptrs.append(ptr)
+        arr = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_byte)), shape=(nbytes,)).view(dt)
+        bufs[name] = arr
+        call("rmpcd_particles_download", p.handle, name.encode(), ptr)
+    nbytes_step = sum(N * k * np.dtype(dt).itemsize for _, k, dt in fields)
+    rm.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for name, _, _ in fields:
+            call("rmpcd_particles_upload", p.handle, name.encode(), bufs[name].ctypes.data_as(C.c_void_p))
+        rm.bulk_run(p, cells, rng, TAU, 1)
+        for name, _, _ in fields:
+            call("rmpcd_particles_download", p.handle, name.encode(), bufs[name].ctypes.data_as(C.c_void_p))
+    rm.synchronize()
+    dt_s = time.perf_counter() - t0
+    for ptr in ptrs:
+        call("rmpcd_host_free", ptr)
+    return N * steps / dt_s, nbytes_step, nbytes_step
+
+
+def cpu_sample(L_sample=64, min_seconds=10.0, max_intervals=20, threads=None):
+    """The oracle's OpenMP bulk interval on a 64^3 box at the same density."""
+    from oracle import oracle as O
+
+    nt = threads or os.cpu_count() or 1
+    O.set_threads(nt)
+    N = RHO * L_sample ** 3
+    c = O.Cells([L_sample] * 3)
+    p = O.Particles(N, 1)
+    r = np.random.default_rng(SEED)
+    p.pos[:] = r.random((N, 3)) * L_sample
+    p.vel[:] = r.normal(size=(N, 3)) * np.sqrt(T_INIT)
+    p.species[:] = 1
+    c.origin = O.random_shift_values(SEED, 0)
+    p.sort(c)
+    O.bulk_run(p, c, 1, TAU, SEED, 1)  # warm-up interval
+    t0 = time.perf_counter()
+    n = 0
+    while n < max_intervals and (time.perf_counter() - t0) < min_seconds:
+        O.bulk_run(p, c, 1, TAU, SEED, 3 + 2 * n)
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": N * n / dt, "unit": "particle-steps/s", "cores": nt, "kind": "port",
+            "sample": f"{n} bulk intervals of the FP64 oracle (C, OpenMP) on {L_sample}^3 cells x rho {RHO} "
+                      f"= {N} particles ({n * N} particle-steps, {dt:.1f} s)"}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world == 1:
+        return None, rank, local, world
+    import datetime
+
+    import torch.distributed as dist
+
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return dist, rank, local, world
+
+
+def max_over_ranks(dist, x):
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def run_ours(args):
+    dist, rank, local, world = dist_init()
+    import rmpcdmd_b200 as rm
+
+    rm.set_device(local)
+    L = args.L
+    N = RHO * L ** 3
+    peak, peak_kind = peaks()
+    out = {"metric": "solvent particle-steps/s (bulk SRD fluid, 128^3 cells, rho=10; one step = one MPCD "
+                     "interval: collide + stream + shift + sort)",
+           "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (seeded uniform positions, Maxwell velocities kT=1/3)"}
+    results = {}
+    for precision in (32, 64):
+        p, cells, rng = make_system(rm, L, precision)
+        barrier(dist)
+        with ClockSampler(local) as cs:
+            ms, phases = timed_run(rm, p, cells, rng, args.steps, args.warmup)
+        ms = max_over_ranks(dist, ms)
+        rl = roofline(N, cells.N, precision, phases, peak, peak_kind)
+        results[precision] = dict(ms=ms, phases=phases, roofline=rl, clocks=cs.summary(), p=p, cells=cells, rng=rng)
+        if precision == 64:
+            del p, cells
+    r32, r64 = results[32], results[64]
+    value = world * N * args.steps / (r32["ms"] * 1e-3)
+    out.update(value=value, ms_per_step=r32["ms"] / args.steps)
+    out["config"] = {"workload": f"bulk SRD fluid {L}^3 cells, rho={RHO}, N={N} particles per GPU, "
+                                 f"alpha=pi/2, tau=1, FP32 form", "cells": [L, L, L], "particles_per_gpu": N,
+                     "parallelism": f"replicas x{world} (independent systems, no collective)",
+                     "l2": "inputs larger than L2 (>= 1 GB of particle arrays per copy); no flush"}
+    out["roofline"] = r32["roofline"]
+    out["clocks"] = r32["clocks"]
+    fp64_value = world * N * args.steps / (r64["ms"] * 1e-3)
+    out["fp64_plain"] = {"value": fp64_value, "ms_per_step": r64["ms"] / args.steps, "roofline": r64["roofline"],
+                         "clocks": r64["clocks"], "fp32_over_fp64": value / fp64_value}
+    out["phases_ms"] = {k: round(v[0] * 1e3 / max(1, args.steps), 4)
+                        for k, v in r32["phases"].items()}
+    # kernels launched per step: fused interval, 3 scan kernels, key scatter;
+    # plus the final segment sort (2) and gather (1) of the run
+    out["gpu_launches"] = 5 * args.steps + 3
+    if not args.no_e2e:
+        e2e_steps = max(1, min(args.e2e_steps, args.steps))
+        v, hb, db = e2e_run(rm, r32["p"], r32["cells"], r32["rng"], e2e_steps)
+        v = world * (1.0 / max_over_ranks(dist, 1.0 / v))
+        out["e2e"] = {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": hb, "d2h_bytes_per_step": db,
+                      "steps": e2e_steps,
+                      "path": "rmpcd_particles_upload x6 (pinned host, reference (3,N) layout) -> rmpcd_bulk_run(1) "
+                              "-> rmpcd_particles_download x6"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_sample()
+    if rank == 0:
+        print(json.dumps(out))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+
+    nt = os.cpu_count() or 1
+    O.set_threads(nt)
+    Ls = args.ref_L
+    N = RHO * Ls ** 3
+    c = O.Cells([Ls] * 3)
+    p = O.Particles(N, 1)
+    r = np.random.default_rng(SEED)
+    p.pos[:] = r.random((N, 3)) * Ls
+    p.vel[:] = r.normal(size=(N, 3)) * np.sqrt(T_INIT)
+    p.species[:] = 1
+    c.origin = O.random_shift_values(SEED, 0)
+    p.sort(c)
+    step = 1
+    for _ in range(args.warmup):
+        O.bulk_run(p, c, 1, TAU, SEED, step)
+        step += 2
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.bulk_run(p, c, 1, TAU, SEED, step)
+        step += 2
+    dt = time.perf_counter() - t0
+    v = N * args.steps / dt
+    sample = (f"each step: one bulk interval of the FP64 CPU restatement (C, OpenMP, {nt} threads) on "
+              f"{Ls}^3 cells x rho {RHO} = {N} particles, a bounded 1/{(L_DEFAULT // Ls) ** 3} sample of the "
+              f"{L_DEFAULT}^3 workload (particle-steps/s is per-particle intensive)")
+    out = {"impl": "reference", "metric": "solvent particle-steps/s (bulk SRD fluid, 128^3 cells, rho=10; one step "
+                                          "= one MPCD interval: collide + stream + shift + sort)",
+           "value": v, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic (seeded uniform positions, Gaussian velocities kT=1/3)",
+           "config": {"workload": f"bulk SRD fluid {Ls}^3-cell sample of the {L_DEFAULT}^3 box, rho={RHO}",
+                      "cells": [Ls] * 3, "particles": N},
+           "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": nt, "kind": "port", "sample": sample},
+           "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "note": "the reference (Fortran 2008 + OpenMP) cannot be built here: no Fortran compiler and empty "
+                   "dependency submodules; this arm times the C restatement of its loop"}
+    print(json.dumps(out))
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--L", type=int, default=L_DEFAULT)
+    ap.add_argument("--ref-L", type=int, default=64)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

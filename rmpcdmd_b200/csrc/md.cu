@@ -1,0 +1,442 @@
+// Velocity-Verlet halves, lazy cell-wise streaming with walls, PBC wrap,
+// dimer RATTLE and the colloid integrator (src/md.f90,
+// programs/single_dimer_pbc.f90).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "rmpcd_common.cuh"
+#include "state.cuh"
+#include "timers.cuh"
+
+namespace rmpcd {
+
+// md_pos, src/md.f90:61-77
+template <typename R>
+__global__ void k_md_pos(PView<R> v, R dt, R dt_sq)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < v.N;
+         i += (long long)gridDim.x * blockDim.x) {
+        v.pos.x[i] = v.pos.x[i] + dt * v.vel.x[i] + dt_sq * v.force.x[i];
+        v.pos.y[i] = v.pos.y[i] + dt * v.vel.y[i] + dt_sq * v.force.y[i];
+        v.pos.z[i] = v.pos.z[i] + dt * v.vel.z[i] + dt_sq * v.force.z[i];
+    }
+}
+
+// md_vel, src/md.f90:219-237
+template <typename R>
+__global__ void k_md_vel(PView<R> v, R dt)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < v.N;
+         i += (long long)gridDim.x * blockDim.x) {
+        int f = v.flags[i];
+        if (!((f >> WALL_BIT) & 1)) {
+            v.vel.x[i] = v.vel.x[i] + dt * (v.force.x[i] + v.force_old.x[i]) / 2;
+            v.vel.y[i] = v.vel.y[i] + dt * (v.force.y[i] + v.force_old.y[i]) / 2;
+            v.vel.z[i] = v.vel.z[i] + dt * (v.force.z[i] + v.force_old.z[i]) / 2;
+        } else {
+            v.flags[i] = f & ~(1 << WALL_BIT);
+        }
+    }
+}
+
+// cell_md_pos, src/md.f90:79-102
+template <typename R>
+__global__ void k_cell_md_pos(const int *count, const int *start, const unsigned char *is_md, int S,
+                              PView<R> v, R dt, R dt_sq, int md_flag)
+{
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
+        if ((is_md[s] != 0) != (md_flag != 0)) continue;
+        int a = start[s], n = count[s];
+        for (int i = a; i < a + n; i++) {
+            v.pos.x[i] = v.pos.x[i] + dt * v.vel.x[i] + dt_sq * v.force.x[i];
+            v.pos.y[i] = v.pos.y[i] + dt * v.vel.y[i] + dt_sq * v.force.y[i];
+            v.pos.z[i] = v.pos.z[i] + dt * v.vel.z[i] + dt_sq * v.force.z[i];
+        }
+    }
+}
+
+// cell_md_vel, src/md.f90:239-263
+template <typename R>
+__global__ void k_cell_md_vel(const int *count, const int *start, const unsigned char *is_md, int S,
+                              PView<R> v, R dt, int md_flag)
+{
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
+        if ((is_md[s] != 0) != (md_flag != 0)) continue;
+        int a = start[s], n = count[s];
+        for (int i = a; i < a + n; i++) {
+            int f = v.flags[i];
+            if (!((f >> WALL_BIT) & 1)) {
+                v.vel.x[i] = v.vel.x[i] + dt * (v.force.x[i] + v.force_old.x[i]) / 2;
+                v.vel.y[i] = v.vel.y[i] + dt * (v.force.y[i] + v.force_old.y[i]) / 2;
+                v.vel.z[i] = v.vel.z[i] + dt * (v.force.z[i] + v.force_old.z[i]) / 2;
+            } else {
+                v.flags[i] = f & ~(1 << WALL_BIT);
+            }
+        }
+    }
+}
+
+// cell_md_pos_ywall / cell_md_pos_zwall, src/md.f90:104-200 (dim 1 or 2)
+template <typename R>
+__global__ void k_cell_md_pos_wall(const int *count, const int *start, const unsigned char *is_md, int S,
+                                   PView<R> v, R dt, R dt_sq, int md_flag, int dim, double Lw, int bc)
+{
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
+        if ((is_md[s] != 0) != (md_flag != 0)) continue;
+        int a = start[s], n = count[s];
+        for (int i = a; i < a + n; i++) {
+            R vv[3] = {v.vel.x[i], v.vel.y[i], v.vel.z[i]};
+            R x[3] = {v.pos.x[i] + dt * vv[0] + dt_sq * v.force.x[i],
+                      v.pos.y[i] + dt * vv[1] + dt_sq * v.force.y[i],
+                      v.pos.z[i] + dt * vv[2] + dt_sq * v.force.z[i]};
+            bool collide = false;
+            R overtime = 0;
+            if (x[dim] < (R)0) {
+                collide = true;
+                overtime = x[dim] / vv[dim];
+            } else if ((double)x[dim] > Lw) {
+                collide = true;
+                overtime = (x[dim] - (R)Lw) / vv[dim];
+            }
+            if (collide) {
+                if (bc == BOUNCE_BACK_BC) {
+                    for (int k = 0; k < 3; k++) vv[k] = -vv[k];
+                    for (int k = 0; k < 3; k++) x[k] = x[k] + (R)2 * overtime * vv[k];
+                } else if (bc == SPECULAR_BC) {
+                    vv[dim] = -vv[dim];
+                    x[dim] = x[dim] + (R)2 * overtime * vv[dim];
+                }
+                v.vel.x[i] = vv[0];
+                v.vel.y[i] = vv[1];
+                v.vel.z[i] = vv[2];
+            }
+            v.pos.x[i] = x[0];
+            v.pos.y[i] = x[1];
+            v.pos.z[i] = x[2];
+        }
+    }
+}
+
+// apply_pbc, src/md.f90:202-217
+template <typename R>
+__global__ void k_apply_pbc(PView<R> v, double e0, double e1, double e2)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < v.N;
+         i += (long long)gridDim.x * blockDim.x) {
+        R x = v.pos.x[i], y = v.pos.y[i], z = v.pos.z[i];
+        int jx = ifloor((double)x / e0), jy = ifloor((double)y / e1), jz = ifloor((double)z / e2);
+        if (jx) {
+            v.ix[i] += jx;
+            v.pos.x[i] = x - (R)(jx * e0);
+        }
+        if (jy) {
+            v.iy[i] += jy;
+            v.pos.y[i] = y - (R)(jy * e1);
+        }
+        if (jz) {
+            v.iz[i] += jz;
+            v.pos.z[i] = z - (R)(jz * e2);
+        }
+    }
+}
+
+struct E3 {
+    double e[3];
+};
+
+struct Masses {
+    double m[RMPCD_MAX_SPECIES];
+    int n;
+};
+
+// mass(species(k)) of bead k; out-of-range species flag an error
+__device__ inline double bead_mass(const Masses &ms, const int *species, int k, unsigned *err)
+{
+    int s = species[k];
+    if (s < 1 || s > ms.n) {
+        atomicOr(err, DEV_ERR_RATTLE);
+        return 1.0;
+    }
+    return ms.m[s - 1];
+}
+
+__device__ inline double dot3(const double a[3], const double b[3])
+{
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+
+// rattle_dimer_pos, src/md.f90:265-296
+__global__ void k_rattle_pos(PView<double> v, const double *rx, const double *ry, const double *rz,
+                             Masses ms, double d, double dt, E3 L, unsigned *err)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double m1 = bead_mass(ms, v.species, 0, err), m2 = bead_mass(ms, v.species, 1, err);
+    double r[3], s[3];
+    r[0] = min_image_d(rx[0] - rx[1], L.e[0]);
+    r[1] = min_image_d(ry[0] - ry[1], L.e[1]);
+    r[2] = min_image_d(rz[0] - rz[1], L.e[2]);
+    s[0] = min_image_d(v.pos.x[0] - v.pos.x[1], L.e[0]);
+    s[1] = min_image_d(v.pos.y[0] - v.pos.y[1], L.e[1]);
+    s[2] = min_image_d(v.pos.z[0] - v.pos.z[1], L.e[2]);
+    double inv_mass = 1 / m1 + 1 / m2;
+    double rsq = dot3(r, r), ssq = dot3(s, s), rs = dot3(r, s);
+    double disc = rs * rs - rsq * (ssq - d * d);
+    if (disc < 0) atomicOr(err, DEV_ERR_RATTLE);
+    double g = rs - sqrt(disc);
+    g = g / (dt * inv_mass * rsq);
+    double *px[3] = {v.pos.x, v.pos.y, v.pos.z};
+    double *vx[3] = {v.vel.x, v.vel.y, v.vel.z};
+    for (int k = 0; k < 3; k++) {
+        px[k][0] = px[k][0] - g * dt * r[k] / m1;
+        px[k][1] = px[k][1] + g * dt * r[k] / m2;
+    }
+    for (int k = 0; k < 3; k++) {
+        vx[k][0] = vx[k][0] - g * r[k] / m1;
+        vx[k][1] = vx[k][1] + g * r[k] / m2;
+    }
+}
+
+// rattle_dimer_vel, src/md.f90:298-319
+__global__ void k_rattle_vel(PView<double> v, Masses ms, double d, E3 L, unsigned *err)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double m1 = bead_mass(ms, v.species, 0, err), m2 = bead_mass(ms, v.species, 1, err);
+    double s[3], dv[3];
+    double inv_mass = 1 / m1 + 1 / m2;
+    s[0] = min_image_d(v.pos.x[0] - v.pos.x[1], L.e[0]);
+    s[1] = min_image_d(v.pos.y[0] - v.pos.y[1], L.e[1]);
+    s[2] = min_image_d(v.pos.z[0] - v.pos.z[1], L.e[2]);
+    double *vx[3] = {v.vel.x, v.vel.y, v.vel.z};
+    for (int k = 0; k < 3; k++) dv[k] = vx[k][0] - vx[k][1];
+    double kk = dot3(dv, s) / (d * d * inv_mass);
+    for (int k = 0; k < 3; k++) {
+        vx[k][0] = vx[k][0] - kk * s[k] / m1;
+        vx[k][1] = vx[k][1] + kk * s[k] / m2;
+    }
+}
+
+// colloid VV halves, programs/single_dimer_pbc.f90:312-315 and :356-359
+__global__ void k_colloid_vv_pos(PView<double> v, const double *mass, double dt)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v.N; i += gridDim.x * blockDim.x) {
+        double m2 = 2 * mass[i];
+        v.pos.x[i] = v.pos.x[i] + dt * v.vel.x[i] + dt * dt * v.force.x[i] / m2;
+        v.pos.y[i] = v.pos.y[i] + dt * v.vel.y[i] + dt * dt * v.force.y[i] / m2;
+        v.pos.z[i] = v.pos.z[i] + dt * v.vel.z[i] + dt * dt * v.force.z[i] / m2;
+    }
+}
+
+__global__ void k_colloid_vv_vel(PView<double> v, const double *mass, double dt)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v.N; i += gridDim.x * blockDim.x) {
+        double m2 = 2 * mass[i];
+        v.vel.x[i] = v.vel.x[i] + dt * (v.force.x[i] + v.force_old.x[i]) / m2;
+        v.vel.y[i] = v.vel.y[i] + dt * (v.force.y[i] + v.force_old.y[i]) / m2;
+        v.vel.z[i] = v.vel.z[i] + dt * (v.force.z[i] + v.force_old.z[i]) / m2;
+    }
+}
+
+// per-particle masses cached on the device (re-uploaded only on change)
+struct MassCache {
+    const rmpcd_particles *owner = nullptr;
+    std::vector<double> host;
+    double *dev = nullptr;
+    int cap = 0;
+};
+static MassCache g_mass;
+
+static int mass_on_device(const rmpcd_particles *p, const double *mass, const double **out)
+{
+    int N = p->N;
+    bool same = g_mass.owner == p && (int)g_mass.host.size() == N &&
+                memcmp(g_mass.host.data(), mass, sizeof(double) * (size_t)N) == 0;
+    if (!same) {
+        if (g_mass.cap < N) {
+            cudaStreamSynchronize(stream());
+            cudaFree(g_mass.dev);
+            g_mass.dev = nullptr;
+            RMPCD_CUDA_TRY(cudaMalloc(&g_mass.dev, sizeof(double) * (size_t)(N > 0 ? N : 1)));
+            g_mass.cap = N;
+        }
+        g_mass.host.assign(mass, mass + N);
+        g_mass.owner = p;
+        RMPCD_CUDA_TRY(cudaMemcpyAsync(g_mass.dev, g_mass.host.data(), sizeof(double) * (size_t)N,
+                                       cudaMemcpyHostToDevice, stream()));
+    }
+    *out = g_mass.dev;
+    return RMPCD_OK;
+}
+
+}  // namespace rmpcd
+
+using namespace rmpcd;
+
+#define DISPATCH_R(p, CALL_F, CALL_D)        \
+    do {                                      \
+        if ((p)->precision == RMPCD_FP32) {   \
+            CALL_F;                           \
+        } else {                              \
+            CALL_D;                           \
+        }                                     \
+    } while (0)
+
+extern "C" {
+
+int rmpcd_md_pos(rmpcd_particles *p, double dt)
+{
+    RMPCD_ARG(p, "null argument");
+    if (p->N == 0) return RMPCD_OK;
+    PhaseTimer t("md_pos");
+    double dt_sq = dt * dt / 2;
+    int g = grid_for(p->N, 256);
+    DISPATCH_R(p, (k_md_pos<float><<<g, 256, 0, stream()>>>(cur<float>(p), (float)dt, (float)dt_sq)),
+               (k_md_pos<double><<<g, 256, 0, stream()>>>(cur<double>(p), dt, dt_sq)));
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+int rmpcd_md_vel(rmpcd_particles *p, double dt)
+{
+    RMPCD_ARG(p, "null argument");
+    if (p->N == 0) return RMPCD_OK;
+    PhaseTimer t("md_vel");
+    int g = grid_for(p->N, 256);
+    DISPATCH_R(p, (k_md_vel<float><<<g, 256, 0, stream()>>>(cur<float>(p), (float)dt)),
+               (k_md_vel<double><<<g, 256, 0, stream()>>>(cur<double>(p), dt)));
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+int rmpcd_cell_md_pos(rmpcd_cells *c, rmpcd_particles *p, double dt, int md_flag)
+{
+    RMPCD_ARG(c && p, "null argument");
+    PhaseTimer t("md_pos");
+    double dt_sq = dt * dt / 2;
+    int g = grid_for(c->S, 128);
+    DISPATCH_R(p,
+               (k_cell_md_pos<float><<<g, 128, 0, stream()>>>(c->count, c->start, c->is_md, c->S, cur<float>(p),
+                                                               (float)dt, (float)dt_sq, md_flag)),
+               (k_cell_md_pos<double><<<g, 128, 0, stream()>>>(c->count, c->start, c->is_md, c->S, cur<double>(p),
+                                                                dt, dt_sq, md_flag)));
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+int rmpcd_cell_md_vel(rmpcd_cells *c, rmpcd_particles *p, double dt, int md_flag)
+{
+    RMPCD_ARG(c && p, "null argument");
+    PhaseTimer t("md_vel");
+    int g = grid_for(c->S, 128);
+    DISPATCH_R(p,
+               (k_cell_md_vel<float><<<g, 128, 0, stream()>>>(c->count, c->start, c->is_md, c->S, cur<float>(p),
+                                                               (float)dt, md_flag)),
+               (k_cell_md_vel<double><<<g, 128, 0, stream()>>>(c->count, c->start, c->is_md, c->S, cur<double>(p),
+                                                                dt, md_flag)));
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+static int cell_md_pos_wall(rmpcd_cells *c, rmpcd_particles *p, double dt, int md_flag, int dim)
+{
+    RMPCD_ARG(c && p, "null argument");
+    PhaseTimer t("md_pos");
+    double dt_sq = dt * dt / 2;
+    int g = grid_for(c->S, 128);
+    DISPATCH_R(p,
+               (k_cell_md_pos_wall<float><<<g, 128, 0, stream()>>>(c->count, c->start, c->is_md, c->S,
+                                                                    cur<float>(p), (float)dt, (float)dt_sq,
+                                                                    md_flag, dim, c->edges[dim], c->bc[dim])),
+               (k_cell_md_pos_wall<double><<<g, 128, 0, stream()>>>(c->count, c->start, c->is_md, c->S,
+                                                                     cur<double>(p), dt, dt_sq, md_flag, dim,
+                                                                     c->edges[dim], c->bc[dim])));
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+int rmpcd_cell_md_pos_ywall(rmpcd_cells *c, rmpcd_particles *p, double dt, int md_flag)
+{
+    return cell_md_pos_wall(c, p, dt, md_flag, 1);
+}
+
+int rmpcd_cell_md_pos_zwall(rmpcd_cells *c, rmpcd_particles *p, double dt, int md_flag)
+{
+    return cell_md_pos_wall(c, p, dt, md_flag, 2);
+}
+
+int rmpcd_apply_pbc(rmpcd_particles *p, const double edges[3])
+{
+    RMPCD_ARG(p && edges, "null argument");
+    if (p->N == 0) return RMPCD_OK;
+    PhaseTimer t("apply_pbc");
+    int g = grid_for(p->N, 256);
+    DISPATCH_R(p, (k_apply_pbc<float><<<g, 256, 0, stream()>>>(cur<float>(p), edges[0], edges[1], edges[2])),
+               (k_apply_pbc<double><<<g, 256, 0, stream()>>>(cur<double>(p), edges[0], edges[1], edges[2])));
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+static Masses masses_of(const rmpcd_particles *p)
+{
+    Masses ms;
+    for (int k = 0; k < RMPCD_MAX_SPECIES; k++) ms.m[k] = p->mass[k];
+    ms.n = p->n_species;
+    return ms;
+}
+
+// rattle_dimer_pos, src/md.f90:265-296; masses are mass(species(1)) and
+// mass(species(2)), read on the device
+int rmpcd_rattle_dimer_pos(rmpcd_particles *p, double d, double dt, const double edges[3])
+{
+    RMPCD_ARG(p && edges, "null argument");
+    RMPCD_ARG(p->precision == RMPCD_FP64 && p->N >= 2, "rattle_dimer_pos: needs an FP64 system of >= 2 particles");
+    RMPCD_ARG(p->pos_rattle[0] != nullptr, "rattle_dimer_pos: pos_rattle was never set");
+    E3 L = {{edges[0], edges[1], edges[2]}};
+    PhaseTimer t("rattle_pos");
+    k_rattle_pos<<<1, 32, 0, stream()>>>(cur<double>(p), (const double *)p->pos_rattle[0],
+                                         (const double *)p->pos_rattle[1], (const double *)p->pos_rattle[2],
+                                         masses_of(p), d, dt, L, dev_error_word());
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+// rattle_dimer_vel, src/md.f90:298-319
+int rmpcd_rattle_dimer_vel(rmpcd_particles *p, double d, double dt, const double edges[3])
+{
+    (void)dt;
+    RMPCD_ARG(p && edges, "null argument");
+    RMPCD_ARG(p->precision == RMPCD_FP64 && p->N >= 2, "rattle_dimer_vel: needs an FP64 system of >= 2 particles");
+    E3 L = {{edges[0], edges[1], edges[2]}};
+    PhaseTimer t("rattle_vel");
+    k_rattle_vel<<<1, 32, 0, stream()>>>(cur<double>(p), masses_of(p), d, L, dev_error_word());
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+int rmpcd_colloid_vv_pos(rmpcd_particles *p, double dt, const double *mass)
+{
+    RMPCD_ARG(p && mass, "null argument");
+    RMPCD_ARG(p->precision == RMPCD_FP64, "colloid integrator needs an FP64 system");
+    if (p->N == 0) return RMPCD_OK;
+    const double *dm = nullptr;
+    int rc = mass_on_device(p, mass, &dm);
+    if (rc) return rc;
+    k_colloid_vv_pos<<<grid_for(p->N, 128), 128, 0, stream()>>>(cur<double>(p), dm, dt);
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+int rmpcd_colloid_vv_vel(rmpcd_particles *p, double dt, const double *mass)
+{
+    RMPCD_ARG(p && mass, "null argument");
+    RMPCD_ARG(p->precision == RMPCD_FP64, "colloid integrator needs an FP64 system");
+    if (p->N == 0) return RMPCD_OK;
+    const double *dm = nullptr;
+    int rc = mass_on_device(p, mass, &dm);
+    if (rc) return rc;
+    k_colloid_vv_vel<<<grid_for(p->N, 128), 128, 0, stream()>>>(cur<double>(p), dm, dt);
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,672 @@
+// neighbor_list_t on the GPU (src/neighbor_list.f90): the cell stencil, the
+// colloid -> solvent list built from the sorted cell lists, the list-based
+// Lennard-Jones forces and the O(C^2) colloid-colloid forces.
+//
+// Order fidelity: list entries follow the reference's single-thread order
+// (stencil order, then in-cell order); colloid force sums and energies are
+// accumulated sequentially in list order; a solvent particle touched by one
+// list entry gets force - f directly, one touched by several gets its
+// subtractions in (colloid, entry) order.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "keys.cuh"
+#include "rmpcd_common.cuh"
+#include "state.cuh"
+#include "timers.cuh"
+
+namespace rmpcd {
+
+constexpr int kNlThreads = 256;
+
+struct LJDev {
+    int n1;
+    double epsilon[16], sigma[16], cut_sq[16], cut_energy[16];
+};
+
+static LJDev lj_dev(const rmpcd_lj *lj)
+{
+    LJDev d;
+    memset(&d, 0, sizeof(d));
+    if (!lj) return d;
+    d.n1 = lj->n1;
+    for (int i = 0; i < 16; i++) {
+        d.epsilon[i] = lj->epsilon[i];
+        d.sigma[i] = lj->sigma[i];
+        d.cut_sq[i] = lj->cut_sq[i];
+        d.cut_energy[i] = lj->cut_energy[i];
+    }
+    return d;
+}
+
+// x**3 = x*(x*x), x**6 = x**3 * x**3 (gfortran's constant-power expansion)
+__device__ inline double cube(double x) { return x * (x * x); }
+__device__ inline double sixth(double x)
+{
+    double c = cube(x);
+    return c * c;
+}
+
+// lj_force / lj_energy, src/interaction.f90:83-96,126-136
+__device__ inline double lj_force_over_r(double r_sq, double eps, double sigma)
+{
+    double s6 = sixth(sigma) / cube(r_sq);
+    return 24.0 * eps * s6 / r_sq * (2.0 * s6 - 1.0);
+}
+__device__ inline double lj_energy(double r_sq, double eps, double sigma, double ce)
+{
+    double s6 = sixth(sigma) / cube(r_sq);
+    return 4.0 * eps * (s6 * s6 - s6) - ce;
+}
+
+__device__ inline int imod(int a, int p)
+{
+    int r = a % p;
+    return (r != 0 && ((r < 0) != (p < 0))) ? r + p : r;
+}
+
+// update_list, src/neighbor_list.f90:76-157: one block per colloid; stencil
+// cells are processed in chunks of kNlThreads, their particles enumerated in
+// stencil order and compacted in order with a block scan.
+template <typename R>
+__global__ void k_update_list(Grid g, const double *cx, const double *cy, const double *cz, const int *cs,
+                              const R *sx, const R *sy, const R *sz, const int *sspec, const int *count,
+                              const int *start, const int *stencil, int n_stencil, double radiussq,
+                              LJDev lj, int do_lj, int Nmax, int *list, int *n_out, unsigned char *is_md,
+                              unsigned char *is_reac, unsigned *err)
+{
+    __shared__ int c_slot[kNlThreads], c_start[kNlThreads], c_off[kNlThreads + 1];
+    __shared__ int c_md[kNlThreads], c_noreac[kNlThreads];
+    __shared__ int warp_sum[kNlThreads / 32];
+    __shared__ int s_total, s_base;
+    const int i = blockIdx.x;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    double x0 = cx[i], x1 = cy[i], x2 = cz[i];
+    int si = cs[i];
+    int cell[3];
+    cell_coords(g, x0, x1, x2, cell);  // cartesian_indices (0-based)
+    double L0 = g.L[0] * g.a, L1 = g.L[1] * g.a, L2 = g.L[2] * g.a;
+    if (t == 0) s_base = 0;
+    __syncthreads();
+    for (int j0 = 0; j0 < n_stencil; j0 += kNlThreads) {
+        int j = j0 + t;
+        int cnt = 0;
+        if (j < n_stencil) {
+            int p[3] = {imod(cell[0] + stencil[3 * j], g.L[0]), imod(cell[1] + stencil[3 * j + 1], g.L[1]),
+                        imod(cell[2] + stencil[3 * j + 2], g.L[2])};
+            int s = slot_of_cell(g, p);
+            c_slot[t] = s;
+            c_start[t] = start[s];
+            cnt = count[s];
+        }
+        c_md[t] = 0;
+        c_noreac[t] = 0;
+        // exclusive scan of the candidate counts of this chunk
+        int inc = cnt;
+        for (int o = 1; o < 32; o <<= 1) {
+            int w = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += w;
+        }
+        if (lane == 31) warp_sum[wid] = inc;
+        __syncthreads();
+        if (t == 0) {
+            int acc = 0;
+            for (int w = 0; w < kNlThreads / 32; w++) {
+                int v = warp_sum[w];
+                warp_sum[w] = acc;
+                acc += v;
+            }
+            s_total = acc;
+        }
+        __syncthreads();
+        c_off[t] = warp_sum[wid] + inc - cnt;
+        if (t == 0) c_off[kNlThreads] = s_total;
+        __syncthreads();
+        const int total = c_off[kNlThreads];
+        for (int k0 = 0; k0 < total; k0 += kNlThreads) {
+            int k = k0 + t;
+            int accept = 0;
+            int idx = -1;
+            if (k < total) {
+                // stencil cell of candidate k: last cell with offset <= k
+                int lo = 0, hi = kNlThreads;
+                while (hi - lo > 1) {
+                    int mid = (lo + hi) >> 1;
+                    if (c_off[mid] <= k) lo = mid;
+                    else hi = mid;
+                }
+                const int cl = lo;
+                idx = c_start[cl] + (k - c_off[cl]);
+                int s = sspec[idx];
+                if (s > 0) {
+                    double r0 = min_image_d(x0 - (double)sx[idx], L0);
+                    double r1 = min_image_d(x1 - (double)sy[idx], L1);
+                    double r2 = min_image_d(x2 - (double)sz[idx], L2);
+                    double rsq = r0 * r0 + r1 * r1 + r2 * r2;
+                    if (rsq < radiussq) {
+                        accept = 1;
+                        c_md[cl] = 1;
+                        if (do_lj && rsq <= lj.cut_sq[(s - 1) + lj.n1 * (si - 1)]) c_noreac[cl] = 1;
+                    }
+                }
+            }
+            // ordered compaction of accepted candidates
+            unsigned bal = __ballot_sync(0xffffffffu, accept);
+            if (lane == 0) warp_sum[wid] = __popc(bal);
+            __syncthreads();
+            if (t == 0) {
+                int acc = 0;
+                for (int w = 0; w < kNlThreads / 32; w++) {
+                    int v = warp_sum[w];
+                    warp_sum[w] = acc;
+                    acc += v;
+                }
+                s_total = acc;
+            }
+            __syncthreads();
+            if (accept) {
+                int pos = s_base + warp_sum[wid] + __popc(bal & ((1u << lane) - 1u));
+                if (pos < Nmax) list[(size_t)i * Nmax + pos] = idx;
+                else atomicOr(err, DEV_ERR_NLIST_FULL);
+            }
+            __syncthreads();
+            if (t == 0) s_base += s_total;
+            __syncthreads();
+        }
+        __syncthreads();
+        if (j < n_stencil && c_md[t]) {
+            is_md[c_slot[t]] = 1;
+            if (c_noreac[t]) is_reac[c_slot[t]] = 0;
+        }
+        __syncthreads();
+    }
+    if (t == 0) n_out[i] = s_base < Nmax ? s_base : Nmax;
+}
+
+// PAST_MD <- MD, MD cleared, for every solvent particle (src/neighbor_list.f90:180-188)
+__global__ void k_flag_roll(int *flags, int N)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x) {
+        int f = flags[i];
+        if ((f >> MD_BIT) & 1) f |= (1 << PAST_MD_BIT);
+        else f &= ~(1 << PAST_MD_BIT);
+        flags[i] = f & ~(1 << MD_BIT);
+    }
+}
+
+// pair forces of every list entry (src/neighbor_list.f90:198-219)
+template <typename R>
+__global__ void k_pair_forces(const double *cx, const double *cy, const double *cz, const int *cs,
+                              const R *sx, const R *sy, const R *sz, const int *sspec, int *sflags,
+                              const int *list, const int *n, int Nmax, double L0, double L1, double L2,
+                              LJDev lj, double *pf, double *pe, unsigned char *contrib, int *ncontrib,
+                              int *max_contrib)
+{
+    const int i = blockIdx.y;
+    const int ni = n[i];
+    double x0 = cx[i], x1 = cy[i], x2 = cz[i];
+    int s1 = cs[i];
+    int mask = (1 << MD_BIT) | (s1 == 1 ? (1 << CATALYZED_BIT) : 0);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ni; e += gridDim.x * blockDim.x) {
+        size_t q = (size_t)i * Nmax + e;
+        int idx = list[q];
+        int s2 = sspec[idx];
+        unsigned char c = 0;
+        if (s2 > 0) {
+            double d0 = min_image_d(x0 - (double)sx[idx], L0);
+            double d1 = min_image_d(x1 - (double)sy[idx], L1);
+            double d2 = min_image_d(x2 - (double)sz[idx], L2);
+            double r_sq = d0 * d0 + d1 * d1 + d2 * d2;
+            int tt = (s2 - 1) + lj.n1 * (s1 - 1);
+            if (r_sq <= lj.cut_sq[tt]) {
+                double fr = lj_force_over_r(r_sq, lj.epsilon[tt], lj.sigma[tt]);
+                pf[3 * q] = fr * d0;
+                pf[3 * q + 1] = fr * d1;
+                pf[3 * q + 2] = fr * d2;
+                pe[q] = lj_energy(r_sq, lj.epsilon[tt], lj.sigma[tt], lj.cut_energy[tt]);
+                c = 1;
+                int prev = atomicAdd(ncontrib + idx, 1);
+                if (prev >= 1) atomicMax(max_contrib, prev + 1);
+                atomicOr(sflags + idx, mask);
+            }
+        }
+        contrib[q] = c;
+    }
+}
+
+// solvent force - f for particles with exactly one contribution
+template <typename R>
+__global__ void k_apply_single(const int *list, const int *n, int Nmax, const unsigned char *contrib,
+                               const double *pf, const int *ncontrib, R *fx, R *fy, R *fz)
+{
+    const int i = blockIdx.y;
+    const int ni = n[i];
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ni; e += gridDim.x * blockDim.x) {
+        size_t q = (size_t)i * Nmax + e;
+        if (!contrib[q]) continue;
+        int idx = list[q];
+        if (ncontrib[idx] != 1) continue;
+        fx[idx] = fx[idx] - (R)pf[3 * q];
+        fy[idx] = fy[idx] - (R)pf[3 * q + 1];
+        fz[idx] = fz[idx] - (R)pf[3 * q + 2];
+    }
+}
+
+// particles with several contributions: colloid by colloid in order; inside
+// one colloid's list entries are distinct unless the stencil wraps the box,
+// in which case a single thread applies everything in order
+template <typename R>
+__global__ void k_apply_multi(const int *list, const int *n, int C, int Nmax, const unsigned char *contrib,
+                              const double *pf, const int *ncontrib, const int *max_contrib, int serial,
+                              R *fx, R *fy, R *fz)
+{
+    if (*max_contrib < 2) return;
+    for (int i = 0; i < C; i++) {
+        const int ni = n[i];
+        if (serial) {
+            if (threadIdx.x == 0) {
+                for (int e = 0; e < ni; e++) {
+                    size_t q = (size_t)i * Nmax + e;
+                    if (!contrib[q]) continue;
+                    int idx = list[q];
+                    if (ncontrib[idx] < 2) continue;
+                    fx[idx] = fx[idx] - (R)pf[3 * q];
+                    fy[idx] = fy[idx] - (R)pf[3 * q + 1];
+                    fz[idx] = fz[idx] - (R)pf[3 * q + 2];
+                }
+            }
+        } else {
+            for (int e = threadIdx.x; e < ni; e += blockDim.x) {
+                size_t q = (size_t)i * Nmax + e;
+                if (!contrib[q]) continue;
+                int idx = list[q];
+                if (ncontrib[idx] < 2) continue;
+                fx[idx] = fx[idx] - (R)pf[3 * q];
+                fy[idx] = fy[idx] - (R)pf[3 * q + 1];
+                fz[idx] = fz[idx] - (R)pf[3 * q + 2];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// f1 = sum of the pair forces in list order; force(:,i) = force(:,i) + f1
+__global__ void k_colloid_sum(const int *n, int Nmax, const unsigned char *contrib, const double *pf,
+                              double *cfx, double *cfy, double *cfz, int *clist, int *cn)
+{
+    __shared__ int idxs[kNlThreads];
+    __shared__ int warp_cnt[kNlThreads / 32];
+    __shared__ int s_cnt;
+    const int i = blockIdx.x;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    const int ni = n[i];
+    double f0 = 0, f1 = 0, f2 = 0;
+    int total = 0;
+    for (int e0 = 0; e0 < ni; e0 += kNlThreads) {
+        int e = e0 + t;
+        int c = (e < ni) ? contrib[(size_t)i * Nmax + e] : 0;
+        unsigned bal = __ballot_sync(0xffffffffu, c);
+        if (lane == 0) warp_cnt[wid] = __popc(bal);
+        __syncthreads();
+        if (t == 0) {
+            int acc = 0;
+            for (int w = 0; w < kNlThreads / 32; w++) {
+                int v = warp_cnt[w];
+                warp_cnt[w] = acc;
+                acc += v;
+            }
+            s_cnt = acc;
+        }
+        __syncthreads();
+        if (c) idxs[warp_cnt[wid] + __popc(bal & ((1u << lane) - 1u))] = e;
+        __syncthreads();
+        if (t == 0) {
+            for (int k = 0; k < s_cnt; k++) {
+                size_t q = (size_t)i * Nmax + idxs[k];
+                f0 = f0 + pf[3 * q];
+                f1 = f1 + pf[3 * q + 1];
+                f2 = f2 + pf[3 * q + 2];
+                clist[(size_t)i * Nmax + total + k] = idxs[k];
+            }
+            total += s_cnt;
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        cfx[i] = cfx[i] + f0;
+        cfy[i] = cfy[i] + f1;
+        cfz[i] = cfz[i] + f2;
+        cn[i] = total;
+    }
+}
+
+// e = sum of pair energies in (colloid, entry) order
+__global__ void k_energy(const int *cn, const int *clist, int C, int Nmax, const double *pe, double *out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double e = 0;
+    for (int i = 0; i < C; i++)
+        for (int k = 0; k < cn[i]; k++) e = e + pe[(size_t)i * Nmax + clist[(size_t)i * Nmax + k]];
+    *out = e;
+}
+
+__global__ void k_reset_contrib(const int *list, const int *n, int Nmax, const unsigned char *contrib,
+                                int *ncontrib)
+{
+    const int i = blockIdx.y;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n[i]; e += gridDim.x * blockDim.x) {
+        size_t q = (size_t)i * Nmax + e;
+        if (contrib[q]) ncontrib[list[q]] = 0;
+    }
+}
+
+// compute_force_n2, src/neighbor_list.f90:227-264: colloid m receives, in the
+// sequential loop order, -f(k,m) for k < m and then +f(m,j) for j > m
+__global__ void k_force_n2(const double *px, const double *py, const double *pz, const int *sp, int C,
+                           double L0, double L1, double L2, LJDev lj, double *fx, double *fy, double *fz)
+{
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < C; m += gridDim.x * blockDim.x) {
+        double a0 = fx[m], a1 = fy[m], a2 = fz[m];
+        for (int k = 0; k < C; k++) {
+            if (k == m) continue;
+            int i = k < m ? k : m, j = k < m ? m : k;
+            double d0 = min_image_d(px[i] - px[j], L0);
+            double d1 = min_image_d(py[i] - py[j], L1);
+            double d2 = min_image_d(pz[i] - pz[j], L2);
+            double r_sq = d0 * d0 + d1 * d1 + d2 * d2;
+            int s1 = sp[i], s2 = sp[j];
+            if (r_sq <= lj.cut_sq[(s1 - 1) + lj.n1 * (s2 - 1)]) {
+                int tt = (s2 - 1) + lj.n1 * (s1 - 1);
+                double fr = lj_force_over_r(r_sq, lj.epsilon[tt], lj.sigma[tt]);
+                double f0 = fr * d0, f1 = fr * d1, f2 = fr * d2;
+                if (k < m) {
+                    a0 = a0 - f0;
+                    a1 = a1 - f1;
+                    a2 = a2 - f2;
+                } else {
+                    a0 = a0 + f0;
+                    a1 = a1 + f1;
+                    a2 = a2 + f2;
+                }
+            }
+        }
+        fx[m] = a0;
+        fy[m] = a1;
+        fz[m] = a2;
+    }
+}
+
+__global__ void k_energy_n2(const double *px, const double *py, const double *pz, const int *sp, int C,
+                            double L0, double L1, double L2, LJDev lj, double *out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double e = 0;
+    for (int i = 0; i < C; i++)
+        for (int j = i + 1; j < C; j++) {
+            double d0 = min_image_d(px[i] - px[j], L0);
+            double d1 = min_image_d(py[i] - py[j], L1);
+            double d2 = min_image_d(pz[i] - pz[j], L2);
+            double r_sq = d0 * d0 + d1 * d1 + d2 * d2;
+            int s1 = sp[i], s2 = sp[j];
+            if (r_sq <= lj.cut_sq[(s1 - 1) + lj.n1 * (s2 - 1)]) {
+                int tt = (s2 - 1) + lj.n1 * (s1 - 1);
+                e = e + lj_energy(r_sq, lj.epsilon[tt], lj.sigma[tt], lj.cut_energy[tt]);
+            }
+        }
+    *out = e;
+}
+
+static int ensure_force_scratch(rmpcd_nlist *nl, int N2)
+{
+    if (!nl->pair_f) {
+        size_t ne = (size_t)nl->Npoints * nl->Nmax;
+        RMPCD_CUDA_TRY(cudaMalloc(&nl->pair_f, 3 * ne * sizeof(double) + 8));
+        RMPCD_CUDA_TRY(cudaMalloc(&nl->pair_e, ne * sizeof(double) + 8));
+        RMPCD_CUDA_TRY(cudaMalloc(&nl->contrib, ne + 8));
+        RMPCD_CUDA_TRY(cudaMalloc(&nl->d_status, (2 * nl->Npoints + 16 + ne) * sizeof(int)));
+    }
+    if (nl->ncontrib_cap < N2) {
+        cudaStreamSynchronize(stream());
+        cudaFree(nl->ncontrib);
+        RMPCD_CUDA_TRY(cudaMalloc(&nl->ncontrib, (size_t)(N2 > 0 ? N2 : 1) * sizeof(int)));
+        RMPCD_CUDA_TRY(cudaMemsetAsync(nl->ncontrib, 0, (size_t)(N2 > 0 ? N2 : 1) * sizeof(int), stream()));
+        nl->ncontrib_cap = N2;
+    }
+    return RMPCD_OK;
+}
+
+}  // namespace rmpcd
+
+using namespace rmpcd;
+
+extern "C" {
+
+int rmpcd_nlist_init(rmpcd_nlist **out, int Npoints, int Nmax)
+{
+    RMPCD_ARG(out, "null argument");
+    RMPCD_ARG(Npoints >= 0 && Nmax >= 1, "neighbor_list_t%init: Npoints >= 0 and Nmax >= 1 required");
+    rmpcd_nlist *nl = new rmpcd_nlist();
+    nl->Npoints = Npoints;
+    nl->Nmax = Nmax;
+    size_t ne = (size_t)(Npoints > 0 ? Npoints : 1) * Nmax;
+    if (cudaMalloc(&nl->list, ne * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&nl->n, (size_t)(Npoints > 0 ? Npoints : 1) * sizeof(int)) != cudaSuccess) {
+        cudaFree(nl->list);
+        delete nl;
+        return fail(RMPCD_ERR_CUDA, "neighbor_list_t%%init: device allocation failed");
+    }
+    cudaMemsetAsync(nl->list, 0xff, ne * sizeof(int), stream());
+    cudaMemsetAsync(nl->n, 0, (size_t)(Npoints > 0 ? Npoints : 1) * sizeof(int), stream());
+    *out = nl;
+    return sync();
+}
+
+int rmpcd_nlist_destroy(rmpcd_nlist *nl)
+{
+    if (!nl) return RMPCD_OK;
+    cudaStreamSynchronize(stream());
+    cudaFree(nl->list);
+    cudaFree(nl->n);
+    cudaFree(nl->stencil);
+    cudaFree(nl->pair_f);
+    cudaFree(nl->pair_e);
+    cudaFree(nl->contrib);
+    cudaFree(nl->ncontrib);
+    cudaFree(nl->d_status);
+    delete nl;
+    return RMPCD_OK;
+}
+
+// make_stencil, src/neighbor_list.f90:271-308 (closest, :310-322)
+int rmpcd_nlist_make_stencil(rmpcd_nlist *nl, rmpcd_cells *c, double cut)
+{
+    RMPCD_ARG(nl && c, "null argument");
+    int max_i = (int)floor(cut / c->a) + 1;
+    std::vector<int> st;
+    for (int i = -max_i; i <= max_i; i++)
+        for (int j = -max_i; j <= max_i; j++)
+            for (int k = -max_i; k <= max_i; k++) {
+                int o[3] = {i, j, k};
+                int dist_sq = 0;
+                for (int d = 0; d < 3; d++) {
+                    int v = abs(o[d]) - 1;
+                    if (v < 0) v = 0;
+                    dist_sq += v * v;
+                }
+                if (sqrt((double)dist_sq) < cut) {
+                    st.push_back(i);
+                    st.push_back(j);
+                    st.push_back(k);
+                }
+            }
+    cudaStreamSynchronize(stream());
+    cudaFree(nl->stencil);
+    nl->stencil = nullptr;
+    nl->n_stencil = (int)(st.size() / 3);
+    nl->max_i = max_i;
+    for (int k = 0; k < 3; k++) nl->box_cells[k] = c->L[k];
+    RMPCD_CUDA_TRY(cudaMalloc(&nl->stencil, st.size() * sizeof(int) + 4));
+    RMPCD_CUDA_TRY(cudaMemcpyAsync(nl->stencil, st.data(), st.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                   stream()));
+    return sync();
+}
+
+int rmpcd_nlist_stencil_size(const rmpcd_nlist *nl, int *n)
+{
+    RMPCD_ARG(nl && n, "null argument");
+    *n = nl->n_stencil;
+    return RMPCD_OK;
+}
+
+int rmpcd_nlist_update(rmpcd_nlist *nl, rmpcd_particles *s1, rmpcd_particles *s2, double radius,
+                       rmpcd_cells *c, const rmpcd_lj *lj)
+{
+    RMPCD_ARG(nl && s1 && s2 && c, "null argument");
+    RMPCD_ARG(s1->precision == RMPCD_FP64, "update_list: system1 (colloids) must be FP64");
+    RMPCD_ARG(s1->N == nl->Npoints, "update_list: system1 size differs from Npoints");
+    RMPCD_ARG(nl->stencil != nullptr, "update_list: make_stencil was not called");
+    PhaseTimer t("neigh list update");
+    cudaStream_t s = stream();
+    RMPCD_CUDA_TRY(cudaMemsetAsync(c->is_md, 0, (size_t)c->S, s));
+    RMPCD_CUDA_TRY(cudaMemsetAsync(c->is_reac, 1, (size_t)c->S, s));
+    if (s1->N == 0) return RMPCD_OK;
+    PView<double> cv = cur<double>(s1);
+    LJDev ld = lj_dev(lj);
+    if (s2->precision == RMPCD_FP32) {
+        PView<float> v = cur<float>(s2);
+        k_update_list<float><<<s1->N, kNlThreads, 0, s>>>(grid_of(c), cv.pos.x, cv.pos.y, cv.pos.z, cv.species,
+                                                          v.pos.x, v.pos.y, v.pos.z, v.species, c->count, c->start,
+                                                          nl->stencil, nl->n_stencil, radius * radius, ld,
+                                                          lj ? 1 : 0, nl->Nmax, nl->list, nl->n, c->is_md,
+                                                          c->is_reac, dev_error_word());
+    } else {
+        PView<double> v = cur<double>(s2);
+        k_update_list<double><<<s1->N, kNlThreads, 0, s>>>(grid_of(c), cv.pos.x, cv.pos.y, cv.pos.z, cv.species,
+                                                           v.pos.x, v.pos.y, v.pos.z, v.species, c->count, c->start,
+                                                           nl->stencil, nl->n_stencil, radius * radius, ld,
+                                                           lj ? 1 : 0, nl->Nmax, nl->list, nl->n, c->is_md,
+                                                           c->is_reac, dev_error_word());
+    }
+    RMPCD_CHECK_LAUNCH();
+    return check_dev_error(nullptr);
+}
+
+int rmpcd_nlist_download(const rmpcd_nlist *nl, int *list, int *n)
+{
+    RMPCD_ARG(nl, "null argument");
+    size_t ne = (size_t)nl->Npoints * nl->Nmax;
+    if (list && ne) {
+        RMPCD_CUDA_TRY(cudaMemcpyAsync(list, nl->list, ne * sizeof(int), cudaMemcpyDeviceToHost, stream()));
+    }
+    if (n && nl->Npoints)
+        RMPCD_CUDA_TRY(cudaMemcpyAsync(n, nl->n, (size_t)nl->Npoints * sizeof(int), cudaMemcpyDeviceToHost, stream()));
+    int rc = sync();
+    if (rc) return rc;
+    if (list && n)
+        for (int i = 0; i < nl->Npoints; i++)
+            for (int e = 0; e < nl->Nmax; e++) {
+                size_t q = (size_t)i * nl->Nmax + e;
+                list[q] = e < n[i] ? list[q] + 1 : 0;
+            }
+    return RMPCD_OK;
+}
+
+// compute_force, src/neighbor_list.f90:159-225
+int rmpcd_compute_force(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist *nl, const double L[3],
+                        const rmpcd_lj *lj, double *energy)
+{
+    RMPCD_ARG(ps1 && ps2 && nl && L && lj, "null argument");
+    RMPCD_ARG(ps1->precision == RMPCD_FP64, "compute_force: ps1 (colloids) must be FP64");
+    RMPCD_ARG(ps1->N == nl->Npoints, "compute_force: ps1 size differs from Npoints");
+    int rc = ensure_force_scratch(nl, ps2->N);
+    if (rc) return rc;
+    PhaseTimer tm("neigh list force");
+    cudaStream_t s = stream();
+    int C = ps1->N;
+    if (ps2->N > 0) k_flag_roll<<<grid_for(ps2->N, 256), 256, 0, s>>>(ps2->flags[ps2->cur], ps2->N);
+    int *max_contrib = nl->d_status;
+    int *cn = nl->d_status + 16;
+    int *clist = nl->d_status + 16 + 2 * nl->Npoints;
+    double *e_out = (double *)ps1->d_sums;
+    RMPCD_CUDA_TRY(cudaMemsetAsync(max_contrib, 0, sizeof(int), s));
+    ps2->force_zero = false;
+    ps1->force_zero = false;
+    if (C > 0) {
+        PView<double> cv = cur<double>(ps1);
+        LJDev ld = lj_dev(lj);
+        int gx = (nl->Nmax + 255) / 256;
+        if (gx > 64) gx = 64;
+        dim3 grid(gx, C);
+        // duplicates inside one list exist only when the stencil wraps the box
+        int serial = 0;
+        for (int k = 0; k < 3; k++)
+            if (2 * nl->max_i + 1 > nl->box_cells[k]) serial = 1;
+        if (ps2->precision == RMPCD_FP32) {
+            PView<float> v = cur<float>(ps2);
+            k_pair_forces<float><<<grid, 256, 0, s>>>(cv.pos.x, cv.pos.y, cv.pos.z, cv.species, v.pos.x, v.pos.y,
+                                                      v.pos.z, v.species, v.flags, nl->list, nl->n, nl->Nmax, L[0],
+                                                      L[1], L[2], ld, nl->pair_f, nl->pair_e, nl->contrib,
+                                                      nl->ncontrib, max_contrib);
+            k_apply_single<float><<<grid, 256, 0, s>>>(nl->list, nl->n, nl->Nmax, nl->contrib, nl->pair_f,
+                                                       nl->ncontrib, v.force.x, v.force.y, v.force.z);
+            k_apply_multi<float><<<1, 256, 0, s>>>(nl->list, nl->n, C, nl->Nmax, nl->contrib, nl->pair_f,
+                                                   nl->ncontrib, max_contrib, serial, v.force.x, v.force.y, v.force.z);
+        } else {
+            PView<double> v = cur<double>(ps2);
+            k_pair_forces<double><<<grid, 256, 0, s>>>(cv.pos.x, cv.pos.y, cv.pos.z, cv.species, v.pos.x, v.pos.y,
+                                                       v.pos.z, v.species, v.flags, nl->list, nl->n, nl->Nmax, L[0],
+                                                       L[1], L[2], ld, nl->pair_f, nl->pair_e, nl->contrib,
+                                                       nl->ncontrib, max_contrib);
+            k_apply_single<double><<<grid, 256, 0, s>>>(nl->list, nl->n, nl->Nmax, nl->contrib, nl->pair_f,
+                                                        nl->ncontrib, v.force.x, v.force.y, v.force.z);
+            k_apply_multi<double><<<1, 256, 0, s>>>(nl->list, nl->n, C, nl->Nmax, nl->contrib, nl->pair_f,
+                                                    nl->ncontrib, max_contrib, serial, v.force.x, v.force.y, v.force.z);
+        }
+        k_colloid_sum<<<C, kNlThreads, 0, s>>>(nl->n, nl->Nmax, nl->contrib, nl->pair_f, cv.force.x, cv.force.y,
+                                               cv.force.z, clist, cn);
+        k_reset_contrib<<<grid, 256, 0, s>>>(nl->list, nl->n, nl->Nmax, nl->contrib, nl->ncontrib);
+        if (energy) k_energy<<<1, 32, 0, s>>>(cn, clist, C, nl->Nmax, nl->pair_e, e_out);
+        RMPCD_CHECK_LAUNCH();
+    }
+    if (energy) {
+        if (C > 0) {
+            RMPCD_CUDA_TRY(cudaMemcpyAsync(energy, e_out, sizeof(double), cudaMemcpyDeviceToHost, s));
+            return sync();
+        }
+        *energy = 0;
+    }
+    return RMPCD_OK;
+}
+
+// compute_force_n2, src/neighbor_list.f90:227-264
+int rmpcd_compute_force_n2(rmpcd_particles *ps, const double L[3], const rmpcd_lj *lj, double *energy)
+{
+    RMPCD_ARG(ps && L && lj, "null argument");
+    RMPCD_ARG(ps->precision == RMPCD_FP64, "compute_force_n2: needs an FP64 system");
+    PhaseTimer tm("self force");
+    cudaStream_t s = stream();
+    int C = ps->N;
+    ps->force_zero = false;
+    double *e_out = ps->d_sums + 1;
+    if (C > 0) {
+        PView<double> v = cur<double>(ps);
+        LJDev ld = lj_dev(lj);
+        if (energy)
+            k_energy_n2<<<1, 32, 0, s>>>(v.pos.x, v.pos.y, v.pos.z, v.species, C, L[0], L[1], L[2], ld, e_out);
+        k_force_n2<<<grid_for(C, 128), 128, 0, s>>>(v.pos.x, v.pos.y, v.pos.z, v.species, C, L[0], L[1], L[2], ld,
+                                                    v.force.x, v.force.y, v.force.z);
+        RMPCD_CHECK_LAUNCH();
+    }
+    if (energy) {
+        if (C > 0) {
+            RMPCD_CUDA_TRY(cudaMemcpyAsync(energy, e_out, sizeof(double), cudaMemcpyDeviceToHost, s));
+            return sync();
+        }
+        *energy = 0;
+    }
+    return RMPCD_OK;
+}
+
+}  // extern "C"

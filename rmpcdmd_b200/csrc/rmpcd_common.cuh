@@ -1,0 +1,119 @@
+// Common definitions for the B200 solvent hot path: status handling, the
+// library stream, device error word, and small device helpers.
+//
+// Every translation unit is compiled with -fmad=false: the FP64 form must
+// reproduce the reference's separately-rounded multiply/add sequence
+// (gfortran on baseline x86-64 emits no FMA), and association order is kept
+// as written in the reference expressions.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+#include <string>
+
+#include "../../include/rmpcd.h"
+
+namespace rmpcd {
+
+// ---------------------------------------------------------------------------
+// status / last-error string (thread-local, as rmpcd_last_error_string reads)
+// ---------------------------------------------------------------------------
+void set_error(const char *fmt, ...);
+int fail(int code, const char *fmt, ...);
+
+#define RMPCD_CUDA_TRY(expr)                                                     \
+    do {                                                                         \
+        cudaError_t e__ = (expr);                                                \
+        if (e__ != cudaSuccess)                                                  \
+            return ::rmpcd::fail(RMPCD_ERR_CUDA, "%s:%d %s: %s", __FILE__,       \
+                                 __LINE__, #expr, cudaGetErrorString(e__));      \
+    } while (0)
+
+#define RMPCD_CHECK_LAUNCH()                                                     \
+    do {                                                                         \
+        cudaError_t e__ = cudaGetLastError();                                    \
+        if (e__ != cudaSuccess)                                                  \
+            return ::rmpcd::fail(RMPCD_ERR_CUDA, "%s:%d launch: %s", __FILE__,  \
+                                 __LINE__, cudaGetErrorString(e__));             \
+    } while (0)
+
+#define RMPCD_ARG(cond, msg)                                                     \
+    do {                                                                         \
+        if (!(cond)) return ::rmpcd::fail(RMPCD_ERR_INVALID, "%s", msg);         \
+    } while (0)
+
+// The single library stream every kernel runs on (created on first use for
+// the current device).  Host entry points that return device results
+// synchronize it.
+cudaStream_t stream();
+int sync();
+
+// Device error word: kernels OR bits in, never trap.  Checked by
+// rmpcd_get_status and by entry points that can raise a reference error.
+enum : unsigned {
+    DEV_ERR_NLIST_FULL = 1u,   // 'maximum of neighbor list reached'
+    DEV_ERR_WALL_LOOP = 2u,    // wall-crossing loop hit its iteration cap
+    DEV_ERR_RATTLE = 4u,       // RATTLE square root of a negative number
+};
+unsigned *dev_error_word();
+int check_dev_error(unsigned *bits_out);
+
+int sm_count();
+inline int grid_for(long long n, int block)
+{
+    long long g = (n + block - 1) / block;
+    long long cap = (long long)sm_count() * 32;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+// bit positions, src/common.f90:49-55
+constexpr int REAC_BIT = 1;
+constexpr int MD_BIT = 2;
+constexpr int WALL_BIT = 3;
+constexpr int PAST_MD_BIT = 4;
+constexpr int CATALYZED_BIT = 6;
+
+constexpr int PERIODIC_BC = 1;
+constexpr int BOUNCE_BACK_BC = 2;
+constexpr int SPECULAR_BC = 3;
+
+// rel_pos, src/common.f90:162-178: minimum image with strict < and >.
+template <typename R>
+__host__ __device__ inline R min_image(R r, double L)
+{
+    double h = 0.5 * L;
+    if ((double)r < -h) return (R)((double)r + L);
+    if ((double)r > h) return (R)((double)r - L);
+    return r;
+}
+__host__ __device__ inline double min_image_d(double r, double L)
+{
+    if (r < -0.5 * L) return r + L;
+    if (r > 0.5 * L) return r - L;
+    return r;
+}
+
+// floor of a double as the Fortran default integer
+__host__ __device__ inline int ifloor(double x) { return (int)floor(x); }
+
+// Unsigned ordering of non-negative doubles equals their numeric ordering,
+// so atomicMax on the bit pattern gives a max-reduction of r^2 values.
+__device__ inline void atomic_max_nonneg(unsigned long long *addr, double v)
+{
+    atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+template <typename T>
+__device__ inline T warp_max(T v)
+{
+    for (int o = 16; o > 0; o >>= 1) {
+        T w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = v > w ? v : w;
+    }
+    return v;
+}
+
+}  // namespace rmpcd

@@ -1,0 +1,255 @@
+#include "keys.cuh"
+#include "scan.cuh"
+#include "sortcore.cuh"
+#include "timers.cuh"
+
+namespace rmpcd {
+
+constexpr int kSmallSegment = 64;
+
+// key[i] = slot of particle i; histogram with one atomic per distinct key
+// per warp (consecutive particles usually share a cell).
+template <typename R>
+__global__ void k_key_count(Grid g, const R *__restrict__ x, const R *__restrict__ y,
+                            const R *__restrict__ z, int N, int *__restrict__ key,
+                            int *__restrict__ count)
+{
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < N; base += stride) {
+        long long i = base + threadIdx.x;
+        bool ok = i < N;
+        int s = -1;
+        if (ok) {
+            s = slot_of(g, (double)x[i], (double)y[i], (double)z[i]);
+            key[i] = s;
+        }
+        unsigned peers = __match_any_sync(0xffffffffu, s);
+        if (ok && lane == __ffs(peers) - 1) atomicAdd(count + s, __popc(peers));
+    }
+}
+
+// place every particle inside its cell; the order inside a cell is fixed
+// afterwards by k_segsort
+__global__ void k_perm(const int *__restrict__ key, int N, int *__restrict__ cursor,
+                       int *__restrict__ perm)
+{
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < N; base += stride) {
+        long long i = base + threadIdx.x;
+        bool ok = i < N;
+        int s = ok ? key[i] : -1;
+        unsigned peers = __match_any_sync(0xffffffffu, s);
+        int leader = __ffs(peers) - 1;
+        int b = 0;
+        if (ok && lane == leader) b = atomicAdd(cursor + s, __popc(peers));
+        b = __shfl_sync(peers, b, leader);
+        if (ok) perm[b + __popc(peers & lanemask_lt())] = (int)i;
+    }
+}
+
+// ascending insertion sort of short segments; long ones are queued
+__global__ void k_segsort_small(const int *__restrict__ start, const int *__restrict__ count,
+                                int S, int *__restrict__ perm, int *__restrict__ big,
+                                int *__restrict__ n_big)
+{
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
+        int n = count[s];
+        if (n <= 1) continue;
+        if (n > kSmallSegment) {
+            int q = atomicAdd(n_big, 1);
+            big[q] = s;
+            continue;
+        }
+        int *a = perm + start[s];
+        for (int i = 1; i < n; i++) {
+            int v = a[i];
+            int j = i - 1;
+            while (j >= 0 && a[j] > v) {
+                a[j + 1] = a[j];
+                j--;
+            }
+            a[j + 1] = v;
+        }
+    }
+}
+
+__device__ inline int lower_bound_int(const int *a, int n, int v)
+{
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (a[mid] < v) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// one block per long segment: bottom-up merge sort of distinct values, every
+// element placed by its rank in the partner run; tmp is scratch of the same
+// extent as the segment
+__global__ void k_segsort_big(const int *__restrict__ start, const int *__restrict__ count,
+                              const int *__restrict__ big, const int *__restrict__ n_big,
+                              int *__restrict__ perm, int *__restrict__ tmp)
+{
+    for (int q = blockIdx.x; q < *n_big; q += gridDim.x) {
+        int s = big[q];
+        int n = count[s];
+        int *a = perm + start[s];
+        int *b = tmp + start[s];
+        int *src = a, *dst = b;
+        for (int w = 1; w < n; w <<= 1) {
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                int run = i / w;
+                int r0 = run * w;
+                int v = src[i];
+                int pos;
+                if ((run & 1) == 0) {
+                    int p0 = r0 + w;
+                    int pn = min(w, max(0, n - p0));
+                    pos = r0 + (i - r0) + lower_bound_int(src + p0, pn, v);
+                } else {
+                    int p0 = r0 - w;
+                    pos = p0 + (i - r0) + lower_bound_int(src + p0, w, v);
+                }
+                dst[pos] = v;
+            }
+            __syncthreads();
+            int *t = src;
+            src = dst;
+            dst = t;
+        }
+        if (src != a)
+            for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = src[i];
+        __syncthreads();
+    }
+}
+
+template <typename R>
+__global__ void k_gather(PView<R> s, PView<R> d, const int *__restrict__ perm, int N,
+                         int with_force, int with_force_old)
+{
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < N;
+         j += (long long)gridDim.x * blockDim.x) {
+        int i = perm[j];
+        d.pos.x[j] = s.pos.x[i];
+        d.pos.y[j] = s.pos.y[i];
+        d.pos.z[j] = s.pos.z[i];
+        d.vel.x[j] = s.vel.x[i];
+        d.vel.y[j] = s.vel.y[i];
+        d.vel.z[j] = s.vel.z[i];
+        d.ix[j] = s.ix[i];
+        d.iy[j] = s.iy[i];
+        d.iz[j] = s.iz[i];
+        d.id[j] = s.id[i];
+        d.species[j] = s.species[i];
+        d.flags[j] = s.flags[i];
+        if (with_force) {
+            d.force.x[j] = s.force.x[i];
+            d.force.y[j] = s.force.y[i];
+            d.force.z[j] = s.force.z[i];
+        }
+        if (with_force_old) {
+            d.force_old.x[j] = s.force_old.x[i];
+            d.force_old.y[j] = s.force_old.y[i];
+            d.force_old.z[j] = s.force_old.z[i];
+        }
+    }
+}
+
+template <typename R>
+static int count_and_scan_t(rmpcd_cells *c, rmpcd_particles *p)
+{
+    cudaStream_t st = stream();
+    RMPCD_CUDA_TRY(cudaMemsetAsync(c->count, 0, (size_t)c->S * sizeof(int), st));
+    PView<R> v = cur<R>(p);
+    if (p->N > 0)
+        k_key_count<R><<<grid_for(p->N, 256), 256, 0, st>>>(grid_of(c), v.pos.x, v.pos.y, v.pos.z,
+                                                           p->N, p->key, c->count);
+    RMPCD_CHECK_LAUNCH();
+    return exclusive_scan(c->count, c->start, c->cursor, c->S, c->scan_tmp, false, st);
+}
+
+int count_and_scan(rmpcd_cells *c, rmpcd_particles *p, bool)
+{
+    if (p->precision == RMPCD_FP32) return count_and_scan_t<float>(c, p);
+    return count_and_scan_t<double>(c, p);
+}
+
+int build_perm_unsorted(rmpcd_cells *c, rmpcd_particles *p)
+{
+    if (p->N == 0) return RMPCD_OK;
+    k_perm<<<grid_for(p->N, 256), 256, 0, stream()>>>(p->key, p->N, c->cursor, p->perm);
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+int build_perm(rmpcd_cells *c, rmpcd_particles *p)
+{
+    int rc = build_perm_unsorted(c, p);
+    if (rc) return rc;
+    return sort_perm_segments(c, p);
+}
+
+int sort_perm_segments(rmpcd_cells *c, rmpcd_particles *p)
+{
+    cudaStream_t st = stream();
+    if (p->N == 0) return RMPCD_OK;
+    // big-segment queue lives in cursor[] (free once perm is built) plus a counter
+    int *n_big = p->d_ints;
+    RMPCD_CUDA_TRY(cudaMemsetAsync(n_big, 0, sizeof(int), st));
+    k_segsort_small<<<grid_for(c->S, 256), 256, 0, st>>>(c->start, c->count, c->S, p->perm,
+                                                         c->cursor, n_big);
+    k_segsort_big<<<64, 512, 0, st>>>(c->start, c->count, c->cursor, n_big, p->perm, p->key);
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+template <typename R>
+static int gather_t(rmpcd_particles *p)
+{
+    if (p->N > 0) {
+        k_gather<R><<<grid_for(p->N, 256), 256, 0, stream()>>>(
+            cur<R>(p), alt<R>(p), p->perm, p->N, p->force_zero ? 0 : 1, p->force_old_zero ? 0 : 1);
+        RMPCD_CHECK_LAUNCH();
+    }
+    p->cur = 1 - p->cur;
+    // fields that were not gathered are all zero: keep the live pointer on the
+    // (zero) previous arrays
+    for (int k = 0; k < 3; k++) {
+        if (p->force_zero) {
+            void *t = p->force[p->cur][k];
+            p->force[p->cur][k] = p->force[1 - p->cur][k];
+            p->force[1 - p->cur][k] = t;
+        }
+        if (p->force_old_zero) {
+            void *t = p->force_old[p->cur][k];
+            p->force_old[p->cur][k] = p->force_old[1 - p->cur][k];
+            p->force_old[1 - p->cur][k] = t;
+        }
+    }
+    return RMPCD_OK;
+}
+
+int gather_all(rmpcd_particles *p)
+{
+    if (p->precision == RMPCD_FP32) return gather_t<float>(p);
+    return gather_t<double>(p);
+}
+
+int sort_particles(rmpcd_cells *c, rmpcd_particles *p)
+{
+    int rc;
+    {
+        PhaseTimer t("count");
+        rc = count_and_scan(c, p, true);
+        if (rc) return rc;
+    }
+    PhaseTimer t("sort");
+    rc = build_perm(c, p);
+    if (rc) return rc;
+    return gather_all(p);
+}
+
+}  // namespace rmpcd

@@ -1,0 +1,33 @@
+// Counting and stable cell sort of a particle system (the core of
+// count_particles, src/cell_system.f90:86-129, and particle_system_t%sort,
+// src/particle_system.f90:304-355).
+//
+// Schedule (all on the library stream):
+//   key/count  one pass over positions: key[i] = slot, warp-aggregated
+//              atomic histogram into count[]
+//   scan       exclusive scan count -> start, cursor
+//   perm       one pass over keys: warp-aggregated cursor atomics give every
+//              particle a place inside its cell: perm[place] = i
+//   segsort    each cell's perm segment is sorted ascending, which restores
+//              the reference's single-thread order (stable in i)
+//   gather     dst[j] = src[perm[j]] for every field: coalesced writes,
+//              reads local in the Hilbert order
+#pragma once
+#include "state.cuh"
+
+namespace rmpcd {
+
+// key[] and count/start/cursor of p under the current origin of c
+int count_and_scan(rmpcd_cells *c, rmpcd_particles *p, bool keep_key);
+// perm[] from key[] and cursor[] (cell order fixed, in-cell order arbitrary)
+int build_perm_unsorted(rmpcd_cells *c, rmpcd_particles *p);
+// ascending sort of every cell's perm segment (uses cursor[] and key[] as scratch)
+int sort_perm_segments(rmpcd_cells *c, rmpcd_particles *p);
+// both of the above
+int build_perm(rmpcd_cells *c, rmpcd_particles *p);
+// gather every field through perm into the other buffer and flip buffers
+int gather_all(rmpcd_particles *p);
+// full sort
+int sort_particles(rmpcd_cells *c, rmpcd_particles *p);
+
+}  // namespace rmpcd

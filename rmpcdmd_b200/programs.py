@@ -1,0 +1,169 @@
+"""Host drivers for the reference programs whose solvent loops this library
+accelerates, written against the C ABI exactly as the Fortran programs call
+their modules:
+
+  * :class:`SingleDimerPBC` -- programs/single_dimer_pbc.f90:108-445
+  * :func:`bulk_fluid`      -- the loop of test/setup_bulk_decay.f90:99-121
+
+The randomness differs from the reference only in its source (Philox keyed
+by seed and step instead of per-thread Threefry streams); the order of random
+consumers is fixed so that any other driver making the same calls draws the
+same numbers.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import api as A
+
+PI_SP = float(np.float32(3.14159265))  # the default-real constant of the program
+TWO_SIXTH = 2.0 ** (1.0 / 6.0)
+
+
+def dimer_lj_tables(sigma_C, sigma_N, epsilon_C, epsilon_N, epsilon_CC, epsilon_NC, epsilon_NN):
+    """The two lj_params_t tables of programs/single_dimer_pbc.f90:156-178."""
+    eps = np.zeros((2, 2))
+    eps[:, 0] = epsilon_C
+    eps[:, 1] = epsilon_N
+    sig = np.zeros((2, 2))
+    sig[:, 0] = sigma_C
+    sig[:, 1] = sigma_N
+    solvent_colloid = (eps.copy(), sig.copy(), sig * TWO_SIXTH)
+    ceps = np.array([[epsilon_CC, epsilon_NC], [epsilon_NC, epsilon_NN]], dtype=np.float64)
+    csig = np.array([[2 * sigma_C, sigma_C + sigma_N], [sigma_C + sigma_N, 2 * sigma_N]], dtype=np.float64)
+    colloid = (ceps, csig, csig * TWO_SIXTH)
+    return solvent_colloid, colloid
+
+
+def dimer_masses(rho, sigma_C, sigma_N):
+    """mass = rho * sigma**3 * 4 * 3.14159265/3 (programs/single_dimer_pbc.f90:180-181)."""
+    return np.array([rho * sigma_C ** 3 * 4 * PI_SP / 3, rho * sigma_N ** 3 * 4 * PI_SP / 3])
+
+
+class SingleDimerPBC:
+    """programs/single_dimer_pbc.f90 on the GPU.
+
+    The neighbor-list capacity is a parameter: the program's own value,
+    int(300*max(sigma)**3), is too small for sigma = 2 with skin 2 and makes the
+    reference stop with 'maximum of neighbor list reached'.
+    """
+
+    def __init__(self, L=(32, 32, 32), rho=10, T=1.0 / 3.0, tau=1.0, N_MD=100, sigma_C=2.0, sigma_N=2.0, d=4.5,
+                 epsilon_C=(1.0, 1.0), epsilon_N=(1.0, 0.5), epsilon_CC=1.0, epsilon_NC=1.0, epsilon_NN=1.0,
+                 probability=1.0, bulk_rmpcd=False, bulk_rate=0.001, do_thermostat=False, do_hydro=True,
+                 seed=1, skin=2.0, list_capacity=None, precision=A.FP64, initial_velocities=None):
+        self.L = np.asarray(L, dtype=np.int32)
+        self.rho, self.T, self.tau, self.N_MD = rho, T, tau, N_MD
+        self.dt = tau / N_MD
+        self.d = d
+        self.prob = probability
+        self.bulk_rmpcd, self.bulk_rate = bulk_rmpcd, bulk_rate
+        self.do_thermostat, self.do_hydro = do_thermostat, do_hydro
+        self.skin = skin
+        self.N = int(rho * self.L.prod())
+        (e, s, c), (ce, cs, cc) = dimer_lj_tables(sigma_C, sigma_N, epsilon_C, epsilon_N, epsilon_CC, epsilon_NC,
+                                                  epsilon_NN)
+        self.solvent_colloid_lj = A.LJParams(e, s, c)
+        self.colloid_lj = A.LJParams(ce, cs, cc)
+        self.max_cut = float(c.max())
+        self.mass = dimer_masses(rho, sigma_C, sigma_N)
+        self.rng = A.Rng(seed)
+        self.solvent = A.ParticleSystem(self.N, 2, None, precision)
+        self.colloids = A.ParticleSystem(2, 2, self.mass)
+        self.colloids.species = [1, 2]
+        if initial_velocities is not None:
+            self.solvent.vel = initial_velocities
+        else:
+            self.solvent.maxwell(T, seed)
+        self.solvent.species = 1
+        self.cells = A.CellSystem(self.L, 1.0)
+        self.edges = self.cells.edges
+        cpos = np.array([self.edges / 2.0, self.edges / 2.0])
+        cpos[1, 0] += d
+        self.colloids.pos = cpos
+        self.solvent.random_placement(self.edges, self.colloids, self.solvent_colloid_lj, seed)
+        self.solvent.sort(self.cells)
+        cap = list_capacity if list_capacity is not None else int(300 * max(sigma_C, sigma_N) ** 3)
+        self.neigh = A.NeighborList(2, cap)
+        self.neigh.make_stencil(self.cells, self.max_cut + skin)
+        self.neigh.update_list(self.colloids, self.solvent, self.max_cut + skin, self.cells, self.solvent_colloid_lj)
+        self.cut_sq = self.solvent_colloid_lj.cut_sq
+        self.e1 = A.compute_force(self.colloids, self.solvent, self.neigh, self.edges, self.solvent_colloid_lj)
+        self.e2 = A.compute_force_n2(self.colloids, self.edges, self.colloid_lj)
+        self.solvent.copy_force_old()
+        self.colloids.copy_force_old()
+        self.n_extra_sorting = 0
+        self.md_steps = 0
+
+    def md_step(self, want_energy=False):
+        """One pass of md_loop, programs/single_dimer_pbc.f90:306-384."""
+        s, c, dt = self.solvent, self.colloids, self.dt
+        A.md_pos(s, dt)
+        c.copy_pos_rattle()
+        A.colloid_vv_pos(c, dt, self.mass)
+        A.rattle_dimer_pos(c, self.d, dt, self.edges)
+        so_max = s.maximum_displacement()
+        co_max = c.maximum_displacement()
+        if (co_max >= self.skin * 0.1) or (so_max >= self.skin * 0.89):
+            self._resort()
+            self.n_extra_sorting += 1
+        s.switch_force()
+        c.switch_force()
+        s.zero_force()
+        c.zero_force()
+        self.e1 = A.compute_force(c, s, self.neigh, self.edges, self.solvent_colloid_lj, energy=want_energy)
+        self.e2 = A.compute_force_n2(c, self.edges, self.colloid_lj, energy=want_energy)
+        A.md_vel(s, dt)
+        A.colloid_vv_vel(c, dt, self.mass)
+        A.rattle_dimer_vel(c, self.d, dt, self.edges)
+        A.flag_particles_nl(self.neigh, c, s, self.edges, self.cut_sq[0, 0])
+        A.change_species(s, c, self.edges, self.cut_sq[0, 0], self.cut_sq[0, 1], self.prob, self.rng)
+        self.md_steps += 1
+
+    def _resort(self):
+        A.apply_pbc(self.solvent, self.edges)
+        A.apply_pbc(self.colloids, self.edges)
+        self.solvent.sort(self.cells)
+        self.neigh.update_list(self.colloids, self.solvent, self.max_cut + self.skin, self.cells,
+                               self.solvent_colloid_lj)
+        self.solvent.copy_pos_old()
+        self.colloids.copy_pos_old()
+
+    def interval(self):
+        """md_loop followed by the MPCD part, programs/single_dimer_pbc.f90:303-443."""
+        for _ in range(self.N_MD):
+            self.md_step()
+        self.cells.random_shift(self.rng)
+        self._resort()
+        A.simple_mpcd_step(self.solvent, self.cells, self.rng, thermostat=self.do_thermostat, T=self.T,
+                           hydro=self.do_hydro)
+        if self.bulk_rmpcd:
+            A.bulk_reaction(self.solvent, self.cells, 2, 1, self.bulk_rate, self.tau, self.rng)
+        else:
+            A.refuel(self.solvent, self.colloids, self.edges, int(self.L[0]))
+
+    def observables(self):
+        """temperature, kinetic energy, v_com and n_solvent of the interval."""
+        te = A.compute_temperature(self.solvent, self.cells)
+        cv = self.colloids.vel
+        vs = A.velocity_sums(self.solvent)
+        kin = (self.mass[0] * (cv[0] ** 2).sum() + self.mass[1] * (cv[1] ** 2).sum()) / 2 + vs[0] / 2
+        vcom = (vs[1:] + self.mass[0] * cv[0] + self.mass[1] * cv[1]) / (self.N + self.mass[0] + self.mass[1])
+        return dict(temperature=te, kinetic=kin, v_com=vcom, n_solvent=A.n_solvent(self.solvent, 2))
+
+
+def bulk_fluid(L, rho=10, T=1.0 / 3.0, tau=1.0, n_intervals=200, seed=1, precision=A.FP64, alpha=None):
+    """Bulk SRD fluid: Maxwell velocities, uniform positions, sorted once,
+    then n_intervals of collide -> stream -> shift -> sort (fused)."""
+    L = np.asarray(L, dtype=np.int32)
+    N = int(rho * L.prod())
+    cells = A.CellSystem(L, 1.0)
+    p = A.ParticleSystem(N, 1, None, precision)
+    p.random_placement(cells.edges, seed=seed)
+    p.maxwell(T, seed)
+    p.species = 1
+    rng = A.Rng(seed)
+    cells.random_shift(rng)
+    p.sort(cells)
+    A.bulk_run(p, cells, rng, tau, n_intervals, alpha=alpha)
+    return p, cells, rng

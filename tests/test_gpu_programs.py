@@ -1,0 +1,74 @@
+"""GPU parity of whole schedules: the fused bulk-fluid interval against the
+oracle's collide -> stream -> shift -> sort loop, and the single_dimer_pbc
+MD + MPCD loop, both bit-exact in FP64; FP32 bulk runs checked against the
+conservation laws and the FP64 run."""
+import numpy as np
+import pytest
+
+from helpers import assert_cells_same, assert_same, make_pair
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("L,rho", [([16, 16, 16], 10), ([12, 10, 9], 10), ([6, 5, 4], 300), ([1, 20, 5], 10)])
+def test_bulk_run_fp64_bit_exact(rm, oracle, L, rho):
+    N = int(np.prod(L)) * rho
+    (oc, op), (gc, gp) = make_pair(rm, oracle, L, N, seed=N % 101, origin=[-0.1, -0.9, -0.45])
+    n_int = 4
+    rng = rm.Rng(99, 7)
+    rm.bulk_run(gp, gc, rng, 1.0, n_int)
+    oracle.bulk_run(op, oc, n_int, 1.0, 99, 7)
+    assert rng.step == 7 + 2 * n_int
+    assert np.array_equal(gc.origin, oc.origin)
+    assert_cells_same(gc, oc)
+    assert_same(gp, op, ("pos", "vel", "image", "id", "species", "flags"))
+
+
+def test_bulk_run_alpha_and_injected_axes(rm, oracle):
+    L = [8, 8, 8]
+    N = 5120
+    (oc, op), (gc, gp) = make_pair(rm, oracle, L, N, seed=3)
+    rm.bulk_run(gp, gc, rm.Rng(5, 0), 1.0, 3, alpha=2.3)
+    oracle.bulk_run(op, oc, 3, 1.0, 5, 0, alpha=2.3)
+    assert_same(gp, op, ("pos", "vel", "image", "id"))
+
+
+def test_bulk_run_fp32_conservation(rm, oracle):
+    L = [16, 16, 16]
+    N = 40960
+    (oc, op), (gc, gp) = make_pair(rm, oracle, L, N, seed=4, precision=32)
+    p0 = gp.download("vel").sum(0)
+    e0 = (gp.download("vel") ** 2).sum()
+    rm.bulk_run(gp, gc, rm.Rng(8), 1.0, 20)
+    v = gp.download("vel")
+    # SRD conserves momentum and energy cell by cell; FP32 drift per step is tiny
+    assert np.abs(v.sum(0) - p0).max() / np.sqrt(e0) < 1e-4
+    assert abs((v ** 2).sum() - e0) / e0 < 1e-4
+    # the final state is sorted for the final grid
+    ids = gp.download("id")
+    assert np.array_equal(np.sort(ids), np.arange(1, N + 1))
+    cnt = gc.cell_count
+    assert cnt.sum() == N
+    # temperature of the FP32 run agrees with the FP64 oracle run statistically
+    oracle.bulk_run(op, oc, 20, 1.0, 8, 0)
+    t64 = oracle.compute_temperature(op, oc)
+    t32 = rm.compute_temperature(gp, gc)
+    assert abs(t32 - t64) / t64 < 0.05
+
+
+@pytest.mark.parametrize("n_int", [2])
+def test_single_dimer_pbc_bit_exact(rm, oracle, n_int):
+    from oracle.programs import SingleDimerPBC as OD
+    from rmpcdmd_b200.programs import SingleDimerPBC as GD
+
+    kw = dict(L=(12, 12, 12), rho=10, N_MD=25, seed=11, list_capacity=4000)
+    o = OD(**kw)
+    g = GD(**kw)
+    assert_same(g.solvent, o.s, ("pos", "vel", "species", "id"))
+    for _ in range(n_int):
+        o.interval()
+        g.interval()
+    assert_same(g.colloids, o.c, ("pos", "vel", "force"))
+    assert_same(g.solvent, o.s, ("pos", "vel", "image", "id", "species", "flags", "force"))
+    assert g.n_extra_sorting == o.n_extra_sorting
+    assert g.rng.step == o.step

@@ -1,0 +1,99 @@
+"""GPU parity: count_particles and particle_system_t%sort (bit-exact).
+
+cell_count, cell_start, the sorted order (id) and every permuted array must
+equal the oracle's single-thread result, including the padded-slot boxes,
+walls, empty systems, oversized cells and positions outside the box.
+"""
+import numpy as np
+import pytest
+
+from helpers import assert_cells_same, assert_same, make_pair, upload
+
+pytestmark = pytest.mark.gpu
+
+BOXES = [([8, 8, 8], 5120), ([5, 7, 9], 3150), ([1, 20, 5], 1000), ([32, 32, 32], 327680), ([96, 96, 96], 400000)]
+
+
+@pytest.mark.parametrize("L,N", BOXES)
+@pytest.mark.parametrize("precision", [64, 32])
+def test_sort_bit_exact(rm, oracle, L, N, precision):
+    (oc, op), (gc, gp) = make_pair(rm, oracle, L, N, seed=N % 97, precision=precision,
+                                   origin=[-0.25, -0.5, -0.75], sorted_=False)
+    if precision == 32:
+        # the FP32 form keys its float positions: give the oracle the same values
+        op.pos[:] = gp.download("pos")
+        op.vel[:] = gp.download("vel")
+    op.sort(oc)
+    gp.sort(gc)
+    assert_cells_same(gc, oc)
+    assert_same(gp, op, ("pos", "vel", "image", "id", "species", "flags"))
+    assert np.array_equal(gp.id_to_idx, op.id_to_idx)
+
+
+def test_sort_chain_with_forces_and_pos_old(rm, oracle):
+    L, N = [12, 10, 9], 12000
+    (oc, op), (gc, gp) = make_pair(rm, oracle, L, N, seed=3)
+    rng = np.random.default_rng(4)
+    op.force[:] = rng.normal(size=(N, 3))
+    op.force_old[:] = rng.normal(size=(N, 3))
+    op.image[:] = rng.integers(-3, 3, size=(N, 3))
+    op.flags[:] = rng.integers(0, 64, size=N)
+    upload(gp, op, ("force", "force_old", "image", "flags"))
+    for k in range(4):
+        o = rng.random(3) - 1
+        oc.origin = o
+        gc.origin = o
+        op.pos[:] = (op.pos + rng.normal(size=(N, 3)) * 0.3) % L
+        gp.upload("pos", op.pos)
+        op.sort(oc)
+        gp.sort(gc)
+        assert_cells_same(gc, oc)
+        assert_same(gp, op, ("pos", "vel", "force", "force_old", "image", "id", "species", "flags", "pos_old"))
+
+
+def test_sort_walls(rm, oracle):
+    (oc, op), (gc, gp) = make_pair(rm, oracle, [6, 6, 6], 3000, seed=5, walls=True, origin=[-0.4, -0.6, 0.0])
+    assert gc.N == oc.S
+    assert_cells_same(gc, oc)
+    assert_same(gp, op)
+
+
+def test_sort_empty_and_single(rm, oracle):
+    for N in (0, 1):
+        (oc, op), (gc, gp) = make_pair(rm, oracle, [4, 4, 4], N, seed=1)
+        assert_cells_same(gc, oc)
+        assert_same(gp, op)
+
+
+def test_sort_one_dense_cell(rm, oracle):
+    # 5000 particles in one cell: the long-segment ordering path
+    N = 5000
+    (oc, op), (gc, gp) = make_pair(rm, oracle, [4, 4, 4], N, seed=2, sorted_=False)
+    rng = np.random.default_rng(9)
+    op.pos[:] = 1.0 + 0.5 * rng.random((N, 3))
+    op.pos[::7] = rng.random((len(op.pos[::7]), 3)) * 4
+    gp.upload("pos", op.pos)
+    op.sort(oc)
+    gp.sort(gc)
+    assert_cells_same(gc, oc)
+    assert_same(gp, op)
+
+
+def test_sort_positions_outside_box(rm, oracle):
+    # out-of-box positions are hashed as the reference's compact_p_to_h does
+    N = 4000
+    (oc, op), (gc, gp) = make_pair(rm, oracle, [8, 6, 10], N, seed=6, sorted_=False)
+    rng = np.random.default_rng(10)
+    op.pos[:] = rng.random((N, 3)) * 30 - 10
+    gp.upload("pos", op.pos)
+    op.sort(oc)
+    gp.sort(gc)
+    assert_cells_same(gc, oc)
+    assert_same(gp, op)
+
+
+def test_count_particles(rm, oracle):
+    (oc, op), (gc, gp) = make_pair(rm, oracle, [16, 8, 12], 20000, seed=7, sorted_=False, origin=[-0.9, -0.1, -0.5])
+    op.count(oc)
+    gc.count_particles(gp)
+    assert_cells_same(gc, oc)

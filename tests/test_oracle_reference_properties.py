@@ -1,0 +1,145 @@
+"""The reference's own tests, ported to the oracle (CPU).
+
+These are the checks RMPCDMD's ctest suite holds for the hot path; they pin
+the restatement to the reference's documented behaviour:
+  test/test_cell_system_0.f90      counts, starts, Hilbert-monotone order
+  test/test_neighbor_list_0.f90    list completeness at the cutoff
+  test/test_md_0.f90               wall reflection in cell_md_pos_ywall
+  test/test_particle_system_0.f90  maximum displacement bound and zero
+Seeds are fixed here (the reference seeds from the clock).
+"""
+import numpy as np
+import pytest
+
+
+def cartesian(pos, c):
+    p = np.floor(pos / c.g.a - c.origin).astype(np.int64)
+    L = c.L
+    for k in (0, 1):
+        p[p[:, k] == L[k], k] = 0
+    if not c.g.has_walls:
+        p[p[:, 2] == L[2], 2] = 0
+    return p
+
+
+def test_cell_system_0(oracle):
+    # test/test_cell_system_0.f90:37-69 with N = 2e5 (the reference uses 1e6)
+    N = 200_000
+    L = [120, 30, 30]
+    rng = np.random.default_rng(1)
+    c = oracle.Cells(L, 1.0)
+    p = oracle.Particles(N)
+    p.pos[:] = rng.random((N, 3)) * L
+    p.sort(c)
+    p.count(c)
+    S = c.S
+    assert c.cell_start[0] == 1
+    assert c.cell_start[S - 1] == N + 1
+    assert c.cell_count.sum() == N
+    # every particle sits in the cell its Hilbert slot decodes to
+    slots = np.repeat(np.arange(S), c.cell_count)
+    occupied = np.unique(slots)
+    decoded = {h: oracle.compact_h_to_p(h, c.M) for h in occupied}
+    want = np.array([decoded[h] for h in slots])
+    assert np.array_equal(cartesian(p.pos, c), want)
+
+
+def test_sort_is_stable(oracle):
+    N = 5000
+    rng = np.random.default_rng(2)
+    c = oracle.Cells([8, 8, 8])
+    p = oracle.Particles(N)
+    p.pos[:] = rng.random((N, 3)) * 8
+    p.sort(c)
+    # ids inside each cell ascend: the single-thread scatter keeps the old order
+    for s in np.nonzero(c.cell_count > 1)[0]:
+        a = c.cell_start[s] - 1
+        ids = p.id[a:a + c.cell_count[s]]
+        assert (np.diff(ids) > 0).all()
+    assert sorted(p.id) == list(range(1, N + 1))
+    assert np.array_equal(p.id_to_idx[p.id - 1], np.arange(1, N + 1))
+
+
+def test_neighbor_list_0(oracle):
+    # test/test_neighbor_list_0.f90:47-81
+    L = np.array([20, 10, 35])
+    rho = 20
+    N = int(L.prod()) * rho
+    rng = np.random.default_rng(3)
+    c = oracle.Cells(L, 1.0)
+    s = oracle.Particles(N)
+    col = oracle.Particles(20)
+    s.species[:] = 1
+    col.species[:] = 1
+    s.pos[:] = rng.random((N, 3)) * L
+    col.pos[:] = rng.random((20, 3)) * L
+    s.sort(c)
+    cutoff = 3.6
+    nl = oracle.NeighborList(20, rho * 6 * int(cutoff ** 3))
+    nl.make_stencil(c, cutoff)
+    nl.update_list(col, s, cutoff, c)
+    for i in range(20):
+        d = s.pos - col.pos[i]
+        d -= L * np.round(d / L)
+        inside = np.nonzero((d * d).sum(1) < cutoff ** 2)[0] + 1
+        assert set(inside) <= set(nl.list[i, :nl.n[i]])
+
+
+@pytest.mark.parametrize("bc", [2, 3])
+def test_md_0(oracle, bc):
+    # test/test_md_0.f90:31-101, bounce-back (2) and specular (3) y walls
+    N = 679
+    L = np.array([1, 20, 5])
+    rng = np.random.default_rng(4 + bc)
+    c = oracle.Cells(L, 1.0)
+    c.set_bc([1, bc, 1])
+    p = oracle.Particles(N, 1)
+    for _ in range(10):
+        p.pos[:] = rng.random((N, 3)) * L
+        p.sort(c)
+        p.vel[:] = (-0.5 + rng.random((N, 3))) * 2 * L
+        x_old, v_old = p.pos.copy(), p.vel.copy()
+        will = (x_old[:, 1] + v_old[:, 1] < 0) | (x_old[:, 1] + v_old[:, 1] > L[1])
+        c.is_md[:] = 0
+        oracle.cell_md_pos_wall(c, p, 1, 1.0, False)
+        assert np.allclose(np.linalg.norm(p.vel, axis=1), np.linalg.norm(v_old, axis=1))
+        assert (p.pos[:, 1] > 0).all() and (L[1] - p.pos[:, 1] > 0).all()
+        if bc == 2:
+            assert np.allclose(p.vel[will], -v_old[will])
+        else:
+            assert np.allclose(p.vel[will, 0], v_old[will, 0])
+            assert np.allclose(p.vel[will, 1], -v_old[will, 1])
+            assert np.allclose(p.vel[will, 2], v_old[will, 2])
+
+
+def test_particle_system_0(oracle):
+    # test/test_particle_system_0.f90:29-47
+    N = 3000
+    rng = np.random.default_rng(6)
+    p = oracle.Particles(N)
+    p.pos[:] = rng.random((N, 3)) * [1, 20, 5]
+    p.pos_old[:] = p.pos
+    i = int(rng.integers(N))
+    x = rng.random(3)
+    p.pos[i] += x
+    assert np.sqrt(3.0) - p.maximum_displacement() > 0
+    p.pos[i] -= x
+    assert abs(p.maximum_displacement()) <= 12 * np.finfo(float).eps
+
+
+def test_srd_conserves_cell_momentum_and_energy(oracle):
+    N = 20000
+    rng = np.random.default_rng(7)
+    c = oracle.Cells([10, 10, 10])
+    p = oracle.Particles(N)
+    p.species[:] = 1
+    p.pos[:] = rng.random((N, 3)) * 10
+    p.vel[:] = rng.normal(size=(N, 3))
+    c.origin = [-0.3, -0.7, -0.1]
+    p.sort(c)
+    v0 = p.vel.copy()
+    oracle.simple_mpcd_step(p, c, 9, 1)
+    for s in np.nonzero(c.cell_count > 1)[0][:500]:
+        a, n = c.cell_start[s] - 1, c.cell_count[s]
+        assert np.allclose(v0[a:a + n].sum(0), p.vel[a:a + n].sum(0), atol=1e-12)
+        assert np.isclose((v0[a:a + n] ** 2).sum(), (p.vel[a:a + n] ** 2).sum(), rtol=1e-12)
