@@ -11,9 +11,15 @@ namespace rmpcd {
 
 __host__ __device__ inline void cell_coords(const Grid &g, double x, double y, double z, int p[3])
 {
-    p[0] = ifloor((x / g.a) - g.origin[0]);
-    p[1] = ifloor((y / g.a) - g.origin[1]);
-    p[2] = ifloor((z / g.a) - g.origin[2]);
+    // x / a is exact for a = 1 (every program uses a = 1): skip the division
+    if (g.a != 1.0) {
+        x = x / g.a;
+        y = y / g.a;
+        z = z / g.a;
+    }
+    p[0] = ifloor(x - g.origin[0]);
+    p[1] = ifloor(y - g.origin[1]);
+    p[2] = ifloor(z - g.origin[2]);
     if (p[0] == g.L[0]) p[0] = 0;
     if (p[1] == g.L[1]) p[1] = 0;
     if ((!g.has_walls) && (p[2] == g.L[2])) p[2] = 0;

@@ -125,7 +125,7 @@ __global__ void k_apply_pbc(PView<R> v, double e0, double e1, double e2)
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < v.N;
          i += (long long)gridDim.x * blockDim.x) {
         R x = v.pos.x[i], y = v.pos.y[i], z = v.pos.z[i];
-        int jx = ifloor((double)x / e0), jy = ifloor((double)y / e1), jz = ifloor((double)z / e2);
+        int jx = floor_div_edge((double)x, e0), jy = floor_div_edge((double)y, e1), jz = floor_div_edge((double)z, e2);
         if (jx) {
             v.ix[i] += jx;
             v.pos.x[i] = x - (R)(jx * e0);

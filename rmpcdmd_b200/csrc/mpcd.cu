@@ -284,7 +284,7 @@ __global__ void k_stream_periodic(PView<R> v, double e0, double e1, double e2, R
         R x = v.pos.x[i] + v.vel.x[i] * dt;
         R y = v.pos.y[i] + v.vel.y[i] * dt;
         R z = v.pos.z[i] + v.vel.z[i] * dt;
-        int jx = ifloor((double)x / e0), jy = ifloor((double)y / e1), jz = ifloor((double)z / e2);
+        int jx = floor_div_edge((double)x, e0), jy = floor_div_edge((double)y, e1), jz = floor_div_edge((double)z, e2);
         if (jx) v.ix[i] += jx;
         if (jy) v.iy[i] += jy;
         if (jz) v.iz[i] += jz;

@@ -3,6 +3,7 @@
 // placement and Maxwell initial velocities.
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "keys.cuh"
 #include "rng.cuh"
@@ -145,26 +146,6 @@ __global__ void k_maxwell(double *vx, double *vy, double *vz, int N, double st, 
     }
 }
 
-// Column sums in a fixed order: block b sums a fixed contiguous range
-// sequentially, then one thread adds the block partials in order.
-__global__ void k_colsum_partial(const double *a, int N, int per, double *part)
-{
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
-    long long lo = (long long)b * per;
-    double s = 0;
-    for (long long i = lo; i < lo + per && i < N; i++) s = s + a[i];
-    part[b] = s;
-}
-
-__global__ void k_colsum_final(const double *part, int nb, double *out)
-{
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double s = 0;
-        for (int b = 0; b < nb; b++) s = s + part[b];
-        *out = s;
-    }
-}
-
 template <typename R>
 __global__ void k_sub_mean(R *v, int N, const double *sum)
 {
@@ -182,14 +163,18 @@ __global__ void k_convert(const A *a, B *b, long long n)
         b[i] = (B)a[i];
 }
 
-// sum(vel, dim=2) in the reference's sequential order (initialisation only:
-// one thread walks the whole column)
-int fixed_order_sum(const double *a, int N, double *d_part, int part_cap, double *d_out)
+// sum(vel, dim=2) in the reference's sequential order.  Initialisation only:
+// the column is summed on the host, where a dependent chain of N adds runs
+// at full clock, and the result goes back to d_out.
+int fixed_order_sum(const double *a, int N, double *d_out)
 {
-    (void)part_cap;
-    k_colsum_partial<<<1, 1, 0, stream()>>>(a, N, N > 0 ? N : 1, d_part);
-    k_colsum_final<<<1, 32, 0, stream()>>>(d_part, 1, d_out);
-    RMPCD_CHECK_LAUNCH();
+    std::vector<double> h((size_t)(N > 0 ? N : 1));
+    RMPCD_CUDA_TRY(cudaMemcpyAsync(h.data(), a, sizeof(double) * (size_t)N, cudaMemcpyDeviceToHost, stream()));
+    RMPCD_CUDA_TRY(cudaStreamSynchronize(stream()));
+    double s = 0;
+    for (int i = 0; i < N; i++) s = s + h[(size_t)i];
+    RMPCD_CUDA_TRY(cudaMemcpyAsync(d_out, &s, sizeof(double), cudaMemcpyHostToDevice, stream()));
+    RMPCD_CUDA_TRY(cudaStreamSynchronize(stream()));
     return RMPCD_OK;
 }
 
@@ -221,6 +206,8 @@ static void free_particles(rmpcd_particles *p)
     cudaFree(p->d_sums);
     cudaFree(p->d_ints);
     cudaFree(p->stage);
+    cudaFree(p->rec[0]);
+    cudaFree(p->rec[1]);
     delete p;
 }
 
@@ -556,7 +543,7 @@ int rmpcd_particles_maxwell(rmpcd_particles *p, double T, uint64_t seed)
     k_maxwell<<<grid_for(p->N, 128), 128, 0, s>>>(vx, vy, vz, p->N, sqrt(T), seed);
     int rc = RMPCD_OK;
     double *comp[3] = {vx, vy, vz};
-    for (int k = 0; k < 3 && !rc; k++) rc = fixed_order_sum(comp[k], p->N, p->d_sums, p->sums_cap, sums + k);
+    for (int k = 0; k < 3 && !rc; k++) rc = fixed_order_sum(comp[k], p->N, sums + k);
     for (int k = 0; k < 3 && !rc; k++)
         k_sub_mean<double><<<grid_for(p->N, 256), 256, 0, s>>>(comp[k], p->N, sums + k);
     if (!rc) {

@@ -99,6 +99,20 @@ __host__ __device__ inline double min_image_d(double r, double L)
 // floor of a double as the Fortran default integer
 __host__ __device__ inline int ifloor(double x) { return (int)floor(x); }
 
+// floor(x / L) for an edge length L > 0 without a division when x lies in
+// [-L, 2L) (always the case for a step shorter than the box): there
+// x/L rounds into [-1, 0), [0, 1) or [1, 2) exactly as the comparisons below
+// say -- a quotient just below an integer k never rounds up to k because
+// x < kL implies x/L <= k - 2^-53 * k in double precision -- so the result
+// equals floor of the correctly rounded quotient.  Other x divide, and so do
+// negative x so small that x/L would underflow to -0.
+__host__ __device__ inline int floor_div_edge(double x, double L)
+{
+    if (x >= -L && x < 2.0 * L && !(x < 0.0 && x > -1e-290))
+        return x < 0.0 ? -1 : (x < L ? 0 : 1);
+    return (int)floor(x / L);
+}
+
 // Unsigned ordering of non-negative doubles equals their numeric ordering,
 // so atomicMax on the bit pattern gives a max-reduction of r^2 values.
 __device__ inline void atomic_max_nonneg(unsigned long long *addr, double v)

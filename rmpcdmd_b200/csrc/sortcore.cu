@@ -30,22 +30,38 @@ __global__ void k_key_count(Grid g, const R *__restrict__ x, const R *__restrict
 }
 
 // place every particle inside its cell; the order inside a cell is fixed
-// afterwards by k_segsort
+// afterwards by k_segsort.  Each warp handles kPermRounds groups of 32
+// consecutive particles and issues all their cursor atomics before using any
+// result, so the atomic round trips overlap.
+constexpr int kPermRounds = 8;
+
 __global__ void k_perm(const int *__restrict__ key, int N, int *__restrict__ cursor,
                        int *__restrict__ perm)
 {
     const int lane = threadIdx.x & 31;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long base = (long long)blockIdx.x * blockDim.x; base < N; base += stride) {
-        long long i = base + threadIdx.x;
-        bool ok = i < N;
-        int s = ok ? key[i] : -1;
-        unsigned peers = __match_any_sync(0xffffffffu, s);
-        int leader = __ffs(peers) - 1;
-        int b = 0;
-        if (ok && lane == leader) b = atomicAdd(cursor + s, __popc(peers));
-        b = __shfl_sync(peers, b, leader);
-        if (ok) perm[b + __popc(peers & lanemask_lt())] = (int)i;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const unsigned lt = lanemask_lt();
+    for (long long base = warp * 32 * kPermRounds; base < N; base += nwarps * 32 * kPermRounds) {
+        int k[kPermRounds];
+        unsigned peers[kPermRounds];
+        int b[kPermRounds];
+#pragma unroll
+        for (int r = 0; r < kPermRounds; r++) {
+            long long i = base + r * 32 + lane;
+            k[r] = i < N ? key[i] : -1;
+        }
+#pragma unroll
+        for (int r = 0; r < kPermRounds; r++) {
+            peers[r] = __match_any_sync(0xffffffffu, k[r]);
+            b[r] = 0;
+            if (k[r] >= 0 && lane == __ffs(peers[r]) - 1) b[r] = atomicAdd(cursor + k[r], __popc(peers[r]));
+        }
+#pragma unroll
+        for (int r = 0; r < kPermRounds; r++) {
+            int bb = __shfl_sync(0xffffffffu, b[r], __ffs(peers[r]) - 1);
+            if (k[r] >= 0) perm[bb + __popc(peers[r] & lt)] = (int)(base + r * 32 + lane);
+        }
     }
 }
 
@@ -132,19 +148,24 @@ __global__ void k_gather(PView<R> s, PView<R> d, const int *__restrict__ perm, i
 {
     for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < N;
          j += (long long)gridDim.x * blockDim.x) {
-        int i = perm[j];
-        d.pos.x[j] = s.pos.x[i];
-        d.pos.y[j] = s.pos.y[i];
-        d.pos.z[j] = s.pos.z[i];
-        d.vel.x[j] = s.vel.x[i];
-        d.vel.y[j] = s.vel.y[i];
-        d.vel.z[j] = s.vel.z[i];
-        d.ix[j] = s.ix[i];
-        d.iy[j] = s.iy[i];
-        d.iz[j] = s.iz[i];
-        d.id[j] = s.id[i];
-        d.species[j] = s.species[i];
-        d.flags[j] = s.flags[i];
+        const int i = perm[j];
+        // all loads first: twelve independent gathers in flight per thread
+        R px = s.pos.x[i], py = s.pos.y[i], pz = s.pos.z[i];
+        R vx = s.vel.x[i], vy = s.vel.y[i], vz = s.vel.z[i];
+        int ix = s.ix[i], iy = s.iy[i], iz = s.iz[i];
+        int id = s.id[i], sp = s.species[i], fl = s.flags[i];
+        d.pos.x[j] = px;
+        d.pos.y[j] = py;
+        d.pos.z[j] = pz;
+        d.vel.x[j] = vx;
+        d.vel.y[j] = vy;
+        d.vel.z[j] = vz;
+        d.ix[j] = ix;
+        d.iy[j] = iy;
+        d.iz[j] = iz;
+        d.id[j] = id;
+        d.species[j] = sp;
+        d.flags[j] = fl;
         if (with_force) {
             d.force.x[j] = s.force.x[i];
             d.force.y[j] = s.force.y[i];

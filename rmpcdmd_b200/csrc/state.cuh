@@ -65,6 +65,10 @@ struct rmpcd_particles {
     int *d_ints = nullptr;           // small integer scratch (64 ints)
     void *stage = nullptr;           // (3,N) layout staging for host transfers, 24 B/particle
     size_t stage_bytes = 0;
+    // packed particle records of the fused bulk schedule (double-buffered):
+    // 6 reals (pos, vel) + 6 ints (image, id, species, flags) per particle
+    unsigned char *rec[2] = {nullptr, nullptr};
+    size_t rec_bytes = 0;
     // force / force_old entries known to be exactly zero: the sort skips
     // permuting them (a permutation of zeros is zeros)
     bool force_zero = true;
