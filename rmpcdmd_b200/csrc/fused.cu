@@ -4,22 +4,24 @@
 //     simple_mpcd_step -> mpcd_stream_periodic(tau) -> random_shift -> sort
 //
 // Layout: inside the schedule each particle is one packed record
-//     6 reals  pos(3) vel(3)        then
-//     6 ints   image(3) id species flags
-// (48 B in FP32 = three 16-byte chunks, 72 B in FP64 = nine 8-byte chunks),
-// so the permutation gather moves whole records instead of twelve separate
-// 4/8-byte fields; the SoA arrays of the API are converted on entry and
-// rebuilt by the final gather.
+//   FP32 (48 B, three 16-byte chunks):
+//     [vx vy vz species] [px py pz flags] [ix iy iz id]
+//   FP64 (72 B, nine 8-byte words):
+//     vx vy vz (species,flags) px py pz (ix,iy) (iz,id)
+// The velocity part (16 / 32 B) is what the collision needs for a whole
+// cell at once; the rest is only needed particle by particle.  The SoA
+// arrays of the API are converted on entry and rebuilt by the final gather.
 //
 // Data flow of interval i (grid G_i, next grid G_{i+1}):
 //   P1  k_bulk_interval  one block per tile of consecutive Hilbert slots of
 //       G_i.  The tile's particles are a contiguous range in G_i order; the
 //       block loads the range's source indices (perm), sorts each cell's
-//       indices ascending (the reference's stable scatter order), gathers
-//       the records into shared memory with cp.async (scattered reads kept in
-//       flight without stalling), performs the SRD rotation of each cell in
-//       place, streams each particle, wraps it, keys it in G_{i+1}, counts
-//       it, and copies the tile's records out with coalesced 16/8-byte stores.
+//       indices ascending (the reference's stable scatter order), gathers the
+//       velocity parts of the records into shared memory with cp.async
+//       (scattered reads in flight without stalling the warp), performs the
+//       SRD rotation of each cell in place, then per particle gathers the
+//       rest of its record, streams and wraps it, keys it in G_{i+1}, counts
+//       it and writes the record in G_i order with coalesced stores.
 //   P2  slot scan of the G_{i+1} counts (starts and scatter cursors).
 //   P3  k_perm: perm[place] = j for every particle j of the new arrays.
 // The records written by P1 hold exactly the reference's arrays after
@@ -36,6 +38,7 @@
 #include "rng.cuh"
 #include "scan.cuh"
 #include "sortcore.cuh"
+#include "sortnet.cuh"
 #include "timers.cuh"
 
 namespace rmpcd {
@@ -43,33 +46,48 @@ namespace rmpcd {
 constexpr int kFusedThreads = 256;
 
 template <typename R>
-struct RecT {
-    static constexpr int kBytes = 6 * (int)sizeof(R) + 6 * 4;  // 48 or 72
-    static constexpr int kChunk = sizeof(R) == 4 ? 16 : 8;     // copy granule
-    static constexpr int kChunks = kBytes / kChunk;            // 3 or 9
-    static constexpr int kIntBase = 6 * (int)sizeof(R) / 4;    // first int word
+struct Rec;
+
+template <>
+struct Rec<float> {
+    static constexpr int kBytes = 48;
+    static constexpr int kVelBytes = 16;
+    __device__ static float *vel(unsigned char *r) { return (float *)r; }
+    __device__ static int &species(unsigned char *r) { return ((int *)r)[3]; }
+    __device__ static float *pos(unsigned char *r) { return (float *)r + 4; }
+    __device__ static int &flags(unsigned char *r) { return ((int *)r)[7]; }
+    __device__ static int *image(unsigned char *r) { return (int *)r + 8; }
+    __device__ static int &id(unsigned char *r) { return ((int *)r)[11]; }
 };
 
-// record field access (rec points at the first byte of one record)
-template <typename R>
-__device__ __host__ inline R *rec_real(unsigned char *rec) { return (R *)rec; }
-template <typename R>
-__device__ __host__ inline int *rec_int(unsigned char *rec) { return (int *)rec + RecT<R>::kIntBase; }
+template <>
+struct Rec<double> {
+    static constexpr int kBytes = 72;
+    static constexpr int kVelBytes = 32;
+    __device__ static double *vel(unsigned char *r) { return (double *)r; }
+    __device__ static int &species(unsigned char *r) { return ((int *)r)[6]; }
+    __device__ static double *pos(unsigned char *r) { return (double *)r + 4; }
+    __device__ static int &flags(unsigned char *r) { return ((int *)r)[7]; }
+    __device__ static int *image(unsigned char *r) { return (int *)r + 14; }
+    __device__ static int &id(unsigned char *r) { return ((int *)r)[17]; }
+};
 
-// cells per block and staged-particle capacity; the capacity is ~7 standard
-// deviations above the mean occupancy of a tile at density 10, and an
-// over-full tile takes the global-memory path
+// cells per block, staged-particle capacity and resident blocks per SM; the
+// capacity is > 7 standard deviations above the mean tile occupancy at
+// density 10 and an over-full tile takes the global-memory path
 template <typename R>
 struct FusedCfg;
 template <>
 struct FusedCfg<float> {
     static constexpr int kSlots = 128;
     static constexpr int kCap = 1792;
+    static constexpr int kMinBlocks = 4;
 };
 template <>
 struct FusedCfg<double> {
     static constexpr int kSlots = 96;
     static constexpr int kCap = 1408;
+    static constexpr int kMinBlocks = 4;
 };
 
 template <typename R>
@@ -91,30 +109,51 @@ struct FusedArgs {
     const double *axes;
 };
 
-__device__ inline void sort_small(int *a, int n)
-{
-    for (int i = 1; i < n; i++) {
-        int v = a[i];
-        int j = i - 1;
-        while (j >= 0 && a[j] > v) {
-            a[j + 1] = a[j];
-            j--;
-        }
-        a[j + 1] = v;
-    }
-}
-
-// SRD of one cell of n consecutive records (src/mpcd.f90:127-178)
+// SRD of one cell of n consecutive velocity parts (src/mpcd.f90:127-178);
+// stride is the distance between consecutive particles in bytes
 template <typename R>
-__device__ inline void srd_cell(unsigned char *rec0, int n, int slot, const FusedArgs<R> &A)
+__device__ inline void srd_cell(unsigned char *v0, int stride, int n, int slot, const FusedArgs<R> &A)
 {
-    constexpr int B = RecT<R>::kBytes;
+    if constexpr (sizeof(R) == 4) {
+        if (stride == 16) {
+            // one 16-byte shared-memory access per particle and pass
+            int n_eff = 0;
+            CellSum<float> sx, sy, sz;
+            for (int k = 0; k < n; k++) {
+                int4 c = ((const int4 *)v0)[k];
+                if (c.w > 0) {
+                    sx.add(__int_as_float(c.x));
+                    sy.add(__int_as_float(c.y));
+                    sz.add(__int_as_float(c.z));
+                    n_eff++;
+                }
+            }
+            if (n_eff <= 1) return;
+            float lv[3] = {sx.value() / n_eff, sy.value() / n_eff, sz.value() / n_eff};
+            double n0, n1, n2;
+            if (A.axes) {
+                n0 = A.axes[3 * (size_t)slot];
+                n1 = A.axes[3 * (size_t)slot + 1];
+                n2 = A.axes[3 * (size_t)slot + 2];
+            } else {
+                rng::sphere(A.seed, A.step, (uint32_t)slot, n0, n1, n2);
+            }
+            Rot o = srd_matrix(n0, n1, n2, A.sin_a, A.cos_a);
+            for (int k = 0; k < n; k++) {
+                int4 c = ((const int4 *)v0)[k];
+                float x = __int_as_float(c.x), y = __int_as_float(c.y), z = __int_as_float(c.z);
+                srd_rotate(x, y, z, lv, o);
+                ((int4 *)v0)[k] = make_int4(__float_as_int(x), __float_as_int(y), __float_as_int(z), c.w);
+            }
+            return;
+        }
+    }
     int n_eff = 0;
     CellSum<R> sx, sy, sz;
     for (int k = 0; k < n; k++) {
-        unsigned char *r = rec0 + (size_t)k * B;
-        if (rec_int<R>(r)[4] > 0) {
-            R *v = rec_real<R>(r) + 3;
+        unsigned char *r = v0 + (size_t)k * stride;
+        if (Rec<R>::species(r) > 0) {
+            R *v = Rec<R>::vel(r);
             sx.add(v[0]);
             sy.add(v[1]);
             sz.add(v[2]);
@@ -133,7 +172,7 @@ __device__ inline void srd_cell(unsigned char *rec0, int n, int slot, const Fuse
     }
     Rot o = srd_matrix(n0, n1, n2, A.sin_a, A.cos_a);
     for (int k = 0; k < n; k++) {
-        R *v = rec_real<R>(rec0 + (size_t)k * B) + 3;
+        R *v = Rec<R>::vel(v0 + (size_t)k * stride);
         R x = v[0], y = v[1], z = v[2];
         srd_rotate(x, y, z, lv, o);
         v[0] = x;
@@ -142,8 +181,8 @@ __device__ inline void srd_cell(unsigned char *rec0, int n, int slot, const Fuse
     }
 }
 
-// stream the particle of record r in place (mpcd_stream_periodic) and
-// return its slot in G_{i+1}
+// mpcd_stream_periodic of one particle (src/mpcd.f90:450-455); returns its
+// slot in G_{i+1}
 template <typename R>
 __device__ inline int stream_values(const FusedArgs<R> &A, R &x, R &y, R &z, R vx, R vy, R vz, int &ix, int &iy,
                                     int &iz)
@@ -163,61 +202,61 @@ __device__ inline int stream_values(const FusedArgs<R> &A, R &x, R &y, R &z, R v
 }
 
 template <typename R>
-__device__ inline int stream_rec(const FusedArgs<R> &A, unsigned char *r)
-{
-    if constexpr (sizeof(R) == 4) {
-        // three 16-byte shared-memory accesses per record (bank-conflict free)
-        int4 *q = (int4 *)r;
-        int4 a = q[0], b = q[1], c = q[2];
-        float x = __int_as_float(a.x), y = __int_as_float(a.y), z = __int_as_float(a.z);
-        float vx = __int_as_float(a.w), vy = __int_as_float(b.x), vz = __int_as_float(b.y);
-        int ix = b.z, iy = b.w, iz = c.x;
-        int key = stream_values<R>(A, x, y, z, vx, vy, vz, ix, iy, iz);
-        q[0] = make_int4(__float_as_int(x), __float_as_int(y), __float_as_int(z), a.w);
-        q[1] = make_int4(b.x, b.y, ix, iy);
-        c.x = iz;
-        q[2] = c;
-        return key;
-    } else {
-        R *f = rec_real<R>(r);
-        int *w = rec_int<R>(r);
-        R x = f[0], y = f[1], z = f[2];
-        int ix = w[0], iy = w[1], iz = w[2];
-        int key = stream_values<R>(A, x, y, z, f[3], f[4], f[5], ix, iy, iz);
-        f[0] = x;
-        f[1] = y;
-        f[2] = z;
-        w[0] = ix;
-        w[1] = iy;
-        w[2] = iz;
-        return key;
-    }
-}
-
-template <typename R>
 constexpr size_t fused_smem()
 {
-    return (size_t)FusedCfg<R>::kCap * (RecT<R>::kBytes + sizeof(int));
+    return (size_t)FusedCfg<R>::kCap * (Rec<R>::kVelBytes + sizeof(int));
 }
 
+// the non-velocity part of a record, as loaded from global memory
 template <typename R>
-__device__ inline void copy_chunk(unsigned char *dst, const unsigned char *src)
+struct Rest;
+template <>
+struct Rest<float> {
+    int4 a, b;  // [px py pz flags] [ix iy iz id]
+};
+template <>
+struct Rest<double> {
+    long long w[5];  // px py pz (ix,iy) (iz,id)
+};
+
+__device__ inline void load_rest(Rest<float> &r, const unsigned char *rec)
 {
-    if (RecT<R>::kChunk == 16) *(int4 *)dst = *(const int4 *)src;
-    else *(long long *)dst = *(const long long *)src;
+    const int4 *q = (const int4 *)rec;
+    r.a = __ldcs(q + 1);
+    r.b = __ldcs(q + 2);
+}
+__device__ inline void load_rest(Rest<double> &r, const unsigned char *rec)
+{
+    const long long *q = (const long long *)rec;
+#pragma unroll
+    for (int k = 0; k < 5; k++) r.w[k] = __ldcs(q + 4 + k);
+}
+
+// stream particle j (velocity part in shared memory at sv, the rest in r)
+// and write its record; returns the G_{i+1} slot
+__device__ inline int finish_particle(const FusedArgs<float> &A, const unsigned char *sv, const Rest<float> &r,
+                                      int4 &c0, int4 &c1, int4 &c2)
+{
+    c0 = *(const int4 *)sv;
+    float x = __int_as_float(r.a.x), y = __int_as_float(r.a.y), z = __int_as_float(r.a.z);
+    int ix = r.b.x, iy = r.b.y, iz = r.b.z;
+    int key = stream_values<float>(A, x, y, z, __int_as_float(c0.x), __int_as_float(c0.y), __int_as_float(c0.z),
+                                   ix, iy, iz);
+    c1 = make_int4(__float_as_int(x), __float_as_int(y), __float_as_int(z), r.a.w);
+    c2 = make_int4(ix, iy, iz, r.b.w);
+    return key;
 }
 
 template <typename R>
-__global__ void __launch_bounds__(kFusedThreads) k_bulk_interval(FusedArgs<R> A)
+__global__ void __launch_bounds__(kFusedThreads, FusedCfg<R>::kMinBlocks) k_bulk_interval(FusedArgs<R> A)
 {
     constexpr int SL = FusedCfg<R>::kSlots;
     constexpr int CAP = FusedCfg<R>::kCap;
-    constexpr int B = RecT<R>::kBytes;
-    constexpr int CH = RecT<R>::kChunk;
-    constexpr int NCH = RecT<R>::kChunks;
+    constexpr int B = Rec<R>::kBytes;
+    constexpr int VB = Rec<R>::kVelBytes;
     extern __shared__ __align__(16) unsigned char smem[];
-    unsigned char *s_rec = smem;
-    int *s_perm = (int *)(smem + (size_t)CAP * B);
+    unsigned char *s_vel = smem;
+    int *s_perm = (int *)(smem + (size_t)CAP * VB);
 
     const int t = threadIdx.x;
     const int lane = t & 31;
@@ -235,39 +274,77 @@ __global__ void __launch_bounds__(kFusedThreads) k_bulk_interval(FusedArgs<R> A)
     if (np <= CAP) {
         // ---- staged path ----
         if (A.perm) {
-            for (int j = t; j < np; j += kFusedThreads) s_perm[j] = A.perm[a0 + j];
+            for (int j = t; j < np; j += kFusedThreads) s_perm[j] = __ldcs(A.perm + a0 + j);
         } else {
             for (int j = t; j < np; j += kFusedThreads) s_perm[j] = a0 + j;
         }
         __syncthreads();
-        if (A.perm && my_n > 1) sort_small(s_perm + (my_a - a0), my_n);
+        if (A.perm && my_n > 1) sort_segment(s_perm + (my_a - a0), my_n);
         __syncthreads();
-        // gather: consecutive threads fetch consecutive chunks of one record
-        for (int q = t; q < np * NCH; q += kFusedThreads) {
-            int j = q / NCH, c = q - j * NCH;
-            const unsigned char *src = A.in + (size_t)s_perm[j] * B + c * CH;
-            if (CH == 16) cp_async16(s_rec + (size_t)j * B + c * CH, src);
-            else cp_async8(s_rec + (size_t)j * B + c * CH, src);
+        // gather the velocity parts (16 B per particle in FP32, 4 x 8 B in FP64)
+        if constexpr (VB == 16) {
+            for (int j = t; j < np; j += kFusedThreads)
+                cp_async16(s_vel + (size_t)j * VB, A.in + (size_t)s_perm[j] * B);
+        } else {
+            for (int q = t; q < np * 4; q += kFusedThreads) {
+                int j = q >> 2, c = q & 3;
+                cp_async8(s_vel + (size_t)j * VB + 8 * c, A.in + (size_t)s_perm[j] * B + 8 * c);
+            }
         }
         cp_async_wait_all();
         __syncthreads();
-        if (my_n > 1) srd_cell<R>(s_rec + (size_t)(my_a - a0) * B, my_n, slot, A);
+        if (my_n > 1) srd_cell<R>(s_vel + (size_t)(my_a - a0) * VB, VB, my_n, slot, A);
         __syncthreads();
+        // stream, key, count and write every particle; the rest of the next
+        // record is fetched while the current one is processed
+        int j = t;
+        Rest<R> cur;
+        if (j < np) load_rest(cur, A.in + (size_t)s_perm[j] * B);
         for (int jb = 0; jb < np; jb += kFusedThreads) {
-            int j = jb + t;
             bool ok = j < np;
+            Rest<R> nxt;
+            int jn = j + kFusedThreads;
+            if (jn < np) load_rest(nxt, A.in + (size_t)s_perm[jn] * B);
             int key = -1;
-            if (ok) {
-                key = stream_rec<R>(A, s_rec + (size_t)j * B);
-                A.key_out[a0 + j] = key;
+            if constexpr (sizeof(R) == 4) {
+                if (ok) {
+                    int4 c0, c1, c2;
+                    key = finish_particle(A, s_vel + (size_t)j * VB, cur, c0, c1, c2);
+                    // three 16-byte stores per record; the L2 merges the
+                    // interleaved chunks of neighbouring lanes into full sectors
+                    int4 *o = (int4 *)(A.out + (size_t)(a0 + j) * B);
+                    __stcs(o, c0);
+                    __stcs(o + 1, c1);
+                    __stcs(o + 2, c2);
+                }
+            } else {
+                if (ok) {
+                    unsigned char *o = A.out + (size_t)(a0 + j) * B;
+                    const double *sv = (const double *)(s_vel + (size_t)j * VB);
+                    double x = __longlong_as_double(cur.w[0]), y = __longlong_as_double(cur.w[1]),
+                           z = __longlong_as_double(cur.w[2]);
+                    int ix = (int)(cur.w[3] & 0xffffffffll), iy = (int)(cur.w[3] >> 32);
+                    int iz = (int)(cur.w[4] & 0xffffffffll);
+                    key = stream_values<double>(A, x, y, z, sv[0], sv[1], sv[2], ix, iy, iz);
+                    long long *ow = (long long *)o;
+                    const long long *sw = (const long long *)sv;
+                    ow[0] = sw[0];
+                    ow[1] = sw[1];
+                    ow[2] = sw[2];
+                    ow[3] = sw[3];
+                    ow[4] = __double_as_longlong(x);
+                    ow[5] = __double_as_longlong(y);
+                    ow[6] = __double_as_longlong(z);
+                    ow[7] = ((long long)(unsigned)iy << 32) | (unsigned)ix;
+                    ow[8] = (cur.w[4] & (long long)0xffffffff00000000ull) | (unsigned)iz;
+                }
             }
+            if (ok) A.key_out[a0 + j] = key;
             unsigned peers = __match_any_sync(0xffffffffu, key);
             if (ok && lane == __ffs(peers) - 1) atomicAdd(A.count_next + key, __popc(peers));
+            cur = nxt;
+            j = jn;
         }
-        __syncthreads();
-        // coalesced copy-out of the tile
-        unsigned char *dst = A.out + (size_t)a0 * B;
-        for (int q = t; q < np * NCH; q += kFusedThreads) copy_chunk<R>(dst + (size_t)q * CH, s_rec + (size_t)q * CH);
     } else {
         // ---- over-full tile (dense cells): the same steps in global memory ----
         if (A.perm && my_n > 1) sort_small(A.perm + my_a, my_n);
@@ -275,10 +352,11 @@ __global__ void __launch_bounds__(kFusedThreads) k_bulk_interval(FusedArgs<R> A)
         if (my_n > 0) {
             for (int k = 0; k < my_n; k++) {
                 int src = A.perm ? A.perm[my_a + k] : my_a + k;
-                for (int c = 0; c < NCH; c++)
-                    copy_chunk<R>(A.out + (size_t)(my_a + k) * B + c * CH, A.in + (size_t)src * B + c * CH);
+                const long long *s = (const long long *)(A.in + (size_t)src * B);
+                long long *d = (long long *)(A.out + (size_t)(my_a + k) * B);
+                for (int w = 0; w < B / 8; w++) d[w] = s[w];
             }
-            if (my_n > 1) srd_cell<R>(A.out + (size_t)my_a * B, my_n, slot, A);
+            if (my_n > 1) srd_cell<R>(A.out + (size_t)my_a * B, B, my_n, slot, A);
         }
         __syncthreads();
         for (int jb = 0; jb < np; jb += kFusedThreads) {
@@ -286,7 +364,18 @@ __global__ void __launch_bounds__(kFusedThreads) k_bulk_interval(FusedArgs<R> A)
             bool ok = jb + t < np;
             int key = -1;
             if (ok) {
-                key = stream_rec<R>(A, A.out + (size_t)j * B);
+                unsigned char *r = A.out + (size_t)j * B;
+                R *p = Rec<R>::pos(r), *v = Rec<R>::vel(r);
+                int *im = Rec<R>::image(r);
+                R x = p[0], y = p[1], z = p[2];
+                int ix = im[0], iy = im[1], iz = im[2];
+                key = stream_values<R>(A, x, y, z, v[0], v[1], v[2], ix, iy, iz);
+                p[0] = x;
+                p[1] = y;
+                p[2] = z;
+                im[0] = ix;
+                im[1] = iy;
+                im[2] = iz;
                 A.key_out[j] = key;
             }
             unsigned peers = __match_any_sync(0xffffffffu, key);
@@ -295,43 +384,62 @@ __global__ void __launch_bounds__(kFusedThreads) k_bulk_interval(FusedArgs<R> A)
     }
 }
 
-// SoA (API layout) -> records, in place order
+// SoA (API layout) -> records, in place order.  Each block assembles 256
+// records in shared memory and writes them out as one contiguous range of
+// 8-byte words (coalesced).
+constexpr int kPackThreads = 256;
+
 template <typename R>
-__global__ void k_soa_to_rec(PView<R> v, unsigned char *rec, int N)
+__global__ void __launch_bounds__(kPackThreads) k_soa_to_rec(PView<R> v, unsigned char *rec, int N)
 {
-    constexpr int B = RecT<R>::kBytes;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
-         i += (long long)gridDim.x * blockDim.x) {
-        unsigned char *r = rec + (size_t)i * B;
-        R *f = rec_real<R>(r);
-        int *w = rec_int<R>(r);
-        f[0] = v.pos.x[i];
-        f[1] = v.pos.y[i];
-        f[2] = v.pos.z[i];
-        f[3] = v.vel.x[i];
-        f[4] = v.vel.y[i];
-        f[5] = v.vel.z[i];
-        w[0] = v.ix[i];
-        w[1] = v.iy[i];
-        w[2] = v.iz[i];
-        w[3] = v.id[i];
-        w[4] = v.species[i];
-        w[5] = v.flags[i];
+    constexpr int B = Rec<R>::kBytes;
+    __shared__ __align__(16) unsigned char s[kPackThreads * B];
+    for (long long base = (long long)blockIdx.x * kPackThreads; base < N; base += (long long)gridDim.x * kPackThreads) {
+        const long long i = base + threadIdx.x;
+        if (i < N) {
+            unsigned char *r = s + (size_t)threadIdx.x * B;
+            R *p = Rec<R>::pos(r), *w = Rec<R>::vel(r);
+            int *im = Rec<R>::image(r);
+            p[0] = v.pos.x[i];
+            p[1] = v.pos.y[i];
+            p[2] = v.pos.z[i];
+            w[0] = v.vel.x[i];
+            w[1] = v.vel.y[i];
+            w[2] = v.vel.z[i];
+            im[0] = v.ix[i];
+            im[1] = v.iy[i];
+            im[2] = v.iz[i];
+            Rec<R>::id(r) = v.id[i];
+            Rec<R>::species(r) = v.species[i];
+            Rec<R>::flags(r) = v.flags[i];
+        }
+        __syncthreads();
+        const int n = (int)min((long long)kPackThreads, N - base);
+        long long *dst = (long long *)(rec + (size_t)base * B);
+        const long long *src = (const long long *)s;
+        for (int q = threadIdx.x; q < n * (B / 8); q += kPackThreads) dst[q] = src[q];
+        __syncthreads();
     }
 }
 
-// final gather: records through perm -> SoA (API layout)
+// final gather: records through perm -> SoA (API layout); each record is
+// read with 8-byte loads
 template <typename R>
 __global__ void k_rec_gather_to_soa(const unsigned char *rec, const int *perm, PView<R> d, int N)
 {
-    constexpr int B = RecT<R>::kBytes;
+    constexpr int B = Rec<R>::kBytes;
     for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < N;
          j += (long long)gridDim.x * blockDim.x) {
-        const unsigned char *r = rec + (size_t)perm[j] * B;
-        const R *f = (const R *)r;
-        const int *w = (const int *)r + RecT<R>::kIntBase;
-        R px = f[0], py = f[1], pz = f[2], vx = f[3], vy = f[4], vz = f[5];
-        int ix = w[0], iy = w[1], iz = w[2], id = w[3], sp = w[4], fl = w[5];
+        long long w8[B / 8];
+        const long long *src = (const long long *)(rec + (size_t)perm[j] * B);
+#pragma unroll
+        for (int k = 0; k < B / 8; k++) w8[k] = __ldcs(src + k);
+        unsigned char *r = (unsigned char *)w8;
+        const R *p = Rec<R>::pos(r), *w = Rec<R>::vel(r);
+        const int *im = Rec<R>::image(r);
+        R px = p[0], py = p[1], pz = p[2], vx = w[0], vy = w[1], vz = w[2];
+        int ix = im[0], iy = im[1], iz = im[2], id = Rec<R>::id(r), sp = Rec<R>::species(r),
+            fl = Rec<R>::flags(r);
         d.pos.x[j] = px;
         d.pos.y[j] = py;
         d.pos.z[j] = pz;
@@ -350,7 +458,7 @@ __global__ void k_rec_gather_to_soa(const unsigned char *rec, const int *perm, P
 template <typename R>
 static int ensure_records(rmpcd_particles *p)
 {
-    size_t need = (size_t)p->N * RecT<R>::kBytes + 64;
+    size_t need = (size_t)p->N * Rec<R>::kBytes + 64;
     if (p->rec_bytes >= need && p->rec[0] && p->rec[1]) return RMPCD_OK;
     cudaStreamSynchronize(stream());
     cudaFree(p->rec[0]);

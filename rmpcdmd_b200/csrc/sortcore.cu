@@ -1,6 +1,7 @@
 #include "keys.cuh"
 #include "scan.cuh"
 #include "sortcore.cuh"
+#include "sortnet.cuh"
 #include "timers.cuh"
 
 namespace rmpcd {
@@ -78,16 +79,7 @@ __global__ void k_segsort_small(const int *__restrict__ start, const int *__rest
             big[q] = s;
             continue;
         }
-        int *a = perm + start[s];
-        for (int i = 1; i < n; i++) {
-            int v = a[i];
-            int j = i - 1;
-            while (j >= 0 && a[j] > v) {
-                a[j + 1] = a[j];
-                j--;
-            }
-            a[j + 1] = v;
-        }
+        sort_segment(perm + start[s], n);
     }
 }
 
