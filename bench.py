@@ -40,7 +40,7 @@ SEED = 20241203
 # HBM bytes the fused interval kernel must move per particle and per slot
 # (read + write of the full particle record, the permutation index and the
 # next key; see the traffic table in DESIGN.md)
-BYTES_PER_PARTICLE = {32: 104, 64: 152}
+BYTES_PER_PARTICLE = {32: 72, 64: 120}
 BYTES_PER_SLOT = 12
 
 

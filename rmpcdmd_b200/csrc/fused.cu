@@ -3,14 +3,16 @@
 //
 //     simple_mpcd_step -> mpcd_stream_periodic(tau) -> random_shift -> sort
 //
-// Layout: inside the schedule each particle is one packed record
-//   FP32 (48 B, three 16-byte chunks):
-//     [vx vy vz species] [px py pz flags] [ix iy iz id]
-//   FP64 (72 B, nine 8-byte words):
-//     vx vy vz (species,flags) px py pz (ix,iy) (iz,id)
-// The velocity part (16 / 32 B) is what the collision needs for a whole
-// cell at once; the rest is only needed particle by particle.  The SoA
-// arrays of the API are converted on entry and rebuilt by the final gather.
+// Layout: inside the schedule each particle is one packed record holding what
+// changes or is needed every interval,
+//   FP32 (32 B, two 16-byte chunks):  [vx vy vz species] [px py pz idx]
+//   FP64 (56 B, seven 8-byte words):  vx vy vz (species,idx) px py pz
+// where idx is the particle's position when the schedule started.  image,
+// flags and id do not move: they stay in the API arrays at idx (image is
+// updated there, in place, only for the few particles that wrap in an
+// interval) and are gathered into sorted order once, at the end.  The velocity
+// part (16 / 32 B) is what the collision needs for a whole cell at once; the
+// rest is needed particle by particle.
 //
 // Data flow of interval i (grid G_i, next grid G_{i+1}):
 //   P1  k_bulk_interval  one block per tile of consecutive Hilbert slots of
@@ -29,7 +31,8 @@
 // completed by the gather of the next P1 (or by the final gather).
 //
 // HBM traffic of P1 per particle: perm 4 + record read + record write +
-// key 4 (104 B in FP32, 152 B in FP64), plus 12 B per slot.
+// key 4 (72 B in FP32, 120 B in FP64), plus 12 B per slot, plus a 12-byte
+// image update for each particle that wraps.
 #include <cmath>
 
 #include "async_copy.cuh"
@@ -50,26 +53,22 @@ struct Rec;
 
 template <>
 struct Rec<float> {
-    static constexpr int kBytes = 48;
+    static constexpr int kBytes = 32;
     static constexpr int kVelBytes = 16;
     __device__ static float *vel(unsigned char *r) { return (float *)r; }
     __device__ static int &species(unsigned char *r) { return ((int *)r)[3]; }
     __device__ static float *pos(unsigned char *r) { return (float *)r + 4; }
-    __device__ static int &flags(unsigned char *r) { return ((int *)r)[7]; }
-    __device__ static int *image(unsigned char *r) { return (int *)r + 8; }
-    __device__ static int &id(unsigned char *r) { return ((int *)r)[11]; }
+    __device__ static int &idx(unsigned char *r) { return ((int *)r)[7]; }
 };
 
 template <>
 struct Rec<double> {
-    static constexpr int kBytes = 72;
+    static constexpr int kBytes = 56;
     static constexpr int kVelBytes = 32;
     __device__ static double *vel(unsigned char *r) { return (double *)r; }
     __device__ static int &species(unsigned char *r) { return ((int *)r)[6]; }
+    __device__ static int &idx(unsigned char *r) { return ((int *)r)[7]; }
     __device__ static double *pos(unsigned char *r) { return (double *)r + 4; }
-    __device__ static int &flags(unsigned char *r) { return ((int *)r)[7]; }
-    __device__ static int *image(unsigned char *r) { return (int *)r + 14; }
-    __device__ static int &id(unsigned char *r) { return ((int *)r)[17]; }
 };
 
 // cells per block, staged-particle capacity and resident blocks per SM; the
@@ -101,6 +100,7 @@ struct FusedArgs {
     int N;
     int *count_next;          // G_{i+1} histogram (accumulated)
     int *key_out;             // G_{i+1} slot of out[j]
+    int *ix, *iy, *iz;        // image, indexed by idx (updated in place on a wrap)
     Grid g_next;
     double e0, e1, e2;        // edges
     R dt;
@@ -182,22 +182,27 @@ __device__ inline void srd_cell(unsigned char *v0, int stride, int n, int slot, 
 }
 
 // mpcd_stream_periodic of one particle (src/mpcd.f90:450-455); returns its
-// slot in G_{i+1}
+// slot in G_{i+1}; a wrap updates the particle's image at its idx
 template <typename R>
-__device__ inline int stream_values(const FusedArgs<R> &A, R &x, R &y, R &z, R vx, R vy, R vz, int &ix, int &iy,
-                                    int &iz)
+__device__ inline int stream_values(const FusedArgs<R> &A, R &x, R &y, R &z, R vx, R vy, R vz, int idx)
 {
     x = x + vx * A.dt;
     y = y + vy * A.dt;
     z = z + vz * A.dt;
     int jx = floor_div_edge((double)x, A.e0), jy = floor_div_edge((double)y, A.e1),
         jz = floor_div_edge((double)z, A.e2);
-    if (jx) x = x - (R)(jx * A.e0);
-    if (jy) y = y - (R)(jy * A.e1);
-    if (jz) z = z - (R)(jz * A.e2);
-    ix += jx;
-    iy += jy;
-    iz += jz;
+    if (jx) {
+        x = x - (R)(jx * A.e0);
+        A.ix[idx] += jx;
+    }
+    if (jy) {
+        y = y - (R)(jy * A.e1);
+        A.iy[idx] += jy;
+    }
+    if (jz) {
+        z = z - (R)(jz * A.e2);
+        A.iz[idx] += jz;
+    }
     return slot_of(A.g_next, (double)x, (double)y, (double)z);
 }
 
@@ -212,38 +217,55 @@ template <typename R>
 struct Rest;
 template <>
 struct Rest<float> {
-    int4 a, b;  // [px py pz flags] [ix iy iz id]
+    int4 a;  // [px py pz idx]
 };
 template <>
 struct Rest<double> {
-    long long w[5];  // px py pz (ix,iy) (iz,id)
+    long long w[3];  // px py pz
 };
 
 __device__ inline void load_rest(Rest<float> &r, const unsigned char *rec)
 {
-    const int4 *q = (const int4 *)rec;
-    r.a = __ldcs(q + 1);
-    r.b = __ldcs(q + 2);
+    r.a = __ldcs((const int4 *)rec + 1);
 }
 __device__ inline void load_rest(Rest<double> &r, const unsigned char *rec)
 {
     const long long *q = (const long long *)rec;
 #pragma unroll
-    for (int k = 0; k < 5; k++) r.w[k] = __ldcs(q + 4 + k);
+    for (int k = 0; k < 3; k++) r.w[k] = __ldcs(q + 4 + k);
 }
 
-// stream particle j (velocity part in shared memory at sv, the rest in r)
-// and write its record; returns the G_{i+1} slot
+// stream particle j (velocity part in shared memory at sv, the rest in r),
+// write its record at o and return its G_{i+1} slot
 __device__ inline int finish_particle(const FusedArgs<float> &A, const unsigned char *sv, const Rest<float> &r,
-                                      int4 &c0, int4 &c1, int4 &c2)
+                                      unsigned char *o)
 {
-    c0 = *(const int4 *)sv;
+    int4 c0 = *(const int4 *)sv;
     float x = __int_as_float(r.a.x), y = __int_as_float(r.a.y), z = __int_as_float(r.a.z);
-    int ix = r.b.x, iy = r.b.y, iz = r.b.z;
     int key = stream_values<float>(A, x, y, z, __int_as_float(c0.x), __int_as_float(c0.y), __int_as_float(c0.z),
-                                   ix, iy, iz);
-    c1 = make_int4(__float_as_int(x), __float_as_int(y), __float_as_int(z), r.a.w);
-    c2 = make_int4(ix, iy, iz, r.b.w);
+                                   r.a.w);
+    int4 *q = (int4 *)o;
+    __stcs(q, c0);
+    __stcs(q + 1, make_int4(__float_as_int(x), __float_as_int(y), __float_as_int(z), r.a.w));
+    return key;
+}
+
+__device__ inline int finish_particle(const FusedArgs<double> &A, const unsigned char *sv, const Rest<double> &r,
+                                      unsigned char *o)
+{
+    const long long *sw = (const long long *)sv;
+    const double *v = (const double *)sv;
+    double x = __longlong_as_double(r.w[0]), y = __longlong_as_double(r.w[1]), z = __longlong_as_double(r.w[2]);
+    int idx = ((const int *)sv)[7];
+    int key = stream_values<double>(A, x, y, z, v[0], v[1], v[2], idx);
+    long long *ow = (long long *)o;
+    __stcs(ow, sw[0]);
+    __stcs(ow + 1, sw[1]);
+    __stcs(ow + 2, sw[2]);
+    __stcs(ow + 3, sw[3]);
+    __stcs(ow + 4, __double_as_longlong(x));
+    __stcs(ow + 5, __double_as_longlong(y));
+    __stcs(ow + 6, __double_as_longlong(z));
     return key;
 }
 
@@ -306,40 +328,10 @@ __global__ void __launch_bounds__(kFusedThreads, FusedCfg<R>::kMinBlocks) k_bulk
             int jn = j + kFusedThreads;
             if (jn < np) load_rest(nxt, A.in + (size_t)s_perm[jn] * B);
             int key = -1;
-            if constexpr (sizeof(R) == 4) {
-                if (ok) {
-                    int4 c0, c1, c2;
-                    key = finish_particle(A, s_vel + (size_t)j * VB, cur, c0, c1, c2);
-                    // three 16-byte stores per record; the L2 merges the
-                    // interleaved chunks of neighbouring lanes into full sectors
-                    int4 *o = (int4 *)(A.out + (size_t)(a0 + j) * B);
-                    __stcs(o, c0);
-                    __stcs(o + 1, c1);
-                    __stcs(o + 2, c2);
-                }
-            } else {
-                if (ok) {
-                    unsigned char *o = A.out + (size_t)(a0 + j) * B;
-                    const double *sv = (const double *)(s_vel + (size_t)j * VB);
-                    double x = __longlong_as_double(cur.w[0]), y = __longlong_as_double(cur.w[1]),
-                           z = __longlong_as_double(cur.w[2]);
-                    int ix = (int)(cur.w[3] & 0xffffffffll), iy = (int)(cur.w[3] >> 32);
-                    int iz = (int)(cur.w[4] & 0xffffffffll);
-                    key = stream_values<double>(A, x, y, z, sv[0], sv[1], sv[2], ix, iy, iz);
-                    long long *ow = (long long *)o;
-                    const long long *sw = (const long long *)sv;
-                    ow[0] = sw[0];
-                    ow[1] = sw[1];
-                    ow[2] = sw[2];
-                    ow[3] = sw[3];
-                    ow[4] = __double_as_longlong(x);
-                    ow[5] = __double_as_longlong(y);
-                    ow[6] = __double_as_longlong(z);
-                    ow[7] = ((long long)(unsigned)iy << 32) | (unsigned)ix;
-                    ow[8] = (cur.w[4] & (long long)0xffffffff00000000ull) | (unsigned)iz;
-                }
+            if (ok) {
+                key = finish_particle(A, s_vel + (size_t)j * VB, cur, A.out + (size_t)(a0 + j) * B);
+                A.key_out[a0 + j] = key;
             }
-            if (ok) A.key_out[a0 + j] = key;
             unsigned peers = __match_any_sync(0xffffffffu, key);
             if (ok && lane == __ffs(peers) - 1) atomicAdd(A.count_next + key, __popc(peers));
             cur = nxt;
@@ -366,16 +358,11 @@ __global__ void __launch_bounds__(kFusedThreads, FusedCfg<R>::kMinBlocks) k_bulk
             if (ok) {
                 unsigned char *r = A.out + (size_t)j * B;
                 R *p = Rec<R>::pos(r), *v = Rec<R>::vel(r);
-                int *im = Rec<R>::image(r);
                 R x = p[0], y = p[1], z = p[2];
-                int ix = im[0], iy = im[1], iz = im[2];
-                key = stream_values<R>(A, x, y, z, v[0], v[1], v[2], ix, iy, iz);
+                key = stream_values<R>(A, x, y, z, v[0], v[1], v[2], Rec<R>::idx(r));
                 p[0] = x;
                 p[1] = y;
                 p[2] = z;
-                im[0] = ix;
-                im[1] = iy;
-                im[2] = iz;
                 A.key_out[j] = key;
             }
             unsigned peers = __match_any_sync(0xffffffffu, key);
@@ -384,7 +371,7 @@ __global__ void __launch_bounds__(kFusedThreads, FusedCfg<R>::kMinBlocks) k_bulk
     }
 }
 
-// SoA (API layout) -> records, in place order.  Each block assembles 256
+// SoA (API layout) -> records with idx = position.  Each block assembles 256
 // records in shared memory and writes them out as one contiguous range of
 // 8-byte words (coalesced).
 constexpr int kPackThreads = 256;
@@ -399,19 +386,14 @@ __global__ void __launch_bounds__(kPackThreads) k_soa_to_rec(PView<R> v, unsigne
         if (i < N) {
             unsigned char *r = s + (size_t)threadIdx.x * B;
             R *p = Rec<R>::pos(r), *w = Rec<R>::vel(r);
-            int *im = Rec<R>::image(r);
             p[0] = v.pos.x[i];
             p[1] = v.pos.y[i];
             p[2] = v.pos.z[i];
             w[0] = v.vel.x[i];
             w[1] = v.vel.y[i];
             w[2] = v.vel.z[i];
-            im[0] = v.ix[i];
-            im[1] = v.iy[i];
-            im[2] = v.iz[i];
-            Rec<R>::id(r) = v.id[i];
             Rec<R>::species(r) = v.species[i];
-            Rec<R>::flags(r) = v.flags[i];
+            Rec<R>::idx(r) = (int)i;
         }
         __syncthreads();
         const int n = (int)min((long long)kPackThreads, N - base);
@@ -422,10 +404,10 @@ __global__ void __launch_bounds__(kPackThreads) k_soa_to_rec(PView<R> v, unsigne
     }
 }
 
-// final gather: records through perm -> SoA (API layout); each record is
-// read with 8-byte loads
+// final gather into the API arrays: pos, vel, species from the records
+// through perm; image, flags and id from the position-at-start idx
 template <typename R>
-__global__ void k_rec_gather_to_soa(const unsigned char *rec, const int *perm, PView<R> d, int N)
+__global__ void k_rec_gather_to_soa(const unsigned char *rec, const int *perm, PView<R> side, PView<R> d, int N)
 {
     constexpr int B = Rec<R>::kBytes;
     for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < N;
@@ -436,22 +418,20 @@ __global__ void k_rec_gather_to_soa(const unsigned char *rec, const int *perm, P
         for (int k = 0; k < B / 8; k++) w8[k] = __ldcs(src + k);
         unsigned char *r = (unsigned char *)w8;
         const R *p = Rec<R>::pos(r), *w = Rec<R>::vel(r);
-        const int *im = Rec<R>::image(r);
-        R px = p[0], py = p[1], pz = p[2], vx = w[0], vy = w[1], vz = w[2];
-        int ix = im[0], iy = im[1], iz = im[2], id = Rec<R>::id(r), sp = Rec<R>::species(r),
-            fl = Rec<R>::flags(r);
-        d.pos.x[j] = px;
-        d.pos.y[j] = py;
-        d.pos.z[j] = pz;
-        d.vel.x[j] = vx;
-        d.vel.y[j] = vy;
-        d.vel.z[j] = vz;
+        const int idx = Rec<R>::idx(r);
+        int ix = side.ix[idx], iy = side.iy[idx], iz = side.iz[idx], fl = side.flags[idx], id = side.id[idx];
+        d.pos.x[j] = p[0];
+        d.pos.y[j] = p[1];
+        d.pos.z[j] = p[2];
+        d.vel.x[j] = w[0];
+        d.vel.y[j] = w[1];
+        d.vel.z[j] = w[2];
+        d.species[j] = Rec<R>::species(r);
         d.ix[j] = ix;
         d.iy[j] = iy;
         d.iz[j] = iz;
-        d.id[j] = id;
-        d.species[j] = sp;
         d.flags[j] = fl;
+        d.id[j] = id;
     }
 }
 
@@ -494,6 +474,8 @@ static int bulk_run_fused(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r, doub
         k_soa_to_rec<R><<<grid_for(p->N, 256), 256, 0, st>>>(cur<R>(p), p->rec[0], p->N);
         RMPCD_CHECK_LAUNCH();
     }
+    // image, flags and id stay in the current API arrays, addressed by idx
+    const PView<R> side = cur<R>(p);
     int rb = 0;  // record buffer holding the current arrays
     const int nblocks = (c->S + FusedCfg<R>::kSlots - 1) / FusedCfg<R>::kSlots;
     int *perm = nullptr;  // identity for the first interval (data sorted on entry)
@@ -514,6 +496,9 @@ static int bulk_run_fused(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r, doub
         A.N = p->N;
         A.count_next = c->count_next;
         A.key_out = p->key;
+        A.ix = side.ix;
+        A.iy = side.iy;
+        A.iz = side.iz;
         A.g_next = grid_of(c);
         A.g_next.origin[0] = u0 - 1;
         A.g_next.origin[1] = u1 - 1;
@@ -556,7 +541,7 @@ static int bulk_run_fused(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r, doub
     PhaseTimer t("sort");
     rc = sort_perm_segments(c, p);
     if (rc) return rc;
-    k_rec_gather_to_soa<R><<<grid_for(p->N, 256), 256, 0, st>>>(p->rec[rb], p->perm, alt<R>(p), p->N);
+    k_rec_gather_to_soa<R><<<grid_for(p->N, 256), 256, 0, st>>>(p->rec[rb], p->perm, side, alt<R>(p), p->N);
     RMPCD_CHECK_LAUNCH();
     p->cur = 1 - p->cur;
     return RMPCD_OK;
