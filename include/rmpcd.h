@@ -235,6 +235,18 @@ int rmpcd_rattle_dimer_vel(rmpcd_particles *p, double d, double dt, const double
  * (programs/single_dimer_pbc.f90:312-315,356-359); mass[k] per particle */
 int rmpcd_colloid_vv_pos(rmpcd_particles *p, double dt, const double *mass);
 int rmpcd_colloid_vv_vel(rmpcd_particles *p, double dt, const double *mass);
+/* rmpcd_colloid_vv_pos without any device allocation; no counterpart in the
+ * reference.  rmpcd_colloid_vv_pos keeps the masses in a device buffer that it
+ * allocates (and frees, which synchronises the whole device) whenever a larger
+ * system comes along; a caller that cannot allocate at that point (device
+ * memory already committed to the solvent, or other streams that must not be
+ * stalled by a synchronising free) calls this one instead.  The masses go to a
+ * fixed 64 KB scratch array inside the library, so N must be <= 8192
+ * (RMPCD_ERR_CAPACITY otherwise).  The first call on each device looks up the
+ * scratch address (one-time setup): make it before starting any stream
+ * capture.  Nothing in the scratch has to start at zero.  There is one scratch
+ * array per device, so calls that overlap (several host threads) race on it. */
+int rmpcd_colloid_vv_pos_noalloc(rmpcd_particles *p, double dt, const double *mass);
 
 /* ------------------------------------------------------------------ */
 /* Lennard-Jones, src/interaction.f90                                   */

@@ -116,6 +116,7 @@ PROTOTYPES = {
     "rmpcd_rattle_dimer_vel": [PART_P, C.c_double, C.c_double, c_double_p],
     "rmpcd_colloid_vv_pos": [PART_P, C.c_double, c_double_p],
     "rmpcd_colloid_vv_vel": [PART_P, C.c_double, c_double_p],
+    "rmpcd_colloid_vv_pos_noalloc": [PART_P, C.c_double, c_double_p],
     "rmpcd_lj_init": [LJ_P, C.c_int, C.c_int, c_double_p, c_double_p, c_double_p],
     "rmpcd_nlist_init": [C.POINTER(NL_P), C.c_int, C.c_int],
     "rmpcd_nlist_destroy": [NL_P],

@@ -268,6 +268,32 @@ static int mass_on_device(const rmpcd_particles *p, const double *mass, const do
     return RMPCD_OK;
 }
 
+// Fixed device scratch of rmpcd_colloid_vv_pos_noalloc: the masses of at most
+// kNoAllocMaxParticles particles (64 KB), part of the library image, so the
+// entry point never calls the allocator.  Nothing in it has to start at zero:
+// every call writes the first N entries before its kernel reads them.
+constexpr int kNoAllocMaxParticles = 8192;
+constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) double g_noalloc_mass[kNoAllocMaxParticles];
+
+// address of g_noalloc_mass on the current device, looked up once per device
+static int noalloc_mass_scratch(double **out)
+{
+    static double *addr[kNoAllocMaxDevices] = {};
+    int dev = 0;
+    RMPCD_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        return fail(RMPCD_ERR_CAPACITY, "rmpcd_colloid_vv_pos_noalloc: device %d is above the %d devices it tracks",
+                    dev, kNoAllocMaxDevices);
+    if (!addr[dev]) {
+        double *a = nullptr;
+        RMPCD_CUDA_TRY(cudaGetSymbolAddress((void **)&a, g_noalloc_mass));
+        addr[dev] = a;
+    }
+    *out = addr[dev];
+    return RMPCD_OK;
+}
+
 }  // namespace rmpcd
 
 using namespace rmpcd;
@@ -435,6 +461,25 @@ int rmpcd_colloid_vv_vel(rmpcd_particles *p, double dt, const double *mass)
     int rc = mass_on_device(p, mass, &dm);
     if (rc) return rc;
     k_colloid_vv_vel<<<grid_for(p->N, 128), 128, 0, stream()>>>(cur<double>(p), dm, dt);
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+int rmpcd_colloid_vv_pos_noalloc(rmpcd_particles *p, double dt, const double *mass)
+{
+    RMPCD_ARG(p && mass, "null argument");
+    RMPCD_ARG(p->precision == RMPCD_FP64, "colloid integrator needs an FP64 system");
+    if (p->N > kNoAllocMaxParticles)
+        return fail(RMPCD_ERR_CAPACITY,
+                    "rmpcd_colloid_vv_pos_noalloc: N = %d is above its fixed scratch of %d particles "
+                    "(use rmpcd_colloid_vv_pos)",
+                    p->N, kNoAllocMaxParticles);
+    double *dm = nullptr;
+    int rc = noalloc_mass_scratch(&dm);
+    if (rc) return rc;
+    if (p->N == 0) return RMPCD_OK;
+    RMPCD_CUDA_TRY(cudaMemcpyAsync(dm, mass, sizeof(double) * (size_t)p->N, cudaMemcpyHostToDevice, stream()));
+    k_colloid_vv_pos<<<grid_for(p->N, 128), 128, 0, stream()>>>(cur<double>(p), dm, dt);
     RMPCD_CHECK_LAUNCH();
     return RMPCD_OK;
 }
