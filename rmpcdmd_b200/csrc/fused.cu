@@ -109,10 +109,50 @@ struct FusedArgs {
     const double *axes;
 };
 
+// rotation matrix of one cell in the working precision: the injected axis or
+// rand_sphere (src/mpcd.f90:43-62), then omega (src/mpcd.f90:163-171)
+template <typename R>
+struct CellRot {
+    R m[3][3];
+};
+
+template <typename R>
+__device__ inline CellRot<R> cell_rotation(int slot, const FusedArgs<R> &A)
+{
+    double n0, n1, n2;
+    if (A.axes) {
+        n0 = A.axes[3 * (size_t)slot];
+        n1 = A.axes[3 * (size_t)slot + 1];
+        n2 = A.axes[3 * (size_t)slot + 2];
+    } else {
+        rng::sphere(A.seed, A.step, (uint32_t)slot, n0, n1, n2);
+    }
+    Rot o = srd_matrix(n0, n1, n2, A.sin_a, A.cos_a);
+    CellRot<R> r;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) r.m[i][k] = (R)o.m[i][k];
+    return r;
+}
+
+// v = lv + matmul(omega, v - lv), the arithmetic of srd_rotate
+template <typename R>
+__device__ inline void cell_rotate(R &x, R &y, R &z, const R lv[3], const CellRot<R> &o)
+{
+    R d0 = x - lv[0], d1 = y - lv[1], d2 = z - lv[2];
+    R r0 = o.m[0][0] * d0 + o.m[0][1] * d1 + o.m[0][2] * d2;
+    R r1 = o.m[1][0] * d0 + o.m[1][1] * d1 + o.m[1][2] * d2;
+    R r2 = o.m[2][0] * d0 + o.m[2][1] * d1 + o.m[2][2] * d2;
+    x = lv[0] + r0;
+    y = lv[1] + r1;
+    z = lv[2] + r2;
+}
+
 // SRD of one cell of n consecutive velocity parts (src/mpcd.f90:127-178);
 // stride is the distance between consecutive particles in bytes
 template <typename R>
-__device__ inline void srd_cell(unsigned char *v0, int stride, int n, int slot, const FusedArgs<R> &A)
+__device__ inline void srd_cell(unsigned char *v0, int stride, int n, const CellRot<R> &o)
 {
     if constexpr (sizeof(R) == 4) {
         if (stride == 16) {
@@ -130,19 +170,10 @@ __device__ inline void srd_cell(unsigned char *v0, int stride, int n, int slot, 
             }
             if (n_eff <= 1) return;
             float lv[3] = {sx.value() / n_eff, sy.value() / n_eff, sz.value() / n_eff};
-            double n0, n1, n2;
-            if (A.axes) {
-                n0 = A.axes[3 * (size_t)slot];
-                n1 = A.axes[3 * (size_t)slot + 1];
-                n2 = A.axes[3 * (size_t)slot + 2];
-            } else {
-                rng::sphere(A.seed, A.step, (uint32_t)slot, n0, n1, n2);
-            }
-            Rot o = srd_matrix(n0, n1, n2, A.sin_a, A.cos_a);
             for (int k = 0; k < n; k++) {
                 int4 c = ((const int4 *)v0)[k];
                 float x = __int_as_float(c.x), y = __int_as_float(c.y), z = __int_as_float(c.z);
-                srd_rotate(x, y, z, lv, o);
+                cell_rotate(x, y, z, lv, o);
                 ((int4 *)v0)[k] = make_int4(__float_as_int(x), __float_as_int(y), __float_as_int(z), c.w);
             }
             return;
@@ -162,23 +193,29 @@ __device__ inline void srd_cell(unsigned char *v0, int stride, int n, int slot, 
     }
     if (n_eff <= 1) return;
     R lv[3] = {sx.value() / n_eff, sy.value() / n_eff, sz.value() / n_eff};
-    double n0, n1, n2;
-    if (A.axes) {
-        n0 = A.axes[3 * (size_t)slot];
-        n1 = A.axes[3 * (size_t)slot + 1];
-        n2 = A.axes[3 * (size_t)slot + 2];
-    } else {
-        rng::sphere(A.seed, A.step, (uint32_t)slot, n0, n1, n2);
-    }
-    Rot o = srd_matrix(n0, n1, n2, A.sin_a, A.cos_a);
     for (int k = 0; k < n; k++) {
         R *v = Rec<R>::vel(v0 + (size_t)k * stride);
         R x = v[0], y = v[1], z = v[2];
-        srd_rotate(x, y, z, lv, o);
+        cell_rotate(x, y, z, lv, o);
         v[0] = x;
         v[1] = y;
         v[2] = z;
     }
+}
+
+// floor(x / L) of the FP32 form, decided by float comparisons for
+// -L <= x < 2L (every streamed position of a wrapped particle)
+__device__ inline int floor_div_edge_f(float x, float L)
+{
+    if (x >= -L && x < 2.0f * L && !(x < 0.0f && x > -1e-30f)) return x < 0.0f ? -1 : (x < L ? 0 : 1);
+    return (int)floorf(x / L);
+}
+
+template <typename R>
+__device__ inline int wrap_jump(R x, double L)
+{
+    if constexpr (sizeof(R) == 4) return floor_div_edge_f(x, (float)L);
+    else return floor_div_edge(x, L);
 }
 
 // mpcd_stream_periodic of one particle (src/mpcd.f90:450-455); returns its
@@ -189,8 +226,7 @@ __device__ inline int stream_values(const FusedArgs<R> &A, R &x, R &y, R &z, R v
     x = x + vx * A.dt;
     y = y + vy * A.dt;
     z = z + vz * A.dt;
-    int jx = floor_div_edge((double)x, A.e0), jy = floor_div_edge((double)y, A.e1),
-        jz = floor_div_edge((double)z, A.e2);
+    int jx = wrap_jump<R>(x, A.e0), jy = wrap_jump<R>(y, A.e1), jz = wrap_jump<R>(z, A.e2);
     if (jx) {
         x = x - (R)(jx * A.e0);
         A.ix[idx] += jx;
@@ -313,9 +349,12 @@ __global__ void __launch_bounds__(kFusedThreads, FusedCfg<R>::kMinBlocks) k_bulk
                 cp_async8(s_vel + (size_t)j * VB + 8 * c, A.in + (size_t)s_perm[j] * B + 8 * c);
             }
         }
+        // the cell's rotation is drawn while the gathers are in flight
+        CellRot<R> rot;
+        if (my_n > 1) rot = cell_rotation<R>(slot, A);
         cp_async_wait_all();
         __syncthreads();
-        if (my_n > 1) srd_cell<R>(s_vel + (size_t)(my_a - a0) * VB, VB, my_n, slot, A);
+        if (my_n > 1) srd_cell<R>(s_vel + (size_t)(my_a - a0) * VB, VB, my_n, rot);
         __syncthreads();
         // stream, key, count and write every particle; the rest of the next
         // record is fetched while the current one is processed
@@ -348,7 +387,7 @@ __global__ void __launch_bounds__(kFusedThreads, FusedCfg<R>::kMinBlocks) k_bulk
                 long long *d = (long long *)(A.out + (size_t)(my_a + k) * B);
                 for (int w = 0; w < B / 8; w++) d[w] = s[w];
             }
-            if (my_n > 1) srd_cell<R>(A.out + (size_t)my_a * B, B, my_n, slot, A);
+            if (my_n > 1) srd_cell<R>(A.out + (size_t)my_a * B, B, my_n, cell_rotation<R>(slot, A));
         }
         __syncthreads();
         for (int jb = 0; jb < np; jb += kFusedThreads) {
