@@ -7,6 +7,7 @@
 
 #include "rmpcd_common.cuh"
 #include "state.cuh"
+#include "stepops.cuh"
 #include "timers.cuh"
 
 namespace rmpcd {
@@ -16,11 +17,8 @@ template <typename R>
 __global__ void k_md_pos(PView<R> v, R dt, R dt_sq)
 {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < v.N;
-         i += (long long)gridDim.x * blockDim.x) {
-        v.pos.x[i] = v.pos.x[i] + dt * v.vel.x[i] + dt_sq * v.force.x[i];
-        v.pos.y[i] = v.pos.y[i] + dt * v.vel.y[i] + dt_sq * v.force.y[i];
-        v.pos.z[i] = v.pos.z[i] + dt * v.vel.z[i] + dt_sq * v.force.z[i];
-    }
+         i += (long long)gridDim.x * blockDim.x)
+        md_pos_one(v, i, dt, dt_sq);
 }
 
 // md_vel, src/md.f90:219-237
@@ -28,16 +26,8 @@ template <typename R>
 __global__ void k_md_vel(PView<R> v, R dt)
 {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < v.N;
-         i += (long long)gridDim.x * blockDim.x) {
-        int f = v.flags[i];
-        if (!((f >> WALL_BIT) & 1)) {
-            v.vel.x[i] = v.vel.x[i] + dt * (v.force.x[i] + v.force_old.x[i]) / 2;
-            v.vel.y[i] = v.vel.y[i] + dt * (v.force.y[i] + v.force_old.y[i]) / 2;
-            v.vel.z[i] = v.vel.z[i] + dt * (v.force.z[i] + v.force_old.z[i]) / 2;
-        } else {
-            v.flags[i] = f & ~(1 << WALL_BIT);
-        }
-    }
+         i += (long long)gridDim.x * blockDim.x)
+        md_vel_one(v, i, dt);
 }
 
 // cell_md_pos, src/md.f90:79-102
@@ -123,47 +113,8 @@ template <typename R>
 __global__ void k_apply_pbc(PView<R> v, double e0, double e1, double e2)
 {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < v.N;
-         i += (long long)gridDim.x * blockDim.x) {
-        R x = v.pos.x[i], y = v.pos.y[i], z = v.pos.z[i];
-        int jx = floor_div_edge((double)x, e0), jy = floor_div_edge((double)y, e1), jz = floor_div_edge((double)z, e2);
-        if (jx) {
-            v.ix[i] += jx;
-            v.pos.x[i] = x - (R)(jx * e0);
-        }
-        if (jy) {
-            v.iy[i] += jy;
-            v.pos.y[i] = y - (R)(jy * e1);
-        }
-        if (jz) {
-            v.iz[i] += jz;
-            v.pos.z[i] = z - (R)(jz * e2);
-        }
-    }
-}
-
-struct E3 {
-    double e[3];
-};
-
-struct Masses {
-    double m[RMPCD_MAX_SPECIES];
-    int n;
-};
-
-// mass(species(k)) of bead k; out-of-range species flag an error
-__device__ inline double bead_mass(const Masses &ms, const int *species, int k, unsigned *err)
-{
-    int s = species[k];
-    if (s < 1 || s > ms.n) {
-        atomicOr(err, DEV_ERR_RATTLE);
-        return 1.0;
-    }
-    return ms.m[s - 1];
-}
-
-__device__ inline double dot3(const double a[3], const double b[3])
-{
-    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+         i += (long long)gridDim.x * blockDim.x)
+        apply_pbc_one(v, i, e0, e1, e2);
 }
 
 // rattle_dimer_pos, src/md.f90:265-296
@@ -171,70 +122,27 @@ __global__ void k_rattle_pos(PView<double> v, const double *rx, const double *ry
                              Masses ms, double d, double dt, E3 L, unsigned *err)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double m1 = bead_mass(ms, v.species, 0, err), m2 = bead_mass(ms, v.species, 1, err);
-    double r[3], s[3];
-    r[0] = min_image_d(rx[0] - rx[1], L.e[0]);
-    r[1] = min_image_d(ry[0] - ry[1], L.e[1]);
-    r[2] = min_image_d(rz[0] - rz[1], L.e[2]);
-    s[0] = min_image_d(v.pos.x[0] - v.pos.x[1], L.e[0]);
-    s[1] = min_image_d(v.pos.y[0] - v.pos.y[1], L.e[1]);
-    s[2] = min_image_d(v.pos.z[0] - v.pos.z[1], L.e[2]);
-    double inv_mass = 1 / m1 + 1 / m2;
-    double rsq = dot3(r, r), ssq = dot3(s, s), rs = dot3(r, s);
-    double disc = rs * rs - rsq * (ssq - d * d);
-    if (disc < 0) atomicOr(err, DEV_ERR_RATTLE);
-    double g = rs - sqrt(disc);
-    g = g / (dt * inv_mass * rsq);
-    double *px[3] = {v.pos.x, v.pos.y, v.pos.z};
-    double *vx[3] = {v.vel.x, v.vel.y, v.vel.z};
-    for (int k = 0; k < 3; k++) {
-        px[k][0] = px[k][0] - g * dt * r[k] / m1;
-        px[k][1] = px[k][1] + g * dt * r[k] / m2;
-    }
-    for (int k = 0; k < 3; k++) {
-        vx[k][0] = vx[k][0] - g * r[k] / m1;
-        vx[k][1] = vx[k][1] + g * r[k] / m2;
-    }
+    rattle_pos_dimer(v, rx, ry, rz, ms, d, dt, L, err);
 }
 
 // rattle_dimer_vel, src/md.f90:298-319
 __global__ void k_rattle_vel(PView<double> v, Masses ms, double d, E3 L, unsigned *err)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double m1 = bead_mass(ms, v.species, 0, err), m2 = bead_mass(ms, v.species, 1, err);
-    double s[3], dv[3];
-    double inv_mass = 1 / m1 + 1 / m2;
-    s[0] = min_image_d(v.pos.x[0] - v.pos.x[1], L.e[0]);
-    s[1] = min_image_d(v.pos.y[0] - v.pos.y[1], L.e[1]);
-    s[2] = min_image_d(v.pos.z[0] - v.pos.z[1], L.e[2]);
-    double *vx[3] = {v.vel.x, v.vel.y, v.vel.z};
-    for (int k = 0; k < 3; k++) dv[k] = vx[k][0] - vx[k][1];
-    double kk = dot3(dv, s) / (d * d * inv_mass);
-    for (int k = 0; k < 3; k++) {
-        vx[k][0] = vx[k][0] - kk * s[k] / m1;
-        vx[k][1] = vx[k][1] + kk * s[k] / m2;
-    }
+    rattle_vel_dimer(v, ms, d, L, err);
 }
 
 // colloid VV halves, programs/single_dimer_pbc.f90:312-315 and :356-359
 __global__ void k_colloid_vv_pos(PView<double> v, const double *mass, double dt)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v.N; i += gridDim.x * blockDim.x) {
-        double m2 = 2 * mass[i];
-        v.pos.x[i] = v.pos.x[i] + dt * v.vel.x[i] + dt * dt * v.force.x[i] / m2;
-        v.pos.y[i] = v.pos.y[i] + dt * v.vel.y[i] + dt * dt * v.force.y[i] / m2;
-        v.pos.z[i] = v.pos.z[i] + dt * v.vel.z[i] + dt * dt * v.force.z[i] / m2;
-    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v.N; i += gridDim.x * blockDim.x)
+        colloid_vv_pos_one(v, i, mass[i], dt);
 }
 
 __global__ void k_colloid_vv_vel(PView<double> v, const double *mass, double dt)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v.N; i += gridDim.x * blockDim.x) {
-        double m2 = 2 * mass[i];
-        v.vel.x[i] = v.vel.x[i] + dt * (v.force.x[i] + v.force_old.x[i]) / m2;
-        v.vel.y[i] = v.vel.y[i] + dt * (v.force.y[i] + v.force_old.y[i]) / m2;
-        v.vel.z[i] = v.vel.z[i] + dt * (v.force.z[i] + v.force_old.z[i]) / m2;
-    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v.N; i += gridDim.x * blockDim.x)
+        colloid_vv_vel_one(v, i, mass[i], dt);
 }
 
 // per-particle masses cached on the device (re-uploaded only on change)

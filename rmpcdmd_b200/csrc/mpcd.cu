@@ -8,86 +8,18 @@
 #include "hilbert.cuh"
 #include "keys.cuh"
 #include "rng.cuh"
+#include "stepops.cuh"
 #include "timers.cuh"
 
 namespace rmpcd {
-
-struct SrdParams {
-    double sin_a, cos_a, t_factor;
-    int thermostat, hydro;
-    uint64_t seed, step;
-    const double *axes;   // injected per-slot axes or null
-    const double *gauss;  // injected per-particle normals or null
-};
-
-__device__ inline double at_normal(const SrdParams &q, int j, int k)
-{
-    return q.gauss ? q.gauss[3 * (size_t)j + k] : rng::normal(q.seed, q.step, (uint32_t)j, (uint32_t)k);
-}
 
 // simple_mpcd_step, src/mpcd.f90:71-183
 template <typename R>
 __global__ void k_simple_mpcd(const int *__restrict__ count, const int *__restrict__ start, int S,
                               R *vx, R *vy, R *vz, const int *__restrict__ species, SrdParams q)
 {
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
-        int n = count[s];
-        if (n <= 1) continue;
-        int a = start[s];
-        int n_eff = 0;
-        CellSum<R> sx, sy, sz;
-        for (int i = a; i < a + n; i++) {
-            if (species[i] > 0) {
-                sx.add(vx[i]);
-                sy.add(vy[i]);
-                sz.add(vz[i]);
-                n_eff++;
-            }
-        }
-        if (n_eff <= 1) continue;
-        R lv[3] = {sx.value() / n_eff, sy.value() / n_eff, sz.value() / n_eff};
-        if (q.thermostat) {
-            CellSum<R> wx, wy, wz;
-            for (int i = a; i < a + n; i++) {
-                if (species[i] <= 0) continue;
-                R nx = (R)(at_normal(q, i, 0) * q.t_factor);
-                R ny = (R)(at_normal(q, i, 1) * q.t_factor);
-                R nz = (R)(at_normal(q, i, 2) * q.t_factor);
-                vx[i] = nx;
-                vy[i] = ny;
-                vz[i] = nz;
-                wx.add(nx);
-                wy.add(ny);
-                wz.add(nz);
-            }
-            R dv[3] = {lv[0] - wx.value() / n_eff, lv[1] - wy.value() / n_eff, lv[2] - wz.value() / n_eff};
-            if (q.hydro) {
-                for (int i = a; i < a + n; i++) {
-                    if (species[i] <= 0) continue;
-                    vx[i] = vx[i] + dv[0];
-                    vy[i] = vy[i] + dv[1];
-                    vz[i] = vz[i] + dv[2];
-                }
-            }
-        } else {
-            double n0, n1, n2;
-            if (q.axes) {
-                n0 = q.axes[3 * (size_t)s];
-                n1 = q.axes[3 * (size_t)s + 1];
-                n2 = q.axes[3 * (size_t)s + 2];
-            } else {
-                rng::sphere(q.seed, q.step, (uint32_t)s, n0, n1, n2);
-            }
-            Rot o = srd_matrix(n0, n1, n2, q.sin_a, q.cos_a);
-            for (int i = a; i < a + n; i++) {
-                R x = vx[i], y = vy[i], z = vz[i];
-                srd_rotate(x, y, z, lv, o);
-                vx[i] = x;
-                vy[i] = y;
-                vz[i] = z;
-            }
-        }
-    }
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x)
+        srd_slot<R>(count[s], start[s], s, 0, vx, vy, vz, species, q);
 }
 
 // wall_mpcd_step, src/mpcd.f90:193-337

@@ -1,0 +1,331 @@
+// Neighbor-list and Lennard-Jones bodies (src/neighbor_list.f90,
+// src/interaction.f90) shared by the single-system kernels and the batched
+// replica engine.
+#pragma once
+
+#include "keys.cuh"
+#include "rmpcd_common.cuh"
+#include "state.cuh"
+
+namespace rmpcd {
+
+constexpr int kNlBlockThreads = 256;
+
+
+struct LJDev {
+    int n1;
+    double epsilon[16], sigma[16], cut_sq[16], cut_energy[16];
+};
+
+// x**3 = x*(x*x), x**6 = x**3 * x**3 (gfortran's constant-power expansion)
+__device__ inline double cube(double x) { return x * (x * x); }
+__device__ inline double sixth(double x)
+{
+    double c = cube(x);
+    return c * c;
+}
+
+// lj_force / lj_energy, src/interaction.f90:83-96,126-136
+__device__ inline double lj_force_over_r(double r_sq, double eps, double sigma)
+{
+    double s6 = sixth(sigma) / cube(r_sq);
+    return 24.0 * eps * s6 / r_sq * (2.0 * s6 - 1.0);
+}
+__device__ inline double lj_energy(double r_sq, double eps, double sigma, double ce)
+{
+    double s6 = sixth(sigma) / cube(r_sq);
+    return 4.0 * eps * (s6 * s6 - s6) - ce;
+}
+
+__device__ inline int imod(int a, int p)
+{
+    int r = a % p;
+    return (r != 0 && ((r < 0) != (p < 0))) ? r + p : r;
+}
+
+// update_list, src/neighbor_list.f90:76-157: one block per colloid; stencil
+// cells are processed in chunks of kNlBlockThreads, their particles enumerated in
+// stencil order and compacted in order with a block scan.
+template <typename R>
+__device__ inline void update_list_block(int i, const Grid &g, const double *cx, const double *cy, const double *cz,
+                                         const int *cs, const R *sx, const R *sy, const R *sz, const int *sspec,
+                                         const int *count, const int *start, const int *stencil, int n_stencil,
+                                         double radiussq, const LJDev &lj, int do_lj, int Nmax, int *list,
+                                         int *n_out, unsigned char *is_md, unsigned char *is_reac, unsigned *err)
+{
+    __shared__ int c_slot[kNlBlockThreads], c_start[kNlBlockThreads], c_off[kNlBlockThreads + 1];
+    __shared__ int c_md[kNlBlockThreads], c_noreac[kNlBlockThreads];
+    __shared__ int warp_sum[kNlBlockThreads / 32];
+    __shared__ int s_total, s_base;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    double x0 = cx[i], x1 = cy[i], x2 = cz[i];
+    int si = cs[i];
+    int cell[3];
+    cell_coords(g, x0, x1, x2, cell);  // cartesian_indices (0-based)
+    double L0 = g.L[0] * g.a, L1 = g.L[1] * g.a, L2 = g.L[2] * g.a;
+    if (t == 0) s_base = 0;
+    __syncthreads();
+    for (int j0 = 0; j0 < n_stencil; j0 += kNlBlockThreads) {
+        int j = j0 + t;
+        int cnt = 0;
+        if (j < n_stencil) {
+            int p[3] = {imod(cell[0] + stencil[3 * j], g.L[0]), imod(cell[1] + stencil[3 * j + 1], g.L[1]),
+                        imod(cell[2] + stencil[3 * j + 2], g.L[2])};
+            int s = slot_of_cell(g, p);
+            c_slot[t] = s;
+            c_start[t] = start[s];
+            cnt = count[s];
+        }
+        c_md[t] = 0;
+        c_noreac[t] = 0;
+        // exclusive scan of the candidate counts of this chunk
+        int inc = cnt;
+        for (int o = 1; o < 32; o <<= 1) {
+            int w = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += w;
+        }
+        if (lane == 31) warp_sum[wid] = inc;
+        __syncthreads();
+        if (t == 0) {
+            int acc = 0;
+            for (int w = 0; w < kNlBlockThreads / 32; w++) {
+                int v = warp_sum[w];
+                warp_sum[w] = acc;
+                acc += v;
+            }
+            s_total = acc;
+        }
+        __syncthreads();
+        c_off[t] = warp_sum[wid] + inc - cnt;
+        if (t == 0) c_off[kNlBlockThreads] = s_total;
+        __syncthreads();
+        const int total = c_off[kNlBlockThreads];
+        for (int k0 = 0; k0 < total; k0 += kNlBlockThreads) {
+            int k = k0 + t;
+            int accept = 0;
+            int idx = -1;
+            if (k < total) {
+                // stencil cell of candidate k: last cell with offset <= k
+                int lo = 0, hi = kNlBlockThreads;
+                while (hi - lo > 1) {
+                    int mid = (lo + hi) >> 1;
+                    if (c_off[mid] <= k) lo = mid;
+                    else hi = mid;
+                }
+                const int cl = lo;
+                idx = c_start[cl] + (k - c_off[cl]);
+                int s = sspec[idx];
+                if (s > 0) {
+                    double r0 = min_image_d(x0 - (double)sx[idx], L0);
+                    double r1 = min_image_d(x1 - (double)sy[idx], L1);
+                    double r2 = min_image_d(x2 - (double)sz[idx], L2);
+                    double rsq = r0 * r0 + r1 * r1 + r2 * r2;
+                    if (rsq < radiussq) {
+                        accept = 1;
+                        c_md[cl] = 1;
+                        if (do_lj && rsq <= lj.cut_sq[(s - 1) + lj.n1 * (si - 1)]) c_noreac[cl] = 1;
+                    }
+                }
+            }
+            // ordered compaction of accepted candidates
+            unsigned bal = __ballot_sync(0xffffffffu, accept);
+            if (lane == 0) warp_sum[wid] = __popc(bal);
+            __syncthreads();
+            if (t == 0) {
+                int acc = 0;
+                for (int w = 0; w < kNlBlockThreads / 32; w++) {
+                    int v = warp_sum[w];
+                    warp_sum[w] = acc;
+                    acc += v;
+                }
+                s_total = acc;
+            }
+            __syncthreads();
+            if (accept) {
+                int pos = s_base + warp_sum[wid] + __popc(bal & ((1u << lane) - 1u));
+                if (pos < Nmax) list[(size_t)i * Nmax + pos] = idx;
+                else atomicOr(err, DEV_ERR_NLIST_FULL);
+            }
+            __syncthreads();
+            if (t == 0) s_base += s_total;
+            __syncthreads();
+        }
+        __syncthreads();
+        if (j < n_stencil && c_md[t]) {
+            is_md[c_slot[t]] = 1;
+            if (c_noreac[t]) is_reac[c_slot[t]] = 0;
+        }
+        __syncthreads();
+    }
+    if (t == 0) n_out[i] = s_base < Nmax ? s_base : Nmax;
+}
+
+
+// pair force of list entry q (src/neighbor_list.f90:198-219): colloid at x
+// of species s1 and the entry's solvent particle
+template <typename R>
+__device__ inline void pair_force_entry(size_t q, const double x[3], int s1, const R *sx, const R *sy, const R *sz,
+                                        const int *sspec, int *sflags, const int *list, double L0, double L1,
+                                        double L2, const LJDev &lj, double *pf, double *pe, unsigned char *contrib,
+                                        int *ncontrib, int *max_contrib)
+{
+    const int mask = (1 << MD_BIT) | (s1 == 1 ? (1 << CATALYZED_BIT) : 0);
+    int idx = list[q];
+    int s2 = sspec[idx];
+    unsigned char c = 0;
+    if (s2 > 0) {
+        double d0 = min_image_d(x[0] - (double)sx[idx], L0);
+        double d1 = min_image_d(x[1] - (double)sy[idx], L1);
+        double d2 = min_image_d(x[2] - (double)sz[idx], L2);
+        double r_sq = d0 * d0 + d1 * d1 + d2 * d2;
+        int tt = (s2 - 1) + lj.n1 * (s1 - 1);
+        if (r_sq <= lj.cut_sq[tt]) {
+            double fr = lj_force_over_r(r_sq, lj.epsilon[tt], lj.sigma[tt]);
+            pf[3 * q] = fr * d0;
+            pf[3 * q + 1] = fr * d1;
+            pf[3 * q + 2] = fr * d2;
+            pe[q] = lj_energy(r_sq, lj.epsilon[tt], lj.sigma[tt], lj.cut_energy[tt]);
+            c = 1;
+            int prev = atomicAdd(ncontrib + idx, 1);
+            if (prev >= 1) atomicMax(max_contrib, prev + 1);
+            atomicOr(sflags + idx, mask);
+        }
+    }
+    contrib[q] = c;
+}
+
+// solvent force - f of entry q when its particle has exactly one contribution
+template <typename R>
+__device__ inline void apply_single_entry(size_t q, const int *list, const unsigned char *contrib, const double *pf,
+                                          const int *ncontrib, R *fx, R *fy, R *fz)
+{
+    if (!contrib[q]) return;
+    int idx = list[q];
+    if (ncontrib[idx] != 1) return;
+    fx[idx] = fx[idx] - (R)pf[3 * q];
+    fy[idx] = fy[idx] - (R)pf[3 * q + 1];
+    fz[idx] = fz[idx] - (R)pf[3 * q + 2];
+}
+
+// particles with several contributions: colloid by colloid in order; inside
+// one colloid's list entries are distinct unless the stencil wraps the box,
+// in which case a single thread applies everything in order (one block)
+template <typename R>
+__device__ inline void apply_multi_block(const int *list, const int *n, int C, int Nmax, const unsigned char *contrib,
+                                         const double *pf, const int *ncontrib, int serial, R *fx, R *fy, R *fz)
+{
+    for (int i = 0; i < C; i++) {
+        const int ni = n[i];
+        if (serial) {
+            if (threadIdx.x == 0) {
+                for (int e = 0; e < ni; e++) {
+                    size_t q = (size_t)i * Nmax + e;
+                    if (!contrib[q]) continue;
+                    int idx = list[q];
+                    if (ncontrib[idx] < 2) continue;
+                    fx[idx] = fx[idx] - (R)pf[3 * q];
+                    fy[idx] = fy[idx] - (R)pf[3 * q + 1];
+                    fz[idx] = fz[idx] - (R)pf[3 * q + 2];
+                }
+            }
+        } else {
+            for (int e = threadIdx.x; e < ni; e += blockDim.x) {
+                size_t q = (size_t)i * Nmax + e;
+                if (!contrib[q]) continue;
+                int idx = list[q];
+                if (ncontrib[idx] < 2) continue;
+                fx[idx] = fx[idx] - (R)pf[3 * q];
+                fy[idx] = fy[idx] - (R)pf[3 * q + 1];
+                fz[idx] = fz[idx] - (R)pf[3 * q + 2];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// f1 = sum of colloid i's pair forces in list order; force(:,i) += f1; the
+// contributing entries are compacted in order into clist (one block)
+__device__ inline void colloid_sum_block(int i, const int *n, int Nmax, const unsigned char *contrib, const double *pf,
+                                         double *cfx, double *cfy, double *cfz, int *clist, int *cn)
+{
+    __shared__ int idxs[kNlBlockThreads];
+    __shared__ int warp_cnt[kNlBlockThreads / 32];
+    __shared__ int s_cnt;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    const int ni = n[i];
+    double f0 = 0, f1 = 0, f2 = 0;
+    int total = 0;
+    for (int e0 = 0; e0 < ni; e0 += kNlBlockThreads) {
+        int e = e0 + t;
+        int c = (e < ni) ? contrib[(size_t)i * Nmax + e] : 0;
+        unsigned bal = __ballot_sync(0xffffffffu, c);
+        if (lane == 0) warp_cnt[wid] = __popc(bal);
+        __syncthreads();
+        if (t == 0) {
+            int acc = 0;
+            for (int w = 0; w < kNlBlockThreads / 32; w++) {
+                int v = warp_cnt[w];
+                warp_cnt[w] = acc;
+                acc += v;
+            }
+            s_cnt = acc;
+        }
+        __syncthreads();
+        if (c) idxs[warp_cnt[wid] + __popc(bal & ((1u << lane) - 1u))] = e;
+        __syncthreads();
+        if (t == 0) {
+            for (int k = 0; k < s_cnt; k++) {
+                size_t q = (size_t)i * Nmax + idxs[k];
+                f0 = f0 + pf[3 * q];
+                f1 = f1 + pf[3 * q + 1];
+                f2 = f2 + pf[3 * q + 2];
+                clist[(size_t)i * Nmax + total + k] = idxs[k];
+            }
+            total += s_cnt;
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        cfx[i] = cfx[i] + f0;
+        cfy[i] = cfy[i] + f1;
+        cfz[i] = cfz[i] + f2;
+        cn[i] = total;
+    }
+}
+
+// compute_force_n2, src/neighbor_list.f90:227-264: colloid m receives, in the
+// sequential loop order, -f(k,m) for k < m and then +f(m,j) for j > m
+__device__ inline void force_n2_one(int m, const double *px, const double *py, const double *pz, const int *sp, int C,
+                                    double L0, double L1, double L2, const LJDev &lj, double *fx, double *fy,
+                                    double *fz)
+{
+    double a0 = fx[m], a1 = fy[m], a2 = fz[m];
+    for (int k = 0; k < C; k++) {
+        if (k == m) continue;
+        int i = k < m ? k : m, j = k < m ? m : k;
+        double d0 = min_image_d(px[i] - px[j], L0);
+        double d1 = min_image_d(py[i] - py[j], L1);
+        double d2 = min_image_d(pz[i] - pz[j], L2);
+        double r_sq = d0 * d0 + d1 * d1 + d2 * d2;
+        int s1 = sp[i], s2 = sp[j];
+        if (r_sq <= lj.cut_sq[(s1 - 1) + lj.n1 * (s2 - 1)]) {
+            int tt = (s2 - 1) + lj.n1 * (s1 - 1);
+            double fr = lj_force_over_r(r_sq, lj.epsilon[tt], lj.sigma[tt]);
+            double f0 = fr * d0, f1 = fr * d1, f2 = fr * d2;
+            if (k < m) {
+                a0 = a0 - f0;
+                a1 = a1 - f1;
+                a2 = a2 - f2;
+            } else {
+                a0 = a0 + f0;
+                a1 = a1 + f1;
+                a2 = a2 + f2;
+            }
+        }
+    }
+    fx[m] = a0;
+    fy[m] = a1;
+    fz[m] = a2;
+}
+
+}  // namespace rmpcd

@@ -8,6 +8,7 @@
 #include "keys.cuh"
 #include "rng.cuh"
 #include "sortcore.cuh"
+#include "stepops.cuh"
 #include "timers.cuh"
 
 namespace rmpcd {
@@ -59,13 +60,8 @@ __global__ void k_max_disp(Vec3<R> pos, Vec3<R> old, const int *species, int N,
     double m = 0;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
          i += (long long)gridDim.x * blockDim.x) {
-        if (species[i] >= 0) {
-            double d0 = (double)pos.x[i] - (double)old.x[i];
-            double d1 = (double)pos.y[i] - (double)old.y[i];
-            double d2 = (double)pos.z[i] - (double)old.z[i];
-            double r = d0 * d0 + d1 * d1 + d2 * d2;
-            m = m > r ? m : r;
-        }
+        double r = disp_sq_one(pos, old, species, i);
+        m = m > r ? m : r;
     }
     m = warp_max(m);
     if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out, m);

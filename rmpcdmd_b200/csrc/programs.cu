@@ -8,13 +8,10 @@
 #include "rmpcd_common.cuh"
 #include "rng.cuh"
 #include "state.cuh"
+#include "stepops.cuh"
 #include "timers.cuh"
 
 namespace rmpcd {
-
-struct C2 {
-    double c1[3], c2[3];
-};
 
 // flag_particles_nl, programs/single_dimer_pbc.f90:493-509
 template <typename R>
@@ -23,45 +20,21 @@ __global__ void k_flag_nl(const int *list, const int *n, int point, int Nmax, co
                           const int *species, int *flags, double L0, double L1, double L2, double cut_sq)
 {
     int n1 = n[point];
-    double x0 = cx[point], x1 = cy[point], x2 = cz[point];
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n1; s += gridDim.x * blockDim.x) {
-        int r = list[(size_t)point * Nmax + s];
-        if (species[r] == 1) {
-            double d0 = min_image_d(x0 - (double)sx[r], L0);
-            double d1 = min_image_d(x1 - (double)sy[r], L1);
-            double d2 = min_image_d(x2 - (double)sz[r], L2);
-            double d = d0 * d0 + d1 * d1 + d2 * d2;
-            if (d < cut_sq) atomicOr(flags + r, 1 << REAC_BIT);
-        }
-    }
+    double x[3] = {cx[point], cy[point], cz[point]};
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n1; s += gridDim.x * blockDim.x)
+        flag_nl_one(list[(size_t)point * Nmax + s], x, sx, sy, sz, species, flags, L0, L1, L2, cut_sq);
 }
 
-// change_species, programs/single_dimer_pbc.f90:511-542; the acceptance
-// uniform of particle m is Philox(seed, step, m, REACT)
+// change_species, programs/single_dimer_pbc.f90:511-542
 template <typename R>
 __global__ void k_change_species(PView<R> v, const double *cx, const double *cy, const double *cz,
                                  double L0, double L1, double L2, double cut_c, double cut_n, double prob,
                                  uint64_t seed, uint64_t step)
 {
-    double a0 = cx[0], a1 = cy[0], a2 = cz[0], b0 = cx[1], b1 = cy[1], b2 = cz[1];
+    double a[3] = {cx[0], cy[0], cz[0]}, b[3] = {cx[1], cy[1], cz[1]};
     for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < v.N;
-         m += (long long)gridDim.x * blockDim.x) {
-        int f = v.flags[m];
-        if (!((f >> REAC_BIT) & 1)) continue;
-        double px = (double)v.pos.x[m], py = (double)v.pos.y[m], pz = (double)v.pos.z[m];
-        double d0 = min_image_d(a0 - px, L0), d1 = min_image_d(a1 - py, L1), d2 = min_image_d(a2 - pz, L2);
-        double dC = d0 * d0 + d1 * d1 + d2 * d2;
-        d0 = min_image_d(b0 - px, L0);
-        d1 = min_image_d(b1 - py, L1);
-        d2 = min_image_d(b2 - pz, L2);
-        double dN = d0 * d0 + d1 * d1 + d2 * d2;
-        if ((dC > cut_c) && (dN > cut_n)) {
-            double u0, u1;
-            rng::uniform2(seed, step, (uint32_t)m, rng::REACT, 0, u0, u1);
-            if (u0 <= prob) v.species[m] = 2;
-            v.flags[m] = f & ~(1 << REAC_BIT);
-        }
-    }
+         m += (long long)gridDim.x * blockDim.x)
+        change_species_one(v, m, m, a, b, L0, L1, L2, cut_c, cut_n, prob, seed, step);
 }
 
 // refuel, programs/single_dimer_pbc.f90:544-565
@@ -69,19 +42,10 @@ template <typename R>
 __global__ void k_refuel(PView<R> v, const double *cx, const double *cy, const double *cz, double L0,
                          double L1, double L2, double far)
 {
-    double a0 = cx[0], a1 = cy[0], a2 = cz[0], b0 = cx[1], b1 = cy[1], b2 = cz[1];
+    double a[3] = {cx[0], cy[0], cz[0]}, b[3] = {cx[1], cy[1], cz[1]};
     for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < v.N;
-         m += (long long)gridDim.x * blockDim.x) {
-        if (v.species[m] != 2) continue;
-        double px = (double)v.pos.x[m], py = (double)v.pos.y[m], pz = (double)v.pos.z[m];
-        double d0 = min_image_d(a0 - px, L0), d1 = min_image_d(a1 - py, L1), d2 = min_image_d(a2 - pz, L2);
-        double dC = d0 * d0 + d1 * d1 + d2 * d2;
-        d0 = min_image_d(b0 - px, L0);
-        d1 = min_image_d(b1 - py, L1);
-        d2 = min_image_d(b2 - pz, L2);
-        double dN = d0 * d0 + d1 * d1 + d2 * d2;
-        if ((dC > far) && (dN > far)) v.species[m] = 1;
-    }
+         m += (long long)gridDim.x * blockDim.x)
+        refuel_one(v, m, a, b, L0, L1, L2, far);
 }
 
 __global__ void k_n_solvent(const int *species, int N, int n_species, int *counts)
