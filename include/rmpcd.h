@@ -308,6 +308,58 @@ int rmpcd_velocity_sums(rmpcd_particles *p, double out[4]);
 int rmpcd_bulk_run(rmpcd_particles *p, rmpcd_cells *cells, rmpcd_rng *rng,
                    double tau, int has_alpha, double alpha, int n_intervals);
 
+/* Batched single_dimer_pbc: the main loop of programs/single_dimer_pbc.f90
+ * (:303-443: N_MD MD steps with the program's re-sort test, then
+ * random_shift, re-sort, simple_mpcd_step and refuel) for R independent
+ * systems advanced together, one launch per phase for all of them, the
+ * whole interval captured once in a CUDA graph.  This replaces the program's
+ * own loop (it has no module counterpart in the reference): each replica is
+ * set up with the module entry points above exactly as the program does,
+ * handed over with rmpcd_dimer_batch_create, and copied back into handles
+ * with rmpcd_dimer_batch_scatter for output.  Replica r then holds, bit for
+ * bit, the state of its own handles advanced by the same calls one by one. */
+typedef struct rmpcd_dimer_batch rmpcd_dimer_batch;
+typedef struct rmpcd_dimer_params {
+    double tau;          /* MPCD interval; dt = tau / N_MD */
+    int N_MD;            /* MD steps per interval */
+    double bond;         /* dimer bond length d (rattle) */
+    double skin;         /* list skin: re-sort when a colloid moved >= skin/10
+                            or a solvent particle >= 0.89 skin */
+    double list_radius;  /* update_list radius: max cut + skin */
+    double prob;         /* A -> B probability of change_species */
+    double cut_sq_C;     /* cut_sq(1,1): flag_particles_nl and change_species */
+    double cut_sq_N;     /* cut_sq(1,2): change_species */
+    double vv_mass[2];   /* masses of the two beads in the velocity-Verlet halves */
+    int thermostat;      /* simple_mpcd_step options */
+    int hydro;
+    double T;
+} rmpcd_dimer_params;
+/* solvent[r], colloids[r] (2 FP64 beads), cells[r] (periodic), nlists[r]
+ * (2 points, stencil made) and rngs[r] (same step for every r) describe
+ * replica r after the program's set-up; their state is copied, the handles
+ * stay the caller's.  solvent_colloid / colloid_colloid are the two
+ * lj_params_t of the program. */
+int rmpcd_dimer_batch_create(rmpcd_dimer_batch **batch, int n_replicas, rmpcd_particles *const *solvent,
+                             rmpcd_particles *const *colloids, rmpcd_cells *const *cells,
+                             rmpcd_nlist *const *nlists, const rmpcd_rng *rngs,
+                             const rmpcd_lj *solvent_colloid, const rmpcd_lj *colloid_colloid,
+                             const rmpcd_dimer_params *params);
+int rmpcd_dimer_batch_destroy(rmpcd_dimer_batch *batch);
+/* n_intervals MPCD intervals of every replica */
+int rmpcd_dimer_batch_run(rmpcd_dimer_batch *batch, int n_intervals);
+/* replay a captured interval graph (1, the default) or launch the kernels
+ * one by one (0) */
+int rmpcd_dimer_batch_set_graph(rmpcd_dimer_batch *batch, int use_graph);
+/* copy replica r's state into handles shaped like the ones it came from
+ * (any of them may be NULL) */
+int rmpcd_dimer_batch_scatter(rmpcd_dimer_batch *batch, int replica, rmpcd_particles *solvent,
+                              rmpcd_particles *colloids, rmpcd_cells *cells, rmpcd_nlist *nlist,
+                              rmpcd_rng *rng);
+/* replica count, total solvent, and per replica the number of extra re-sorts
+ * (the program's n_extra_sorting; array of n_replicas, may be NULL) */
+int rmpcd_dimer_batch_info(const rmpcd_dimer_batch *batch, int *n_replicas, long long *n_solvent,
+                           int *n_extra_sorting);
+
 #ifdef __cplusplus
 }
 #endif

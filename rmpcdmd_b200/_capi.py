@@ -40,6 +40,25 @@ class RNG(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("step", C.c_uint64)]
 
 
+class DIMER_PARAMS(C.Structure):
+    """rmpcd_dimer_params: the constants of the single_dimer_pbc main loop."""
+
+    _fields_ = [
+        ("tau", C.c_double),
+        ("N_MD", C.c_int),
+        ("bond", C.c_double),
+        ("skin", C.c_double),
+        ("list_radius", C.c_double),
+        ("prob", C.c_double),
+        ("cut_sq_C", C.c_double),
+        ("cut_sq_N", C.c_double),
+        ("vv_mass", C.c_double * 2),
+        ("thermostat", C.c_int),
+        ("hydro", C.c_int),
+        ("T", C.c_double),
+    ]
+
+
 CELLS_P = c_void_p
 PART_P = c_void_p
 NL_P = c_void_p
@@ -134,6 +153,14 @@ PROTOTYPES = {
                                           C.c_double, C.c_double, C.c_double, C.c_int, c_double_p],
     "rmpcd_velocity_sums": [PART_P, c_double_p],
     "rmpcd_bulk_run": [PART_P, CELLS_P, RNG_P, C.c_double, C.c_int, C.c_double, C.c_int],
+    "rmpcd_dimer_batch_create": [C.POINTER(c_void_p), C.c_int, C.POINTER(c_void_p), C.POINTER(c_void_p),
+                                 C.POINTER(c_void_p), C.POINTER(c_void_p), RNG_P, LJ_P, LJ_P,
+                                 C.POINTER(DIMER_PARAMS)],
+    "rmpcd_dimer_batch_destroy": [c_void_p],
+    "rmpcd_dimer_batch_run": [c_void_p, C.c_int],
+    "rmpcd_dimer_batch_set_graph": [c_void_p, C.c_int],
+    "rmpcd_dimer_batch_scatter": [c_void_p, C.c_int, PART_P, PART_P, CELLS_P, NL_P, RNG_P],
+    "rmpcd_dimer_batch_info": [c_void_p, c_int_p, C.POINTER(C.c_longlong), c_int_p],
 }
 
 

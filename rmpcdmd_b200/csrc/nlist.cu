@@ -22,21 +22,6 @@ namespace rmpcd {
 
 constexpr int kNlThreads = kNlBlockThreads;
 
-static LJDev lj_dev(const rmpcd_lj *lj)
-{
-    LJDev d;
-    memset(&d, 0, sizeof(d));
-    if (!lj) return d;
-    d.n1 = lj->n1;
-    for (int i = 0; i < 16; i++) {
-        d.epsilon[i] = lj->epsilon[i];
-        d.sigma[i] = lj->sigma[i];
-        d.cut_sq[i] = lj->cut_sq[i];
-        d.cut_energy[i] = lj->cut_energy[i];
-    }
-    return d;
-}
-
 template <typename R>
 __global__ void k_update_list(Grid g, const double *cx, const double *cy, const double *cz, const int *cs,
                               const R *sx, const R *sy, const R *sz, const int *sspec, const int *count,

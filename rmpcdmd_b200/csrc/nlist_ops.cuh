@@ -3,6 +3,8 @@
 // replica engine.
 #pragma once
 
+#include <cstring>
+
 #include "keys.cuh"
 #include "rmpcd_common.cuh"
 #include "state.cuh"
@@ -16,6 +18,21 @@ struct LJDev {
     int n1;
     double epsilon[16], sigma[16], cut_sq[16], cut_energy[16];
 };
+
+inline LJDev lj_dev(const rmpcd_lj *lj)
+{
+    LJDev d;
+    memset(&d, 0, sizeof(d));
+    if (!lj) return d;
+    d.n1 = lj->n1;
+    for (int i = 0; i < 16; i++) {
+        d.epsilon[i] = lj->epsilon[i];
+        d.sigma[i] = lj->sigma[i];
+        d.cut_sq[i] = lj->cut_sq[i];
+        d.cut_energy[i] = lj->cut_energy[i];
+    }
+    return d;
+}
 
 // x**3 = x*(x*x), x**6 = x**3 * x**3 (gfortran's constant-power expansion)
 __device__ inline double cube(double x) { return x * (x * x); }

@@ -6,7 +6,7 @@
 
 namespace rmpcd {
 
-constexpr int kSmallSegment = 64;
+constexpr int kSmallSegment = kSmallSegmentMax;
 
 // key[i] = slot of particle i; histogram with one atomic per distinct key
 // per warp (consecutive particles usually share a cell).
@@ -243,6 +243,12 @@ static int gather_t(rmpcd_particles *p)
         }
     }
     return RMPCD_OK;
+}
+
+void launch_segsort_big(const int *start, const int *count, const int *big, const int *n_big, int *perm,
+                        int *tmp, cudaStream_t st)
+{
+    k_segsort_big<<<64, 512, 0, st>>>(start, count, big, n_big, perm, tmp);
 }
 
 int gather_all(rmpcd_particles *p)

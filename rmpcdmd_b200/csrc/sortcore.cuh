@@ -29,5 +29,11 @@ int build_perm(rmpcd_cells *c, rmpcd_particles *p);
 int gather_all(rmpcd_particles *p);
 // full sort
 int sort_particles(rmpcd_cells *c, rmpcd_particles *p);
+// ascending merge sort of the *n_big queued cells big[] of more than 64
+// particles (tmp: scratch of the extent of perm)
+void launch_segsort_big(const int *start, const int *count, const int *big, const int *n_big, int *perm,
+                        int *tmp, cudaStream_t st);
+// largest cell handled by sort_segment; larger ones go to launch_segsort_big
+constexpr int kSmallSegmentMax = 64;
 
 }  // namespace rmpcd

@@ -3,6 +3,8 @@ accelerates, written against the C ABI exactly as the Fortran programs call
 their modules:
 
   * :class:`SingleDimerPBC` -- programs/single_dimer_pbc.f90:108-445
+  * :class:`DimerBatch`     -- that program's main loop for many replicas at
+                               once (one launch per phase, graph-replayed)
   * :func:`bulk_fluid`      -- the loop of test/setup_bulk_decay.f90:99-121
 
 The randomness differs from the reference only in its source (Philox keyed
@@ -12,9 +14,12 @@ same numbers.
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 
 from . import api as A
+from ._capi import DIMER_PARAMS, RNG, call, lib
 
 PI_SP = float(np.float32(3.14159265))  # the default-real constant of the program
 TWO_SIXTH = 2.0 ** (1.0 / 6.0)
@@ -150,6 +155,77 @@ class SingleDimerPBC:
         kin = (self.mass[0] * (cv[0] ** 2).sum() + self.mass[1] * (cv[1] ** 2).sum()) / 2 + vs[0] / 2
         vcom = (vs[1:] + self.mass[0] * cv[0] + self.mass[1] * cv[1]) / (self.N + self.mass[0] + self.mass[1])
         return dict(temperature=te, kinetic=kin, v_com=vcom, n_solvent=A.n_solvent(self.solvent, 2))
+
+
+class DimerBatch:
+    """Many independent :class:`SingleDimerPBC` systems advanced together by
+    ``rmpcd_dimer_batch_run``: each interval is one captured CUDA graph whose
+    kernels cover every replica.  The drivers passed in provide the set-up
+    (positions, velocities, sort, list, initial forces); :meth:`scatter` copies
+    a replica back into its driver's handles, after which the driver's own
+    methods (observables, further intervals) continue from there.
+
+    All drivers must share N_MD, tau, the dimer and the LJ tables, start at the
+    same RNG step and use the same solvent precision; boxes and seeds may differ.
+    """
+
+    def __init__(self, dimers, use_graph: bool = True):
+        self.dimers = list(dimers)
+        d0 = self.dimers[0]
+        R = len(self.dimers)
+        prm = DIMER_PARAMS()
+        prm.tau, prm.N_MD, prm.bond, prm.skin = d0.tau, d0.N_MD, d0.d, d0.skin
+        prm.list_radius = d0.max_cut + d0.skin
+        prm.prob = d0.prob
+        prm.cut_sq_C, prm.cut_sq_N = float(d0.cut_sq[0, 0]), float(d0.cut_sq[0, 1])
+        prm.vv_mass[0], prm.vv_mass[1] = float(d0.mass[0]), float(d0.mass[1])
+        prm.thermostat, prm.hydro, prm.T = int(bool(d0.do_thermostat)), int(bool(d0.do_hydro)), float(d0.T)
+        for d in self.dimers:
+            if d.N_MD != d0.N_MD or d.tau != d0.tau or d.bulk_rmpcd:
+                raise ValueError("DimerBatch: replicas must share N_MD and tau and use refuel")
+        def hv(xs):
+            return (C.c_void_p * R)(*[x.handle.value for x in xs])
+
+        self._extra0 = [d.n_extra_sorting for d in self.dimers]
+        rngs = (RNG * R)(*[RNG(d.rng.seed, d.rng.step) for d in self.dimers])
+        self._h = C.c_void_p()
+        call("rmpcd_dimer_batch_create", C.byref(self._h), R, hv([d.solvent for d in self.dimers]),
+             hv([d.colloids for d in self.dimers]), hv([d.cells for d in self.dimers]),
+             hv([d.neigh for d in self.dimers]), rngs, C.byref(d0.solvent_colloid_lj.struct),
+             C.byref(d0.colloid_lj.struct), C.byref(prm))
+        call("rmpcd_dimer_batch_set_graph", self._h, int(bool(use_graph)))
+        self.R = R
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().rmpcd_dimer_batch_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @property
+    def n_solvent(self) -> int:
+        n = C.c_longlong()
+        call("rmpcd_dimer_batch_info", self._h, None, C.byref(n), None)
+        return int(n.value)
+
+    def run(self, n_intervals: int) -> None:
+        call("rmpcd_dimer_batch_run", self._h, int(n_intervals))
+
+    def n_extra_sorting(self) -> np.ndarray:
+        out = np.zeros(self.R, np.int32)
+        call("rmpcd_dimer_batch_info", self._h, None, None, out.ctypes.data_as(C.POINTER(C.c_int)))
+        return out
+
+    def scatter(self, r: int, dimer: SingleDimerPBC | None = None) -> SingleDimerPBC:
+        """Copy replica r into the handles of ``dimer`` (its own driver by default)."""
+        d = dimer if dimer is not None else self.dimers[r]
+        call("rmpcd_dimer_batch_scatter", self._h, int(r), d.solvent.handle, d.colloids.handle, d.cells.handle,
+             d.neigh.handle, d.rng.ptr)
+        d.n_extra_sorting = self._extra0[r] + int(self.n_extra_sorting()[r])
+        return d
 
 
 def bulk_fluid(L, rho=10, T=1.0 / 3.0, tau=1.0, n_intervals=200, seed=1, precision=A.FP64, alpha=None):
