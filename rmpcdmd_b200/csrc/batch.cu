@@ -8,14 +8,19 @@
 // Hilbert order stays inside its own range, so the sort kernels of a single
 // system apply to every replica at once.
 //
-// The extra re-sort that single_dimer_pbc performs when a particle moved too
-// far (programs/single_dimer_pbc.f90:320-330) is decided on the device: the
-// colloid kernel writes one flag per replica and every re-sort kernel skips
-// the tiles of replicas whose flag is clear.  The re-sort gathers into the
-// alternate buffers and copies back, so the arrays never change place and a
-// whole interval (N_MD MD steps + shift + sort + collision + refuel) can be
-// captured once in a CUDA graph and replayed: the RNG step and the grid
-// origins are read from device memory, never baked into the graph.
+// One MD step is three kernels plus a conditional re-sort: the step-begin
+// kernel (md_pos, flag roll, displacement; its last block runs every
+// replica's colloid half and the program's re-sort test,
+// programs/single_dimer_pbc.f90:306-330), the pair-force kernel, the kernel
+// applying the pair forces, and the step-end kernel (md_vel, change_species,
+// colloid velocity half).  The re-sort is decided on the device: one flag per
+// replica, and in a captured graph an IF node whose body (the re-sort
+// kernels, which skip the tiles of unflagged replicas) runs only when some
+// replica needs it.  The re-sort gathers into the alternate buffers and
+// copies back, so the arrays never change place and a whole interval (N_MD MD
+// steps + shift + sort + collision + refuel) is captured once and replayed:
+// the RNG step and the grid origins are read from device memory, never baked
+// into the graph.
 //
 // Arithmetic per particle is that of the single-system kernels
 // (stepops.cuh, nlist_ops.cuh), so replica r reproduces, bit for bit, the
@@ -72,6 +77,9 @@ struct rmpcd_dimer_batch {
     rmpcd::BTile *ptile = nullptr, *stile = nullptr;
     int n_ptile = 0, n_stile = 0;
     int *stile_first = nullptr, *stile_count = nullptr;  // per replica
+    int *ptile_first = nullptr, *ptile_count = nullptr;  // per replica
+    int *act_p = nullptr, *act_s = nullptr, *n_act = nullptr;  // tiles of the replicas flagged for a re-sort
+    int *all_p = nullptr, *all_s = nullptr, *n_all = nullptr;  // every tile
     long long *tile_sum = nullptr, *tile_off = nullptr;  // per slot tile
     int *count = nullptr, *start = nullptr, *cursor = nullptr;
     unsigned char *is_md = nullptr, *is_reac = nullptr;
@@ -92,7 +100,11 @@ struct rmpcd_dimer_batch {
     rmpcd::Masses ms{};
     rmpcd::LJDev lj_sc{}, lj_cc{};
     int parity = 0;  // 0: force = buffer force[0], force_old = force_old[0]; swapped by each MD step
+    unsigned *done = nullptr;   // blocks finished in the current step kernel (last-block hand-off)
     bool use_graph = true;
+    bool capturing = false;
+    cudaError_t cap_err = cudaSuccess;
+    cudaStream_t body = nullptr;  // captures the bodies of the re-sort IF nodes
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
 };
 
@@ -136,57 +148,183 @@ __device__ inline PView<R> shifted(PView<R> v, long long off, int n)
     return v;
 }
 
-__device__ inline bool tile_active(const BTile &t, const int *flag)
-{
-    return !flag || flag[t.r];
-}
+// the tiles a re-sort kernel visits: tiles[ids[k]] for k < *n (every tile
+// for the interval's sort, the flagged replicas' tiles for an MD step's)
+struct TileSet {
+    const BTile *tiles;
+    const int *ids;
+    const int *n;
+};
 
 // ------------------------------------------------------------ MD step
+//
+// Force entries that can be non-zero are known from the flags: MD set means
+// the particle received a contribution in the last force evaluation (its
+// `force` entry), PAST_MD in the one before (`force_old`).  Every other entry
+// is exactly zero, so the MD-step kernels neither read nor clear it; the
+// arithmetic uses a zero in its place and stays that of md_pos / md_vel.
 
-// md_pos + the PAST_MD/MD flag roll of compute_force + the solvent's
-// maximum displacement (src/md.f90:61-77, src/neighbor_list.f90:180-188,
-// src/particle_system.f90:357-378)
+__device__ inline bool same_bits(float a, float b) { return __float_as_int(a) == __float_as_int(b); }
+__device__ inline bool same_bits(double a, double b) { return __double_as_longlong(a) == __double_as_longlong(b); }
+
 template <typename R>
-__global__ void __launch_bounds__(kBT) kb_md_pos(const BTile *tiles, PView<R> v, Vec3<R> old, R dt, R dt_sq,
-                                                 unsigned long long *so_max)
+__device__ inline R flagged(const R *a, long long i, bool set)
 {
-    const BTile t = tiles[blockIdx.x];
-    double m = 0;
-    for (long long i = t.begin + threadIdx.x; i < t.end; i += blockDim.x) {
-        md_pos_one(v, i, dt, dt_sq);
-        flag_roll_one(v.flags, i);
-        double r = disp_sq_one(v.pos, old, v.species, i);
-        m = m > r ? m : r;
-    }
-    m = warp_max(m);
-    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(so_max + t.r, m);
+    return set ? a[i] : (R)0;
 }
 
 // colloid position half, RATTLE, colloid displacement and the re-sort
-// decision of programs/single_dimer_pbc.f90:311-330 (one thread per replica)
-__global__ void kb_colloid_pos(int R, const BRep *rep, PView<double> c, Vec3<double> cold, double *rx, double *ry,
-                               double *rz, const double *mass, Masses ms, double d, double dt, double skin,
-                               unsigned long long *so_max, int *resort, int *n_extra, unsigned *err)
+// decision of replica r (programs/single_dimer_pbc.f90:311-330); clears the
+// colloid force entries that become `force` after switch_force
+__device__ inline int colloid_begin(int r, const BRep *rep, const PView<double> &c, const Vec3<double> &cold,
+                                    const Vec3<double> &c_next, double *const rat[3], const double *mass,
+                                    const Masses &ms, double d, double dt, double skin, unsigned long long *so_max,
+                                    int *resort, int *n_extra, unsigned *err)
 {
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
-        PView<double> cr = shifted(c, 2 * (long long)r, 2);
-        for (int k = 0; k < 2; k++) {
-            rx[2 * r + k] = cr.pos.x[k];
-            ry[2 * r + k] = cr.pos.y[k];
-            rz[2 * r + k] = cr.pos.z[k];
+    PView<double> cr = shifted(c, 2 * (long long)r, 2);
+    for (int k = 0; k < 2; k++) {
+        rat[0][2 * r + k] = cr.pos.x[k];
+        rat[1][2 * r + k] = cr.pos.y[k];
+        rat[2][2 * r + k] = cr.pos.z[k];
+    }
+    colloid_vv_pos_one(cr, 0, mass[2 * r], dt);
+    colloid_vv_pos_one(cr, 1, mass[2 * r + 1], dt);
+    E3 L{{rep[r].g.edges[0], rep[r].g.edges[1], rep[r].g.edges[2]}};
+    rattle_pos_dimer(cr, rat[0] + 2 * r, rat[1] + 2 * r, rat[2] + 2 * r, ms, d, dt, L, err);
+    Vec3<double> o = {cold.x + 2 * r, cold.y + 2 * r, cold.z + 2 * r};
+    double m0 = disp_sq_one(cr.pos, o, cr.species, 0), m1 = disp_sq_one(cr.pos, o, cr.species, 1);
+    double co_max = sqrt(m0 > m1 ? m0 : m1);
+    double so = sqrt(__longlong_as_double((long long)__ldcg(so_max + r)));
+    int need = (co_max >= skin * 0.1) || (so >= skin * 0.89);
+    resort[r] = need;
+    if (need) n_extra[r] += 1;
+    so_max[r] = 0;
+    for (int k = 2 * r; k < 2 * r + 2; k++) c_next.x[k] = c_next.y[k] = c_next.z[k] = 0;
+    return need;
+}
+
+struct ColloidStep {
+    PView<double> c;       // colloids, force/force_old of this step
+    Vec3<double> cold;     // colloid pos_old
+    Vec3<double> c_next;   // colloid force entries cleared for the next evaluation
+    double *rat[3];        // pos_rattle
+    const double *mass;    // velocity-Verlet masses, 2 per replica
+    Masses ms;
+    double d, dt, skin;
+    int R;
+};
+
+// exclusive block scan of one int per thread; *total gets the block's sum
+// (ws: kBT / 32 + 1 ints of shared memory)
+__device__ inline int block_excl_scan(int v, int *ws, int *total)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int inc = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) ws[w] = inc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int k = 0; k < kBT / 32; k++) {
+            int y = ws[k];
+            ws[k] = acc;
+            acc += y;
         }
-        colloid_vv_pos_one(cr, 0, mass[2 * r], dt);
-        colloid_vv_pos_one(cr, 1, mass[2 * r + 1], dt);
-        E3 L{{rep[r].g.edges[0], rep[r].g.edges[1], rep[r].g.edges[2]}};
-        rattle_pos_dimer(cr, rx + 2 * r, ry + 2 * r, rz + 2 * r, ms, d, dt, L, err);
-        Vec3<double> o = {cold.x + 2 * r, cold.y + 2 * r, cold.z + 2 * r};
-        double m0 = disp_sq_one(cr.pos, o, cr.species, 0), m1 = disp_sq_one(cr.pos, o, cr.species, 1);
-        double co_max = sqrt(m0 > m1 ? m0 : m1);
-        double so = sqrt(__longlong_as_double((long long)so_max[r]));
-        int need = (co_max >= skin * 0.1) || (so >= skin * 0.89);
-        resort[r] = need;
-        if (need) n_extra[r] += 1;
-        so_max[r] = 0;
+        ws[kBT / 32] = acc;
+    }
+    __syncthreads();
+    int ex = ws[w] + inc - v;
+    *total = ws[kBT / 32];
+    __syncthreads();
+    return ex;
+}
+
+// the tile lists of the replicas flagged for a re-sort
+struct ResortLists {
+    const int *pfirst, *pcount, *sfirst, *scount;  // per replica
+    int *pids, *sids;                              // out: active particle / slot tiles
+    int *n;                                        // out: n[0] particle tiles, n[1] slot tiles
+};
+
+// md_pos of every solvent particle, the PAST_MD/MD roll of compute_force,
+// clearing of the entries that become `force` after switch_force and the
+// solvent's maximum displacement (src/md.f90:61-77,
+// src/neighbor_list.f90:180-188, src/particle_system.f90:357-378); the last
+// block to finish runs the colloid half for every replica, the program's
+// re-sort test, lists the tiles of the replicas to re-sort and raises the
+// graph's re-sort condition when there are any
+template <typename R>
+__global__ void __launch_bounds__(kBT, 6)
+    kb_step_begin(const BTile *tiles, const BRep *rep, PView<R> v, Vec3<R> old, Vec3<R> next, R dt, R dt_sq,
+                  unsigned long long *so_max, unsigned *done, int *resort, int *n_extra, ColloidStep cs,
+                  ResortLists rl, cudaGraphConditionalHandle cond, int use_cond, unsigned *err)
+{
+    __shared__ int s_last;
+    __shared__ int ws[kBT / 32 + 1];
+    __shared__ double s_max[kBT / 32];
+    const BTile t = tiles[blockIdx.x];
+    double m = 0;
+    for (long long i = t.begin + threadIdx.x; i < t.end; i += blockDim.x) {
+        const int f = v.flags[i];
+        const int sp = v.species[i];
+        R px = v.pos.x[i], py = v.pos.y[i], pz = v.pos.z[i];
+        const R vx = v.vel.x[i], vy = v.vel.y[i], vz = v.vel.z[i];
+        const R ox = old.x[i], oy = old.y[i], oz = old.z[i];
+        const bool md = (f >> MD_BIT) & 1, past = (f >> PAST_MD_BIT) & 1;
+        const R fx = flagged(v.force.x, i, md), fy = flagged(v.force.y, i, md), fz = flagged(v.force.z, i, md);
+        px = px + dt * vx + dt_sq * fx;
+        py = py + dt * vy + dt_sq * fy;
+        pz = pz + dt * vz + dt_sq * fz;
+        v.pos.x[i] = px;
+        v.pos.y[i] = py;
+        v.pos.z[i] = pz;
+        if (past) next.x[i] = next.y[i] = next.z[i] = 0;
+        if (md || past) flag_roll_one(v.flags, i);
+        if (sp >= 0) {
+            double d0 = (double)px - (double)ox, d1 = (double)py - (double)oy, d2 = (double)pz - (double)oz;
+            double r = d0 * d0 + d1 * d1 + d2 * d2;
+            m = m > r ? m : r;
+        }
+    }
+    m = warp_max(m);
+    if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kBT / 32; w++) m = m > s_max[w] ? m : s_max[w];
+        // one atomic per block, skipped when it cannot raise the maximum
+        if (m > __longlong_as_double((long long)__ldcg(so_max + t.r))) atomic_max_nonneg(so_max + t.r, m);
+        __threadfence();
+        s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    int any = 0, base_p = 0, base_s = 0;
+    for (int r0 = 0; r0 < cs.R; r0 += blockDim.x) {
+        const int r = r0 + threadIdx.x;
+        int need = 0;
+        if (r < cs.R)
+            need = colloid_begin(r, rep, cs.c, cs.cold, cs.c_next, cs.rat, cs.mass, cs.ms, cs.d, cs.dt, cs.skin, so_max,
+                                 resort, n_extra, err);
+        any |= need;
+        const int np = need ? rl.pcount[r] : 0, ns = need ? rl.scount[r] : 0;
+        int tp, ts;
+        const int ep = base_p + block_excl_scan(np, ws, &tp);
+        const int es = base_s + block_excl_scan(ns, ws, &ts);
+        for (int k = 0; k < np; k++) rl.pids[ep + k] = rl.pfirst[r] + k;
+        for (int k = 0; k < ns; k++) rl.sids[es + k] = rl.sfirst[r] + k;
+        base_p += tp;
+        base_s += ts;
+    }
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) {
+        rl.n[0] = base_p;
+        rl.n[1] = base_s;
+        if (use_cond && any) cudaGraphSetConditional(cond, 1);
+        *done = 0;
     }
 }
 
@@ -213,94 +351,140 @@ __global__ void kb_pair_forces(const BRep *rep, PView<double> c, PView<R> s, con
     }
 }
 
+// the three consumers of the pair forces, on disjoint data: solvent
+// particles with one contribution, those with several (per replica, in
+// order), and the ordered colloid sums
 template <typename R>
-__global__ void kb_apply_single(const int *list, const int *n, int Nmax, const unsigned char *contrib,
-                                const double *pf, const int *ncontrib, R *fx, R *fy, R *fz)
+__global__ void kb_apply_sum(const BRep *rep, int R_, int gx, const int *list, const int *n, int Nmax,
+                             const unsigned char *contrib, const double *pf, const int *ncontrib,
+                             const int *max_contrib, R *fx, R *fy, R *fz, double *cfx, double *cfy, double *cfz,
+                             int *clist, int *cn)
 {
-    const int i = blockIdx.y;
-    const int ni = n[i];
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ni; e += gridDim.x * blockDim.x)
-        apply_single_entry((size_t)i * Nmax + e, list, contrib, pf, ncontrib, fx, fy, fz);
-}
-
-template <typename R>
-__global__ void kb_apply_multi(const BRep *rep, const int *list, const int *n, int Nmax, const unsigned char *contrib,
-                               const double *pf, const int *ncontrib, const int *max_contrib, R *fx, R *fy, R *fz)
-{
-    const int r = blockIdx.x;
-    if (max_contrib[r] < 2) return;
-    const size_t q0 = (size_t)2 * r * Nmax;
-    apply_multi_block(list + q0, n + 2 * r, 2, Nmax, contrib + q0, pf + 3 * q0, ncontrib, rep[r].serial, fx, fy, fz);
-}
-
-__global__ void kb_colloid_sum(const int *n, int Nmax, const unsigned char *contrib, const double *pf, double *cfx,
-                               double *cfy, double *cfz, int *clist, int *cn)
-{
-    colloid_sum_block(blockIdx.x, n, Nmax, contrib, pf, cfx, cfy, cfz, clist, cn);
-}
-
-__global__ void kb_reset_contrib(const int *list, const int *n, int Nmax, const unsigned char *contrib,
-                                 int *ncontrib, int *max_contrib)
-{
-    const int i = blockIdx.y;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n[i]; e += gridDim.x * blockDim.x) {
-        size_t q = (size_t)i * Nmax + e;
-        if (contrib[q]) ncontrib[list[q]] = 0;
+    const int b = blockIdx.x;
+    const int n_single = gx * 2 * R_;
+    if (b < n_single) {
+        const int i = b / gx, bx = b % gx;
+        for (int e = bx * blockDim.x + threadIdx.x; e < n[i]; e += gx * blockDim.x)
+            apply_single_entry((size_t)i * Nmax + e, list, contrib, pf, ncontrib, fx, fy, fz);
+    } else if (b < n_single + R_) {
+        const int r = b - n_single;
+        if (max_contrib[r] < 2) return;
+        const size_t q0 = (size_t)2 * r * Nmax;
+        apply_multi_block(list + q0, n + 2 * r, 2, Nmax, contrib + q0, pf + 3 * q0, ncontrib, rep[r].serial, fx, fy,
+                          fz);
+    } else {
+        colloid_sum_block(b - n_single - R_, n, Nmax, contrib, pf, cfx, cfy, cfz, clist, cn);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0 && (i & 1) == 0) max_contrib[i >> 1] = 0;
 }
 
-// compute_force_n2, colloid velocity half and RATTLE velocity correction
-// (src/neighbor_list.f90:227-264, programs/single_dimer_pbc.f90:356-359,
-// src/md.f90:298-319), one thread per replica
-__global__ void kb_colloid_vel(int R, const BRep *rep, PView<double> c, const double *mass, Masses ms, LJDev lj,
-                               double d, double dt, unsigned *err)
+// md_vel then change_species of every solvent particle (src/md.f90:219-237,
+// programs/single_dimer_pbc.f90:511-542); clearing of the per-particle
+// contribution counters; compute_force_n2, the colloid velocity half and
+// RATTLE's velocity correction per replica (src/neighbor_list.f90:227-264,
+// programs/single_dimer_pbc.f90:356-359, src/md.f90:298-319)
+template <typename R>
+__global__ void __launch_bounds__(kBT, 6)
+    kb_step_end(const BTile *tiles, int n_tiles, int gx, const BRep *rep, PView<R> v, PView<double> c, R dt,
+                double cut_c, double cut_n, double prob, const uint64_t *d_step, int step_off, const int *list,
+                const int *n, int Nmax, const unsigned char *contrib, int *ncontrib, int *max_contrib,
+                ColloidStep cs, LJDev lj_cc, unsigned *err)
 {
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
+    const int b = blockIdx.x;
+    if (b < n_tiles) {
+        const BTile t = tiles[b];
+        const BRep &rp = rep[t.r];
+        const double a[3] = {c.pos.x[2 * t.r], c.pos.y[2 * t.r], c.pos.z[2 * t.r]};
+        const double bb[3] = {c.pos.x[2 * t.r + 1], c.pos.y[2 * t.r + 1], c.pos.z[2 * t.r + 1]};
+        const double L0 = rp.g.edges[0], L1 = rp.g.edges[1], L2 = rp.g.edges[2];
+        const uint64_t step = *d_step + (uint64_t)step_off;
+        const uint64_t seed = rp.seed;
+        const long long off = rp.off;
+        for (long long i = t.begin + threadIdx.x; i < t.end; i += blockDim.x) {
+            int f = v.flags[i];
+            const R vx = v.vel.x[i], vy = v.vel.y[i], vz = v.vel.z[i];
+            if (!((f >> WALL_BIT) & 1)) {
+                const bool md = (f >> MD_BIT) & 1, past = (f >> PAST_MD_BIT) & 1;
+                if (md || past) {
+                    R f0 = flagged(v.force.x, i, md), f1 = flagged(v.force.y, i, md), f2 = flagged(v.force.z, i, md);
+                    R g0 = flagged(v.force_old.x, i, past), g1 = flagged(v.force_old.y, i, past),
+                      g2 = flagged(v.force_old.z, i, past);
+                    v.vel.x[i] = vx + dt * (f0 + g0) / 2;
+                    v.vel.y[i] = vy + dt * (f1 + g1) / 2;
+                    v.vel.z[i] = vz + dt * (f2 + g2) / 2;
+                } else {
+                    // both forces are zero: the update changes a velocity
+                    // only if it is -0, so the store is kept for that case
+                    const R z = 0;
+                    const R nx = vx + dt * (z + z) / 2, ny = vy + dt * (z + z) / 2, nz = vz + dt * (z + z) / 2;
+                    if (!same_bits(nx, vx) || !same_bits(ny, vy) || !same_bits(nz, vz)) {
+                        v.vel.x[i] = nx;
+                        v.vel.y[i] = ny;
+                        v.vel.z[i] = nz;
+                    }
+                }
+            } else {
+                v.flags[i] = f & ~(1 << WALL_BIT);
+                f = f & ~(1 << WALL_BIT);
+            }
+            if ((f >> REAC_BIT) & 1)
+                change_species_one(v, i, i - off, a, bb, L0, L1, L2, cut_c, cut_n, prob, seed, step);
+        }
+        return;
+    }
+    const int n_reset = gx * 2 * cs.R;
+    if (b < n_tiles + n_reset) {
+        const int q = b - n_tiles, i = q / gx, bx = q % gx;
+        for (int e = bx * blockDim.x + threadIdx.x; e < n[i]; e += gx * blockDim.x) {
+            size_t qq = (size_t)i * Nmax + e;
+            if (contrib[qq]) ncontrib[list[qq]] = 0;
+        }
+        if (bx == 0 && threadIdx.x == 0 && (i & 1) == 0) max_contrib[i >> 1] = 0;
+        return;
+    }
+    for (int r = (b - n_tiles - n_reset) * blockDim.x + threadIdx.x; r < cs.R;
+         r += (gridDim.x - n_tiles - n_reset) * blockDim.x) {
         PView<double> cr = shifted(c, 2 * (long long)r, 2);
         const double *e = rep[r].g.edges;
         for (int m = 0; m < 2; m++)
-            force_n2_one(m, cr.pos.x, cr.pos.y, cr.pos.z, cr.species, 2, e[0], e[1], e[2], lj, cr.force.x,
+            force_n2_one(m, cr.pos.x, cr.pos.y, cr.pos.z, cr.species, 2, e[0], e[1], e[2], lj_cc, cr.force.x,
                          cr.force.y, cr.force.z);
-        colloid_vv_vel_one(cr, 0, mass[2 * r], dt);
-        colloid_vv_vel_one(cr, 1, mass[2 * r + 1], dt);
+        colloid_vv_vel_one(cr, 0, cs.mass[2 * r], cs.dt);
+        colloid_vv_vel_one(cr, 1, cs.mass[2 * r + 1], cs.dt);
         E3 L{{e[0], e[1], e[2]}};
-        rattle_vel_dimer(cr, ms, d, L, err);
-    }
-}
-
-// md_vel then change_species of every solvent particle
-// (src/md.f90:219-237, programs/single_dimer_pbc.f90:511-542)
-template <typename R>
-__global__ void __launch_bounds__(kBT)
-    kb_md_vel_species(const BTile *tiles, const BRep *rep, PView<R> v, PView<double> c, R dt, double cut_c,
-                      double cut_n, double prob, const uint64_t *d_step, int step_off)
-{
-    const BTile t = tiles[blockIdx.x];
-    const BRep &rp = rep[t.r];
-    const double a[3] = {c.pos.x[2 * t.r], c.pos.y[2 * t.r], c.pos.z[2 * t.r]};
-    const double b[3] = {c.pos.x[2 * t.r + 1], c.pos.y[2 * t.r + 1], c.pos.z[2 * t.r + 1]};
-    const double L0 = rp.g.edges[0], L1 = rp.g.edges[1], L2 = rp.g.edges[2];
-    const uint64_t step = *d_step + (uint64_t)step_off;
-    const uint64_t seed = rp.seed;
-    const long long off = rp.off;
-    for (long long i = t.begin + threadIdx.x; i < t.end; i += blockDim.x) {
-        md_vel_one(v, i, dt);
-        change_species_one(v, i, i - off, a, b, L0, L1, L2, cut_c, cut_n, prob, seed, step);
+        rattle_vel_dimer(cr, cs.ms, cs.d, L, err);
     }
 }
 
 // ------------------------------------------------------ re-sort / sort
 
-__global__ void kb_zero_slots(const BTile *tiles, const int *flag, int *count, unsigned char *is_md,
-                              unsigned char *is_reac)
+// count = 0, is_md = 0, is_reac = 1 over the active replicas' slots; block 0
+// also clears the big-cell queue and, for the interval's sort, draws every
+// replica's grid shift (random_shift, src/cell_system.f90:153-163)
+__global__ void kb_zero_slots(TileSet ts, int *count, unsigned char *is_md,
+                              unsigned char *is_reac, int *n_big, int R, BRep *rep, const uint64_t *d_step,
+                              int shift_step_off)
 {
-    const BTile t = tiles[blockIdx.x];
-    if (!tile_active(t, flag)) return;
-    for (long long s = t.begin + threadIdx.x; s < t.end; s += blockDim.x) {
-        count[s] = 0;
-        is_md[s] = 0;
-        is_reac[s] = 1;
+    if (blockIdx.x == 0) {
+        if (threadIdx.x == 0) *n_big = 0;
+        if (shift_step_off >= 0) {
+            const uint64_t step = *d_step + (uint64_t)shift_step_off;
+            for (int r = threadIdx.x; r < R; r += blockDim.x) {
+                double u0, u1, u2, u3;
+                rng::uniform2(rep[r].seed, step, 0, rng::SHIFT, 0, u0, u1);
+                rng::uniform2(rep[r].seed, step, 1, rng::SHIFT, 0, u2, u3);
+                rep[r].g.origin[0] = u0 - 1;
+                rep[r].g.origin[1] = u1 - 1;
+                rep[r].g.origin[2] = u2 - 1;
+            }
+        }
+    }
+    for (int k = blockIdx.x; k < *ts.n; k += gridDim.x) {
+        const BTile t = ts.tiles[ts.ids[k]];
+        for (long long s = t.begin + threadIdx.x; s < t.end; s += blockDim.x) {
+            count[s] = 0;
+            is_md[s] = 0;
+            is_reac[s] = 1;
+        }
     }
 }
 
@@ -308,24 +492,25 @@ __global__ void kb_zero_slots(const BTile *tiles, const int *flag, int *count, u
 // particle's slot, histogram with one atomic per distinct key per warp
 template <typename R>
 __global__ void __launch_bounds__(kBT)
-    kb_pbc_key_count(const BTile *tiles, const int *flag, const BRep *rep, PView<R> v, int *key, int *count)
+    kb_pbc_key_count(TileSet ts, const BRep *rep, PView<R> v, int *key, int *count)
 {
-    const BTile t = tiles[blockIdx.x];
-    if (!tile_active(t, flag)) return;
-    const BRep &rp = rep[t.r];
-    const Grid g = rp.g;
     const int lane = threadIdx.x & 31;
-    for (long long base = t.begin; base < t.end; base += blockDim.x) {
-        long long i = base + threadIdx.x;
-        bool ok = i < t.end;
-        int k = -1;
-        if (ok) {
-            apply_pbc_one(v, i, g.edges[0], g.edges[1], g.edges[2]);
-            k = rp.soff + slot_of(g, (double)v.pos.x[i], (double)v.pos.y[i], (double)v.pos.z[i]);
-            key[i] = k;
+    for (int kt = blockIdx.x; kt < *ts.n; kt += gridDim.x) {
+        const BTile t = ts.tiles[ts.ids[kt]];
+        const BRep &rp = rep[t.r];
+        const Grid g = rp.g;
+        for (long long base = t.begin; base < t.end; base += blockDim.x) {
+            long long i = base + threadIdx.x;
+            bool ok = i < t.end;
+            int k = -1;
+            if (ok) {
+                apply_pbc_one(v, i, g.edges[0], g.edges[1], g.edges[2]);
+                k = rp.soff + slot_of(g, (double)v.pos.x[i], (double)v.pos.y[i], (double)v.pos.z[i]);
+                key[i] = k;
+            }
+            unsigned peers = __match_any_sync(0xffffffffu, k);
+            if (ok && lane == __ffs(peers) - 1) atomicAdd(count + k, __popc(peers));
         }
-        unsigned peers = __match_any_sync(0xffffffffu, k);
-        if (ok && lane == __ffs(peers) - 1) atomicAdd(count + k, __popc(peers));
     }
 }
 
@@ -341,21 +526,23 @@ __device__ inline long long block_sum_ll(long long v)
     return s;
 }
 
-__global__ void __launch_bounds__(kBT) kb_scan_reduce(const BTile *tiles, const int *flag, const int *count,
-                                                      long long *tile_sum)
+__global__ void __launch_bounds__(kBT) kb_scan_reduce(TileSet ts, const int *count, long long *tile_sum)
 {
-    const BTile t = tiles[blockIdx.x];
-    if (!tile_active(t, flag)) return;
-    long long a = 0;
-    for (long long s = t.begin + threadIdx.x; s < t.end; s += blockDim.x) a += count[s];
-    long long tot = block_sum_ll(a);
-    if (threadIdx.x == 0) tile_sum[blockIdx.x] = tot;
+    for (int k = blockIdx.x; k < *ts.n; k += gridDim.x) {
+        const int id = ts.ids[k];
+        const BTile t = ts.tiles[id];
+        long long a = 0;
+        for (long long s = t.begin + threadIdx.x; s < t.end; s += blockDim.x) a += count[s];
+        long long tot = block_sum_ll(a);
+        if (threadIdx.x == 0) tile_sum[id] = tot;
+        __syncthreads();
+    }
 }
 
-// tile offsets of every active replica: its first particle + the sums of
-// its earlier tiles
+// tile offsets of every active replica (its first particle + the sums of
+// its earlier tiles); the replica's colloids get apply_pbc and pos_old = pos
 __global__ void kb_scan_reps(int R, const int *flag, const BRep *rep, const int *first, const int *ntiles,
-                             const long long *tile_sum, long long *tile_off)
+                             const long long *tile_sum, long long *tile_off, PView<double> c, Vec3<double> cold)
 {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
         if (flag && !flag[r]) continue;
@@ -364,163 +551,159 @@ __global__ void kb_scan_reps(int R, const int *flag, const BRep *rep, const int 
             tile_off[first[r] + k] = acc;
             acc += tile_sum[first[r] + k];
         }
-    }
-}
-
-// start = cursor = exclusive scan inside the tile + the tile's offset
-__global__ void __launch_bounds__(kBT) kb_scan_apply(const BTile *tiles, const int *flag, const int *count,
-                                                     const long long *tile_off, int *start, int *cursor)
-{
-    __shared__ long long ws[kBT / 32 + 1];
-    const BTile t = tiles[blockIdx.x];
-    if (!tile_active(t, flag)) return;
-    constexpr int PER = kTile / kBT;
-    const long long b = t.begin + (long long)threadIdx.x * PER;
-    int v[PER];
-    long long sum = 0;
-#pragma unroll
-    for (int k = 0; k < PER; k++) {
-        v[k] = b + k < t.end ? count[b + k] : 0;
-        sum += v[k];
-    }
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    long long inc = sum;
-    for (int o = 1; o < 32; o <<= 1) {
-        long long y = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += y;
-    }
-    if (lane == 31) ws[w] = inc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        long long acc = 0;
-        for (int k = 0; k < kBT / 32; k++) {
-            long long y = ws[k];
-            ws[k] = acc;
-            acc += y;
-        }
-    }
-    __syncthreads();
-    long long run = tile_off[blockIdx.x] + ws[w] + inc - sum;
-#pragma unroll
-    for (int k = 0; k < PER; k++) {
-        if (b + k < t.end) {
-            start[b + k] = (int)run;
-            cursor[b + k] = (int)run;
-        }
-        run += v[k];
-    }
-}
-
-// place every particle inside its cell (in-cell order fixed by kb_segsort)
-__global__ void __launch_bounds__(kBT) kb_perm(const BTile *tiles, const int *flag, const int *key, int *cursor,
-                                               int *perm)
-{
-    const BTile t = tiles[blockIdx.x];
-    if (!tile_active(t, flag)) return;
-    const int lane = threadIdx.x & 31;
-    const unsigned lt = lanemask_lt();
-    for (long long base = t.begin; base < t.end; base += blockDim.x) {
-        long long i = base + threadIdx.x;
-        int k = i < t.end ? key[i] : -1;
-        unsigned peers = __match_any_sync(0xffffffffu, k);
-        int b = 0;
-        if (k >= 0 && lane == __ffs(peers) - 1) b = atomicAdd(cursor + k, __popc(peers));
-        b = __shfl_sync(0xffffffffu, b, __ffs(peers) - 1);
-        if (k >= 0) perm[b + __popc(peers & lt)] = (int)i;
-    }
-}
-
-__global__ void kb_segsort(const BTile *tiles, const int *flag, const int *count, const int *start, int *perm,
-                           int *big, int *n_big)
-{
-    const BTile t = tiles[blockIdx.x];
-    if (!tile_active(t, flag)) return;
-    for (long long s = t.begin + threadIdx.x; s < t.end; s += blockDim.x) {
-        int n = count[s];
-        if (n <= 1) continue;
-        if (n > kSmallSegmentMax) {
-            int q = atomicAdd(n_big, 1);
-            big[q] = (int)s;
-            continue;
-        }
-        sort_segment(perm + start[s], n);
-    }
-}
-
-template <typename R>
-__global__ void __launch_bounds__(kBT)
-    kb_gather(const BTile *tiles, const int *flag, PView<R> s, PView<R> d, const int *perm)
-{
-    const BTile t = tiles[blockIdx.x];
-    if (!tile_active(t, flag)) return;
-    for (long long j = t.begin + threadIdx.x; j < t.end; j += blockDim.x) {
-        const int i = perm[j];
-        R px = s.pos.x[i], py = s.pos.y[i], pz = s.pos.z[i];
-        R vx = s.vel.x[i], vy = s.vel.y[i], vz = s.vel.z[i];
-        R fx = s.force.x[i], fy = s.force.y[i], fz = s.force.z[i];
-        R gx = s.force_old.x[i], gy = s.force_old.y[i], gz = s.force_old.z[i];
-        int ix = s.ix[i], iy = s.iy[i], iz = s.iz[i];
-        int id = s.id[i], sp = s.species[i], fl = s.flags[i];
-        d.pos.x[j] = px;
-        d.pos.y[j] = py;
-        d.pos.z[j] = pz;
-        d.vel.x[j] = vx;
-        d.vel.y[j] = vy;
-        d.vel.z[j] = vz;
-        d.force.x[j] = fx;
-        d.force.y[j] = fy;
-        d.force.z[j] = fz;
-        d.force_old.x[j] = gx;
-        d.force_old.y[j] = gy;
-        d.force_old.z[j] = gz;
-        d.ix[j] = ix;
-        d.iy[j] = iy;
-        d.iz[j] = iz;
-        d.id[j] = id;
-        d.species[j] = sp;
-        d.flags[j] = fl;
-    }
-}
-
-// the sorted arrays back into place; the gathered positions stay as pos_old
-template <typename R>
-__global__ void __launch_bounds__(kBT) kb_copyback(const BTile *tiles, const int *flag, PView<R> d, PView<R> s)
-{
-    const BTile t = tiles[blockIdx.x];
-    if (!tile_active(t, flag)) return;
-    for (long long j = t.begin + threadIdx.x; j < t.end; j += blockDim.x) {
-        d.pos.x[j] = s.pos.x[j];
-        d.pos.y[j] = s.pos.y[j];
-        d.pos.z[j] = s.pos.z[j];
-        d.vel.x[j] = s.vel.x[j];
-        d.vel.y[j] = s.vel.y[j];
-        d.vel.z[j] = s.vel.z[j];
-        d.force.x[j] = s.force.x[j];
-        d.force.y[j] = s.force.y[j];
-        d.force.z[j] = s.force.z[j];
-        d.force_old.x[j] = s.force_old.x[j];
-        d.force_old.y[j] = s.force_old.y[j];
-        d.force_old.z[j] = s.force_old.z[j];
-        d.ix[j] = s.ix[j];
-        d.iy[j] = s.iy[j];
-        d.iz[j] = s.iz[j];
-        d.id[j] = s.id[j];
-        d.species[j] = s.species[j];
-        d.flags[j] = s.flags[j];
-    }
-}
-
-// apply_pbc of the colloids and pos_old = pos (one thread per replica)
-__global__ void kb_colloid_resort(int R, const int *flag, const BRep *rep, PView<double> c, Vec3<double> cold)
-{
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
-        if (flag && !flag[r]) continue;
         const double *e = rep[r].g.edges;
         for (int k = 2 * r; k < 2 * r + 2; k++) {
             apply_pbc_one(c, k, e[0], e[1], e[2]);
             cold.x[k] = c.pos.x[k];
             cold.y[k] = c.pos.y[k];
             cold.z[k] = c.pos.z[k];
+        }
+    }
+}
+
+// start = cursor = exclusive scan inside the tile + the tile's offset
+__global__ void __launch_bounds__(kBT) kb_scan_apply(TileSet ts, const int *count, const long long *tile_off,
+                                                     int *start, int *cursor)
+{
+    __shared__ long long ws[kBT / 32 + 1];
+    constexpr int PER = kTile / kBT;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int kt = blockIdx.x; kt < *ts.n; kt += gridDim.x) {
+        const int id = ts.ids[kt];
+        const BTile t = ts.tiles[id];
+        const long long b = t.begin + (long long)threadIdx.x * PER;
+        int v[PER];
+        long long sum = 0;
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            v[k] = b + k < t.end ? count[b + k] : 0;
+            sum += v[k];
+        }
+        long long inc = sum;
+        for (int o = 1; o < 32; o <<= 1) {
+            long long y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane == 31) ws[w] = inc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            long long acc = 0;
+            for (int k = 0; k < kBT / 32; k++) {
+                long long y = ws[k];
+                ws[k] = acc;
+                acc += y;
+            }
+        }
+        __syncthreads();
+        long long run = tile_off[id] + ws[w] + inc - sum;
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            if (b + k < t.end) {
+                start[b + k] = (int)run;
+                cursor[b + k] = (int)run;
+            }
+            run += v[k];
+        }
+        __syncthreads();
+    }
+}
+
+// place every particle inside its cell (in-cell order fixed by kb_segsort)
+__global__ void __launch_bounds__(kBT) kb_perm(TileSet ts, const int *key, int *cursor, int *perm)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = lanemask_lt();
+    for (int kt = blockIdx.x; kt < *ts.n; kt += gridDim.x) {
+        const BTile t = ts.tiles[ts.ids[kt]];
+        for (long long base = t.begin; base < t.end; base += blockDim.x) {
+            long long i = base + threadIdx.x;
+            int k = i < t.end ? key[i] : -1;
+            unsigned peers = __match_any_sync(0xffffffffu, k);
+            int b = 0;
+            if (k >= 0 && lane == __ffs(peers) - 1) b = atomicAdd(cursor + k, __popc(peers));
+            b = __shfl_sync(0xffffffffu, b, __ffs(peers) - 1);
+            if (k >= 0) perm[b + __popc(peers & lt)] = (int)i;
+        }
+    }
+}
+
+__global__ void kb_segsort(TileSet ts, const int *count, const int *start, int *perm, int *big, int *n_big)
+{
+    for (int kt = blockIdx.x; kt < *ts.n; kt += gridDim.x) {
+        const BTile t = ts.tiles[ts.ids[kt]];
+        for (long long s = t.begin + threadIdx.x; s < t.end; s += blockDim.x) {
+            int n = count[s];
+            if (n <= 1) continue;
+            if (n > kSmallSegmentMax) {
+                int q = atomicAdd(n_big, 1);
+                big[q] = (int)s;
+                continue;
+            }
+            sort_segment(perm + start[s], n);
+        }
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kBT) kb_gather(TileSet ts, PView<R> s, PView<R> d, const int *perm)
+{
+    for (int kt = blockIdx.x; kt < *ts.n; kt += gridDim.x) {
+        const BTile t = ts.tiles[ts.ids[kt]];
+        for (long long j = t.begin + threadIdx.x; j < t.end; j += blockDim.x) {
+            const int i = perm[j];
+            R px = s.pos.x[i], py = s.pos.y[i], pz = s.pos.z[i];
+            R vx = s.vel.x[i], vy = s.vel.y[i], vz = s.vel.z[i];
+            R fx = s.force.x[i], fy = s.force.y[i], fz = s.force.z[i];
+            R gx = s.force_old.x[i], gy = s.force_old.y[i], gz = s.force_old.z[i];
+            int ix = s.ix[i], iy = s.iy[i], iz = s.iz[i];
+            int id = s.id[i], sp = s.species[i], fl = s.flags[i];
+            d.pos.x[j] = px;
+            d.pos.y[j] = py;
+            d.pos.z[j] = pz;
+            d.vel.x[j] = vx;
+            d.vel.y[j] = vy;
+            d.vel.z[j] = vz;
+            d.force.x[j] = fx;
+            d.force.y[j] = fy;
+            d.force.z[j] = fz;
+            d.force_old.x[j] = gx;
+            d.force_old.y[j] = gy;
+            d.force_old.z[j] = gz;
+            d.ix[j] = ix;
+            d.iy[j] = iy;
+            d.iz[j] = iz;
+            d.id[j] = id;
+            d.species[j] = sp;
+            d.flags[j] = fl;
+        }
+    }
+}
+
+// the sorted arrays back into place; the gathered positions stay as pos_old
+template <typename R>
+__global__ void __launch_bounds__(kBT) kb_copyback(TileSet ts, PView<R> d, PView<R> s)
+{
+    for (int kt = blockIdx.x; kt < *ts.n; kt += gridDim.x) {
+        const BTile t = ts.tiles[ts.ids[kt]];
+        for (long long j = t.begin + threadIdx.x; j < t.end; j += blockDim.x) {
+            d.pos.x[j] = s.pos.x[j];
+            d.pos.y[j] = s.pos.y[j];
+            d.pos.z[j] = s.pos.z[j];
+            d.vel.x[j] = s.vel.x[j];
+            d.vel.y[j] = s.vel.y[j];
+            d.vel.z[j] = s.vel.z[j];
+            d.force.x[j] = s.force.x[j];
+            d.force.y[j] = s.force.y[j];
+            d.force.z[j] = s.force.z[j];
+            d.force_old.x[j] = s.force_old.x[j];
+            d.force_old.y[j] = s.force_old.y[j];
+            d.force_old.z[j] = s.force_old.z[j];
+            d.ix[j] = s.ix[j];
+            d.iy[j] = s.iy[j];
+            d.iz[j] = s.iz[j];
+            d.id[j] = s.id[j];
+            d.species[j] = s.species[j];
+            d.flags[j] = s.flags[j];
         }
     }
 }
@@ -542,39 +725,24 @@ __global__ void __launch_bounds__(kNlBlockThreads)
 
 // ------------------------------------------------------------ interval
 
-// random_shift (src/cell_system.f90:153-163) of every replica's grid
-__global__ void kb_random_shift(int R, BRep *rep, const uint64_t *d_step, int step_off)
+// simple_mpcd_step (src/mpcd.f90:71-183), one thread per slot, and refuel
+// (programs/single_dimer_pbc.f90:544-565), one thread per particle: the
+// collision writes velocities, refuel reads positions and species only
+template <typename R>
+__global__ void __launch_bounds__(kBT)
+    kb_srd_refuel(const BTile *stiles, int n_stiles, const BTile *ptiles, const BRep *rep, const int *count,
+                  const int *start, PView<R> v, PView<double> c, SrdParams q, const uint64_t *d_step, int step_off)
 {
-    const uint64_t step = *d_step + (uint64_t)step_off;
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
-        double u0, u1, u2, u3;
-        rng::uniform2(rep[r].seed, step, 0, rng::SHIFT, 0, u0, u1);
-        rng::uniform2(rep[r].seed, step, 1, rng::SHIFT, 0, u2, u3);
-        rep[r].g.origin[0] = u0 - 1;
-        rep[r].g.origin[1] = u1 - 1;
-        rep[r].g.origin[2] = u2 - 1;
+    if ((int)blockIdx.x < n_stiles) {
+        const BTile t = stiles[blockIdx.x];
+        const BRep &rp = rep[t.r];
+        q.seed = rp.seed;
+        q.step = *d_step + (uint64_t)step_off;
+        for (long long s = t.begin + threadIdx.x; s < t.end; s += blockDim.x)
+            srd_slot<R>(count[s], start[s], s - rp.soff, rp.off, v.vel.x, v.vel.y, v.vel.z, v.species, q);
+        return;
     }
-}
-
-// simple_mpcd_step (src/mpcd.f90:71-183), one thread per slot
-template <typename R>
-__global__ void __launch_bounds__(kBT) kb_srd(const BTile *tiles, const BRep *rep, const int *count, const int *start,
-                                              R *vx, R *vy, R *vz, const int *species, SrdParams q,
-                                              const uint64_t *d_step, int step_off)
-{
-    const BTile t = tiles[blockIdx.x];
-    const BRep &rp = rep[t.r];
-    q.seed = rp.seed;
-    q.step = *d_step + (uint64_t)step_off;
-    for (long long s = t.begin + threadIdx.x; s < t.end; s += blockDim.x)
-        srd_slot<R>(count[s], start[s], s - rp.soff, rp.off, vx, vy, vz, species, q);
-}
-
-// refuel (programs/single_dimer_pbc.f90:544-565)
-template <typename R>
-__global__ void __launch_bounds__(kBT) kb_refuel(const BTile *tiles, const BRep *rep, PView<R> v, PView<double> c)
-{
-    const BTile t = tiles[blockIdx.x];
+    const BTile t = ptiles[blockIdx.x - n_stiles];
     const BRep &rp = rep[t.r];
     const double a[3] = {c.pos.x[2 * t.r], c.pos.y[2 * t.r], c.pos.z[2 * t.r]};
     const double b[3] = {c.pos.x[2 * t.r + 1], c.pos.y[2 * t.r + 1], c.pos.z[2 * t.r + 1]};
@@ -615,28 +783,69 @@ static int grid_cap(long long n, int bs)
     return (int)g;
 }
 
-template <typename R>
-static void resort_launches(Batch *b, const int *flag)
+// grid of the re-sort kernels, which loop over their tile list
+static int resort_grid(int n_tiles)
 {
-    cudaStream_t st = stream();
+    int g = sm_count() * 8;
+    return n_tiles < g ? (n_tiles > 0 ? n_tiles : 1) : g;
+}
+
+// the re-sort of the flagged replicas (flag = resort flags, lists = their
+// tiles) or of every replica (flag = null, lists = all tiles)
+template <typename R>
+static void resort_launches(Batch *b, const int *flag, bool all, cudaStream_t st, int shift_step_off)
+{
     PView<R> cur = phys<R>(b->sol, 0), alt = phys<R>(b->sol, 1);
     PView<double> cv = phys<double>(b->col, 0), ca = phys<double>(b->col, 1);
-    kb_zero_slots<<<b->n_stile, kBT, 0, st>>>(b->stile, flag, b->count, b->is_md, b->is_reac);
-    kb_pbc_key_count<R><<<b->n_ptile, kBT, 0, st>>>(b->ptile, flag, b->rep, cur, b->sol->key, b->count);
-    kb_scan_reduce<<<b->n_stile, kBT, 0, st>>>(b->stile, flag, b->count, b->tile_sum);
+    TileSet pts{b->ptile, all ? b->all_p : b->act_p, all ? b->n_all : b->n_act};
+    TileSet sts{b->stile, all ? b->all_s : b->act_s, (all ? b->n_all : b->n_act) + 1};
+    const int gp = resort_grid(b->n_ptile), gs = resort_grid(b->n_stile);
+    kb_zero_slots<<<gs, kBT, 0, st>>>(sts, b->count, b->is_md, b->is_reac, b->n_big, b->R, b->rep, b->d_step,
+                                      shift_step_off);
+    kb_pbc_key_count<R><<<gp, kBT, 0, st>>>(pts, b->rep, cur, b->sol->key, b->count);
+    kb_scan_reduce<<<gs, kBT, 0, st>>>(sts, b->count, b->tile_sum);
     kb_scan_reps<<<grid_cap(b->R, 128), 128, 0, st>>>(b->R, flag, b->rep, b->stile_first, b->stile_count, b->tile_sum,
-                                                      b->tile_off);
-    kb_scan_apply<<<b->n_stile, kBT, 0, st>>>(b->stile, flag, b->count, b->tile_off, b->start, b->cursor);
-    kb_perm<<<b->n_ptile, kBT, 0, st>>>(b->ptile, flag, b->sol->key, b->cursor, b->sol->perm);
-    cudaMemsetAsync(b->n_big, 0, sizeof(int), st);
-    kb_segsort<<<b->n_stile, kBT, 0, st>>>(b->stile, flag, b->count, b->start, b->sol->perm, b->big, b->n_big);
+                                                      b->tile_off, cv, ca.pos);
+    kb_scan_apply<<<gs, kBT, 0, st>>>(sts, b->count, b->tile_off, b->start, b->cursor);
+    kb_perm<<<gp, kBT, 0, st>>>(pts, b->sol->key, b->cursor, b->sol->perm);
+    kb_segsort<<<gs, kBT, 0, st>>>(sts, b->count, b->start, b->sol->perm, b->big, b->n_big);
     launch_segsort_big(b->start, b->count, b->big, b->n_big, b->sol->perm, b->sol->key, st);
-    kb_gather<R><<<b->n_ptile, kBT, 0, st>>>(b->ptile, flag, cur, alt, b->sol->perm);
-    kb_copyback<R><<<b->n_ptile, kBT, 0, st>>>(b->ptile, flag, cur, alt);
-    kb_colloid_resort<<<grid_cap(b->R, 128), 128, 0, st>>>(b->R, flag, b->rep, cv, ca.pos);
+    kb_gather<R><<<gp, kBT, 0, st>>>(pts, cur, alt, b->sol->perm);
+    kb_copyback<R><<<gp, kBT, 0, st>>>(pts, cur, alt);
     kb_update_list<R><<<2 * b->R, kNlBlockThreads, 0, st>>>(
         flag, b->rep, cv, cur, b->count, b->start, b->stencil, b->n_stencil, b->prm.list_radius * b->prm.list_radius,
         b->lj_sc, b->Nmax, b->list, b->nn, b->is_md, b->is_reac, dev_error_word());
+}
+
+static void note(Batch *b, cudaError_t e)
+{
+    if (e != cudaSuccess && b->cap_err == cudaSuccess) b->cap_err = e;
+}
+
+// the program's re-sort test, as an IF node of the graph being captured on
+// st whose body is the re-sort of the flagged replicas; cond was created
+// before the kernel that sets it was captured
+template <typename R>
+static void capture_conditional_resort(Batch *b, cudaStream_t st, cudaGraph_t g, cudaGraphConditionalHandle cond)
+{
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    note(b, cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &nd));
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    note(b, cudaGraphAddNode(&node, g, deps, nd, &cp));
+    if (b->cap_err != cudaSuccess) return;
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    note(b, cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    note(b, cudaStreamBeginCaptureToGraph(b->body, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    resort_launches<R>(b, b->resort, false, b->body, -1);
+    cudaGraph_t out = nullptr;
+    note(b, cudaStreamEndCapture(b->body, &out));
 }
 
 template <typename R>
@@ -649,35 +858,39 @@ static void md_step_launches(Batch *b, int k)
     PView<double> c = live<double>(b->col, b->parity);
     PView<R> alt = phys<R>(b->sol, 1);
     PView<double> ca = phys<double>(b->col, 1);
-    kb_md_pos<R><<<b->n_ptile, kBT, 0, st>>>(b->ptile, s, alt.pos, (R)dt, (R)dt_sq, b->so_max);
-    kb_colloid_pos<<<grid_cap(b->R, 128), 128, 0, st>>>(b->R, b->rep, c, ca.pos, b->rattle[0], b->rattle[1],
-                                                        b->rattle[2], b->vv_mass, b->ms, b->prm.bond, dt, b->prm.skin,
-                                                        b->so_max, b->resort, b->n_extra, dev_error_word());
-    resort_launches<R>(b, b->resort);
-    // switch_force + zero_force of both systems
+    ColloidStep cs{c, ca.pos, c.force_old, {b->rattle[0], b->rattle[1], b->rattle[2]}, b->vv_mass, b->ms,
+                   b->prm.bond, dt, b->prm.skin, b->R};
+    cudaGraphConditionalHandle cond = 0;
+    cudaGraph_t g = nullptr;
+    if (b->capturing) {
+        cudaStreamCaptureStatus st_cap;
+        note(b, cudaStreamGetCaptureInfo(st, &st_cap, nullptr, &g, nullptr, nullptr));
+        note(b, cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
+    }
+    kb_step_begin<R><<<b->n_ptile, kBT, 0, st>>>(b->ptile, b->rep, s, alt.pos, s.force_old, (R)dt, (R)dt_sq,
+                                                 b->so_max, b->done, b->resort, b->n_extra, cs,
+                                                 ResortLists{b->ptile_first, b->ptile_count, b->stile_first,
+                                                             b->stile_count, b->act_p, b->act_s, b->n_act},
+                                                 cond, b->capturing ? 1 : 0, dev_error_word());
+    if (b->capturing) capture_conditional_resort<R>(b, st, g, cond);
+    else resort_launches<R>(b, b->resort, false, st, -1);
+    // switch_force: the cleared entries become `force`
     b->parity ^= 1;
     s = live<R>(b->sol, b->parity);
     c = live<double>(b->col, b->parity);
-    for (int q = 0; q < 3; q++) {
-        cudaMemsetAsync(s.force[q], 0, (size_t)b->Ntot * sizeof(R), st);
-        cudaMemsetAsync(c.force[q], 0, (size_t)2 * b->R * sizeof(double), st);
-    }
+    cs.c = c;
     int gx = (b->Nmax + 255) / 256;
     if (gx > 64) gx = 64;
-    dim3 lg(gx, 2 * b->R);
-    kb_pair_forces<R><<<lg, 256, 0, st>>>(b->rep, c, s, b->list, b->nn, b->Nmax, b->lj_sc, b->pair_f, b->pair_e,
-                                          b->contrib, b->ncontrib, b->max_contrib, b->prm.cut_sq_C);
-    kb_apply_single<R><<<lg, 256, 0, st>>>(b->list, b->nn, b->Nmax, b->contrib, b->pair_f, b->ncontrib, s.force.x,
-                                           s.force.y, s.force.z);
-    kb_apply_multi<R><<<b->R, 256, 0, st>>>(b->rep, b->list, b->nn, b->Nmax, b->contrib, b->pair_f, b->ncontrib,
-                                            b->max_contrib, s.force.x, s.force.y, s.force.z);
-    kb_colloid_sum<<<2 * b->R, kNlBlockThreads, 0, st>>>(b->nn, b->Nmax, b->contrib, b->pair_f, c.force.x, c.force.y,
-                                                         c.force.z, b->clist, b->cn);
-    kb_reset_contrib<<<lg, 256, 0, st>>>(b->list, b->nn, b->Nmax, b->contrib, b->ncontrib, b->max_contrib);
-    kb_colloid_vel<<<grid_cap(b->R, 128), 128, 0, st>>>(b->R, b->rep, c, b->vv_mass, b->ms, b->lj_cc, b->prm.bond, dt,
-                                                        dev_error_word());
-    kb_md_vel_species<R><<<b->n_ptile, kBT, 0, st>>>(b->ptile, b->rep, s, c, (R)dt, b->prm.cut_sq_C, b->prm.cut_sq_N,
-                                                     b->prm.prob, b->d_step, k);
+    kb_pair_forces<R><<<dim3(gx, 2 * b->R), 256, 0, st>>>(b->rep, c, s, b->list, b->nn, b->Nmax, b->lj_sc, b->pair_f,
+                                                          b->pair_e, b->contrib, b->ncontrib, b->max_contrib,
+                                                          b->prm.cut_sq_C);
+    kb_apply_sum<R><<<gx * 2 * b->R + 3 * b->R, 256, 0, st>>>(
+        b->rep, b->R, gx, b->list, b->nn, b->Nmax, b->contrib, b->pair_f, b->ncontrib, b->max_contrib, s.force.x,
+        s.force.y, s.force.z, c.force.x, c.force.y, c.force.z, b->clist, b->cn);
+    const int n_col_blocks = (b->R + kBT - 1) / kBT;
+    kb_step_end<R><<<b->n_ptile + gx * 2 * b->R + n_col_blocks, kBT, 0, st>>>(
+        b->ptile, b->n_ptile, gx, b->rep, s, c, (R)dt, b->prm.cut_sq_C, b->prm.cut_sq_N, b->prm.prob, b->d_step, k,
+        b->list, b->nn, b->Nmax, b->contrib, b->ncontrib, b->max_contrib, cs, b->lj_cc, dev_error_word());
 }
 
 template <typename R>
@@ -686,18 +899,16 @@ static void interval_launches(Batch *b)
     cudaStream_t st = stream();
     const int N_MD = b->prm.N_MD;
     for (int k = 0; k < N_MD; k++) md_step_launches<R>(b, k);
-    kb_random_shift<<<grid_cap(b->R, 128), 128, 0, st>>>(b->R, b->rep, b->d_step, N_MD);
-    resort_launches<R>(b, nullptr);
+    resort_launches<R>(b, nullptr, true, st, N_MD);
     SrdParams q{};
     q.sin_a = 1;
     q.cos_a = 0;
     q.thermostat = b->prm.thermostat ? 1 : 0;
     q.hydro = b->prm.hydro ? 1 : 0;
     q.t_factor = b->prm.thermostat ? sqrt(b->prm.T) : 0.0;
-    PView<R> s = live<R>(b->sol, b->parity);
-    kb_srd<R><<<b->n_stile, kBT, 0, st>>>(b->stile, b->rep, b->count, b->start, s.vel.x, s.vel.y, s.vel.z, s.species,
-                                          q, b->d_step, N_MD + 1);
-    kb_refuel<R><<<b->n_ptile, kBT, 0, st>>>(b->ptile, b->rep, s, live<double>(b->col, b->parity));
+    kb_srd_refuel<R><<<b->n_stile + b->n_ptile, kBT, 0, st>>>(b->stile, b->n_stile, b->ptile, b->rep, b->count, b->start,
+                                                              live<R>(b->sol, b->parity), live<double>(b->col, b->parity),
+                                                              q, b->d_step, N_MD + 1);
     kb_advance<<<1, 1, 0, st>>>(b->d_step, (uint64_t)N_MD + 2);
 }
 
@@ -714,14 +925,19 @@ static int run_t(Batch *b, int n_intervals)
             const int p0 = b->parity;
             if (!b->exec[p0]) {
                 cudaGraph_t g = nullptr;
+                b->cap_err = cudaSuccess;
                 RMPCD_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                b->capturing = true;
                 interval_launches<R>(b);
+                b->capturing = false;
                 cudaError_t e = cudaStreamEndCapture(st, &g);
-                if (e != cudaSuccess) return fail(RMPCD_ERR_CUDA, "interval capture: %s", cudaGetErrorString(e));
-                e = cudaGraphInstantiate(&b->exec[p0], g, 0);
-                cudaGraphDestroy(g);
+                if (e == cudaSuccess && b->cap_err != cudaSuccess) e = b->cap_err;
+                if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec[p0], g, 0);
+                if (g) cudaGraphDestroy(g);
                 if (e != cudaSuccess) {
                     b->exec[p0] = nullptr;
+                    b->parity = p0;
+                    cudaGetLastError();
                     return fail(RMPCD_ERR_CUDA, "interval graph: %s", cudaGetErrorString(e));
                 }
             } else {
@@ -740,12 +956,14 @@ static void free_batch(Batch *b)
     cudaStreamSynchronize(stream());
     for (auto &e : b->exec)
         if (e) cudaGraphExecDestroy(e);
+    if (b->body) cudaStreamDestroy(b->body);
     rmpcd_particles_destroy(b->sol);
     rmpcd_particles_destroy(b->col);
     void *ptrs[] = {b->rep, b->ptile, b->stile, b->stile_first, b->stile_count, b->tile_sum, b->tile_off, b->count,
                     b->start, b->cursor, b->is_md, b->is_reac, b->stencil, b->list, b->nn, b->pair_f, b->pair_e,
                     b->contrib, b->ncontrib, b->max_contrib, b->clist, b->cn, b->so_max, b->resort, b->n_extra,
-                    b->big, b->n_big, b->rattle[0], b->rattle[1], b->rattle[2], b->vv_mass, b->d_step};
+                    b->big, b->n_big, b->rattle[0], b->rattle[1], b->rattle[2], b->vv_mass, b->d_step, b->done,
+                    b->ptile_first, b->ptile_count, b->act_p, b->act_s, b->n_act, b->all_p, b->all_s, b->n_all};
     for (void *q : ptrs) cudaFree(q);
     for (int *l : b->luts) cudaFree(l);
     delete b;
@@ -844,7 +1062,7 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
     for (int s = 0; s < RMPCD_MAX_SPECIES; s++) b->ms.m[s] = col[0]->mass[s];
     // replica layout and tiles
     std::vector<BTile> pt, stl;
-    std::vector<int> sfirst(R), scount(R);
+    std::vector<int> sfirst(R), scount(R), pfirst(R), pcount(R);
     std::map<std::vector<int>, int *> lut_of;
     b->rep_h.resize(R);
     long long off = 0;
@@ -876,7 +1094,9 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
             lut_of[key] = l;
         }
         p.g.lut = lut_of[key];
+        pfirst[r] = (int)pt.size();
         for (long long t = 0; t < p.n; t += kTile) pt.push_back({r, 0, off + t, off + (t + kTile < p.n ? t + kTile : p.n)});
+        pcount[r] = (int)pt.size() - pfirst[r];
         sfirst[r] = (int)stl.size();
         for (long long t = 0; t < p.S; t += kTile) stl.push_back({r, 0, soff + t, soff + (t + kTile < p.S ? t + kTile : p.S)});
         scount[r] = (int)stl.size() - sfirst[r];
@@ -902,7 +1122,11 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
               !dalloc(&b->cn, 2 * (size_t)R) && !dalloc(&b->so_max, R) && !dalloc(&b->resort, R) &&
               !dalloc(&b->n_extra, R) && !dalloc(&b->big, soff) && !dalloc(&b->n_big, 1) &&
               !dalloc(&b->rattle[0], 2 * (size_t)R) && !dalloc(&b->rattle[1], 2 * (size_t)R) &&
-              !dalloc(&b->rattle[2], 2 * (size_t)R) && !dalloc(&b->vv_mass, 2 * (size_t)R) && !dalloc(&b->d_step, 1);
+              !dalloc(&b->rattle[2], 2 * (size_t)R) && !dalloc(&b->vv_mass, 2 * (size_t)R) && !dalloc(&b->d_step, 1) &&
+              !dalloc(&b->done, 1) && cudaStreamCreateWithFlags(&b->body, cudaStreamNonBlocking) == cudaSuccess &&
+              !dalloc(&b->ptile_first, R) && !dalloc(&b->ptile_count, R) && !dalloc(&b->act_p, pt.size()) &&
+              !dalloc(&b->act_s, stl.size()) && !dalloc(&b->n_act, 2) && !dalloc(&b->all_p, pt.size()) &&
+              !dalloc(&b->all_s, stl.size()) && !dalloc(&b->n_all, 2);
     if (!ok) {
         free_batch(b);
         return RMPCD_ERR_CUDA;
@@ -923,6 +1147,16 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
     RMPCD_CUDA_TRY(cudaMemcpyAsync(b->stile, stl.data(), stl.size() * sizeof(BTile), cudaMemcpyHostToDevice, st));
     RMPCD_CUDA_TRY(cudaMemcpyAsync(b->stile_first, sfirst.data(), R * sizeof(int), cudaMemcpyHostToDevice, st));
     RMPCD_CUDA_TRY(cudaMemcpyAsync(b->stile_count, scount.data(), R * sizeof(int), cudaMemcpyHostToDevice, st));
+    RMPCD_CUDA_TRY(cudaMemcpyAsync(b->ptile_first, pfirst.data(), R * sizeof(int), cudaMemcpyHostToDevice, st));
+    RMPCD_CUDA_TRY(cudaMemcpyAsync(b->ptile_count, pcount.data(), R * sizeof(int), cudaMemcpyHostToDevice, st));
+    std::vector<int> ids_p(pt.size()), ids_s(stl.size());
+    for (size_t k = 0; k < ids_p.size(); k++) ids_p[k] = (int)k;
+    for (size_t k = 0; k < ids_s.size(); k++) ids_s[k] = (int)k;
+    const int n_all[2] = {(int)pt.size(), (int)stl.size()}, n_none[2] = {0, 0};
+    RMPCD_CUDA_TRY(cudaMemcpyAsync(b->all_p, ids_p.data(), ids_p.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    RMPCD_CUDA_TRY(cudaMemcpyAsync(b->all_s, ids_s.data(), ids_s.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    RMPCD_CUDA_TRY(cudaMemcpyAsync(b->n_all, n_all, sizeof(n_all), cudaMemcpyHostToDevice, st));
+    RMPCD_CUDA_TRY(cudaMemcpyAsync(b->n_act, n_none, sizeof(n_none), cudaMemcpyHostToDevice, st));
     RMPCD_CUDA_TRY(cudaMemcpyAsync(b->vv_mass, vm.data(), vm.size() * sizeof(double), cudaMemcpyHostToDevice, st));
     RMPCD_CUDA_TRY(cudaMemcpyAsync(b->d_step, &b->step, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
     RMPCD_CUDA_TRY(cudaMemsetAsync(b->ncontrib, 0, (size_t)off * sizeof(int), st));
@@ -930,6 +1164,7 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
     RMPCD_CUDA_TRY(cudaMemsetAsync(b->so_max, 0, (size_t)R * sizeof(unsigned long long), st));
     RMPCD_CUDA_TRY(cudaMemsetAsync(b->n_extra, 0, (size_t)R * sizeof(int), st));
     RMPCD_CUDA_TRY(cudaMemsetAsync(b->resort, 0, (size_t)R * sizeof(int), st));
+    RMPCD_CUDA_TRY(cudaMemsetAsync(b->done, 0, sizeof(unsigned), st));
     d2d(b->stencil, nl[0]->stencil, 3 * (size_t)b->n_stencil * sizeof(int));
     for (int r = 0; r < R; r++) {
         const BRep &p = b->rep_h[r];
