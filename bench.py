@@ -172,6 +172,104 @@ def roofline(N, S, precision, phase, peak, peak_kind):
             "avg_launch_ms": round(avg * 1e3, 4), "launches": calls}
 
 
+# single_dimer_pbc configurations (MD step = tau / N_MD = 0.01)
+DIMER_N_MD = 100
+DIMER_LIST_CAPACITY = 4000
+# HBM bytes per solvent particle and MD step of the two streaming kernels of
+# the dimer engine (step begin: flags, species, pos r/w, vel, pos_old; step
+# end: flags, vel; force entries are touched only for flagged particles)
+DIMER_BYTES_PER_MD_STEP = {32: 72, 64: 132}
+
+
+def dimer_boxes_batched(n=512, seed=2024):
+    r = np.random.default_rng(seed)
+    return [(int(s),) * 3 for s in r.choice([16, 20, 24, 32, 40, 48], size=n)]
+
+
+def dimer_time(rm, dimers, n_intervals, use_graph=True):
+    """Device time (ms) of n_intervals of a DimerBatch built from `dimers`,
+    after one warm-up interval (which also captures the interval graph)."""
+    from rmpcdmd_b200.programs import DimerBatch
+    from rmpcdmd_b200._capi import call
+    import ctypes as C
+
+    b = DimerBatch(dimers, use_graph=use_graph)
+    b.run(1)
+    rm.synchronize()
+    a, e = C.c_int(), C.c_int()
+    call("rmpcd_mark", C.byref(a))
+    b.run(n_intervals)
+    call("rmpcd_mark", C.byref(e))
+    rm.synchronize()
+    ms = C.c_float()
+    call("rmpcd_elapsed_ms", a, e, C.byref(ms))
+    extra = int(b.n_extra_sorting().sum())
+    return float(ms.value), b.n_solvent, extra
+
+
+def dimer_entry(N, ms, n_intervals, precision, peak, peak_kind, extra=None):
+    md_steps = n_intervals * DIMER_N_MD
+    secs = ms * 1e-3
+    alg = DIMER_BYTES_PER_MD_STEP[precision] * N * md_steps
+    achieved = alg / secs / 1e9
+    out = {"value": N * md_steps / secs, "us_per_md_step": round(ms * 1e3 / md_steps, 2), "intervals": n_intervals,
+           "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind,
+                        "unit": "GB/s", "frac": round(achieved / peak, 4),
+                        "algorithmic_bytes_per_particle_md_step": DIMER_BYTES_PER_MD_STEP[precision],
+                        "note": "streaming bytes of the MD step over the whole interval time (sort, list and "
+                                "collision included in the time only)"}}
+    if extra is not None:
+        out["n_extra_sorting"] = extra
+    return out
+
+
+def run_dimer(rm, peak, peak_kind, local):
+    """single_dimer_pbc through the batched engine: one dimer at 32^3 (plain
+    FP64, and the call-by-call driver for comparison), one at 96^3 (FP32
+    solvent and FP64), and 512 replicas with uneven boxes (FP32 solvent)."""
+    from rmpcdmd_b200.programs import SingleDimerPBC
+
+    def make(boxes, seeds, precision):
+        return [SingleDimerPBC(L=L, rho=RHO, N_MD=DIMER_N_MD, seed=s, list_capacity=DIMER_LIST_CAPACITY,
+                               precision=precision) for L, s in zip(boxes, seeds)]
+
+    out = {"unit": "particle-steps/s (solvent particles x MD steps / device time, dt = tau/N_MD = 0.01)",
+           "data": "synthetic: seeded uniform solvent (rejected inside the colloid cut), Maxwell kT=1/3, "
+                   "dimer sigma=2, d=4.5, p(A->B)=1, refuel beyond 0.45 L; list capacity 4000"}
+    ms, N, ex = dimer_time(rm, make([(32, 32, 32)], [SEED], 64), 5)
+    out["single_dimer_32_fp64_plain"] = dict(dimer_entry(N, ms, 5, 64, peak, peak_kind, ex), N=N, replicas=1)
+    d = make([(32, 32, 32)], [SEED], 64)[0]
+    d.interval()
+    rm.synchronize()
+    t0 = time.perf_counter()
+    d.interval()
+    rm.synchronize()
+    cbc = time.perf_counter() - t0
+    out["single_dimer_32_fp64_call_by_call"] = {"value": N * DIMER_N_MD / cbc,
+                                                "us_per_md_step": round(cbc * 1e6 / DIMER_N_MD, 2),
+                                                "path": "one C-ABI call per module procedure (wall clock)"}
+    for prec in (32, 64):
+        ms, N, ex = dimer_time(rm, make([(96, 96, 96)], [SEED], prec), 2)
+        out[f"single_dimer_96_fp{prec}"] = dict(dimer_entry(N, ms, 2, prec, peak, peak_kind, ex), N=N, replicas=1)
+    boxes = dimer_boxes_batched()
+    with ClockSampler(local) as cs:
+        ms, N, ex = dimer_time(rm, make(boxes, list(range(1, len(boxes) + 1)), 32), 2)
+    e = dimer_entry(N, ms, 2, 32, peak, peak_kind, ex)
+    e.update(N=N, replicas=len(boxes), boxes="cubic sides drawn from {16,20,24,32,40,48}, seed 2024",
+             clocks=cs.summary())
+    # the same replicas one at a time in plain FP64 (a sample of 8)
+    seq_ms, seq_N = 0.0, 0
+    for k in range(8):
+        m1, n1, _ = dimer_time(rm, make([boxes[k]], [k + 1], 64), 1)
+        seq_ms += m1
+        seq_N += n1
+    e["fp64_plain_one_replica_at_a_time"] = {"value": seq_N * DIMER_N_MD / (seq_ms * 1e-3),
+                                             "sample": "replicas 0-7, one interval each"}
+    e["batched_over_sequential_fp64"] = round(e["value"] / e["fp64_plain_one_replica_at_a_time"]["value"], 3)
+    out["batched_512_fp32"] = e
+    return out
+
+
 def e2e_run(rm, p, cells, rng, steps):
     """The same loop through the public API with host arrays: every step
     uploads the particle arrays from page-locked host memory in the reference
@@ -313,6 +411,11 @@ def run_ours(args):
                       "steps": e2e_steps,
                       "path": "rmpcd_particles_upload x6 (pinned host, reference (3,N) layout) -> rmpcd_bulk_run(1) "
                               "-> rmpcd_particles_download x6"}
+    if not args.no_dimer:
+        for r in (r32, r64):
+            r.pop("p", None)
+            r.pop("cells", None)
+        out["dimer"] = run_dimer(rm, peak, peak_kind, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_sample()
     if rank == 0:
@@ -378,6 +481,7 @@ def main(argv=None):
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-dimer", action="store_true", help="skip the single-dimer engine configurations")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3

@@ -261,16 +261,20 @@ __device__ inline void apply_multi_block(const int *list, const int *n, int C, i
 }
 
 // f1 = sum of colloid i's pair forces in list order; force(:,i) += f1; the
-// contributing entries are compacted in order into clist (one block)
+// contributing entries are compacted in order into clist (one block).  Each
+// chunk of entries is compacted and staged in shared memory by the whole
+// block; the three components are then summed by three threads, each in
+// list order, so every sum is the sequential one.
 __device__ inline void colloid_sum_block(int i, const int *n, int Nmax, const unsigned char *contrib, const double *pf,
                                          double *cfx, double *cfy, double *cfz, int *clist, int *cn)
 {
     __shared__ int idxs[kNlBlockThreads];
+    __shared__ double vals[3][kNlBlockThreads];
     __shared__ int warp_cnt[kNlBlockThreads / 32];
     __shared__ int s_cnt;
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
     const int ni = n[i];
-    double f0 = 0, f1 = 0, f2 = 0;
+    double acc = 0;  // thread c < 3 accumulates component c
     int total = 0;
     for (int e0 = 0; e0 < ni; e0 += kNlBlockThreads) {
         int e = e0 + t;
@@ -279,34 +283,38 @@ __device__ inline void colloid_sum_block(int i, const int *n, int Nmax, const un
         if (lane == 0) warp_cnt[wid] = __popc(bal);
         __syncthreads();
         if (t == 0) {
-            int acc = 0;
+            int a = 0;
             for (int w = 0; w < kNlBlockThreads / 32; w++) {
                 int v = warp_cnt[w];
-                warp_cnt[w] = acc;
-                acc += v;
+                warp_cnt[w] = a;
+                a += v;
             }
-            s_cnt = acc;
+            s_cnt = a;
         }
         __syncthreads();
-        if (c) idxs[warp_cnt[wid] + __popc(bal & ((1u << lane) - 1u))] = e;
-        __syncthreads();
-        if (t == 0) {
-            for (int k = 0; k < s_cnt; k++) {
-                size_t q = (size_t)i * Nmax + idxs[k];
-                f0 = f0 + pf[3 * q];
-                f1 = f1 + pf[3 * q + 1];
-                f2 = f2 + pf[3 * q + 2];
-                clist[(size_t)i * Nmax + total + k] = idxs[k];
-            }
-            total += s_cnt;
+        if (c) {
+            const int k = warp_cnt[wid] + __popc(bal & ((1u << lane) - 1u));
+            const size_t q = (size_t)i * Nmax + e;
+            idxs[k] = e;
+            vals[0][k] = pf[3 * q];
+            vals[1][k] = pf[3 * q + 1];
+            vals[2][k] = pf[3 * q + 2];
         }
+        __syncthreads();
+        const int cnt = s_cnt;
+        if (t < 3)
+            for (int k = 0; k < cnt; k++) acc = acc + vals[t][k];
+        for (int k = t; k < cnt; k += kNlBlockThreads) clist[(size_t)i * Nmax + total + k] = idxs[k];
+        total += cnt;
         __syncthreads();
     }
     if (t == 0) {
-        cfx[i] = cfx[i] + f0;
-        cfy[i] = cfy[i] + f1;
-        cfz[i] = cfz[i] + f2;
+        cfx[i] = cfx[i] + acc;
         cn[i] = total;
+    } else if (t == 1) {
+        cfy[i] = cfy[i] + acc;
+    } else if (t == 2) {
+        cfz[i] = cfz[i] + acc;
     }
 }
 
