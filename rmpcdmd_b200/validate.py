@@ -1,0 +1,138 @@
+"""Statistical check of the FP32-solvent form against the plain FP64 form.
+
+The FP32 form cannot match FP64 bit for bit (positions and velocities are
+rounded to single precision, cell sums are compensated FP32 sums), so it is
+checked on the quantities the physics fixes, each run in both precisions from
+the same seeds:
+
+* bulk SRD fluid (the loop of test/setup_bulk_decay.f90): the change of the
+  total momentum per MPCD interval relative to N * sqrt(kT) (SRD conserves
+  momentum cell by cell), the kinetic temperature, and the solvent velocity
+  autocorrelation C(t) = sum_i v_i(0).v_i(t) / sum_i v_i(0)^2;
+* single_dimer_pbc (programs/single_dimer_pbc.f90): the dimer's propulsion
+  velocity, the centre-of-mass displacement per interval projected on the
+  bond direction (catalytic minus noncatalytic bead), averaged over an
+  ensemble of replicas run by the batched engine, with its standard error.
+
+``python -m rmpcdmd_b200.validate [--quick]`` prints one JSON object.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import time
+
+import numpy as np
+
+from . import api as A
+from ._capi import call
+from .programs import DimerBatch, SingleDimerPBC
+
+KT = 1.0 / 3.0
+
+
+def _bulk(L, precision, seed, n_intervals):
+    L = [L, L, L]
+    cells = A.CellSystem(L, 1.0)
+    N = 10 * int(np.prod(L))
+    p = A.ParticleSystem(N, 1, None, precision)
+    p.random_placement(cells.edges, seed=seed)
+    p.maxwell(KT, seed)
+    p.species = 1
+    rng = A.Rng(seed)
+    cells.random_shift(rng)
+    p.sort(cells)
+    order = np.argsort(p.download("id"))
+    v0 = p.download("vel")[order]
+    norm = float((v0 * v0).sum())
+    mom, temp, vacf, ekin = [], [], [1.0], []
+    s = A.velocity_sums(p)
+    mom.append(s[1:].copy())
+    ekin.append(s[0] / 2)
+    for _ in range(n_intervals):
+        A.bulk_run(p, cells, rng, 1.0, 1)
+        s = A.velocity_sums(p)
+        mom.append(s[1:].copy())
+        ekin.append(s[0] / 2)
+        temp.append(A.compute_temperature(p, cells))
+        v = p.download("vel")[np.argsort(p.download("id"))]
+        vacf.append(float((v0 * v).sum()) / norm)
+    mom = np.array(mom)
+    scale = N * np.sqrt(KT)
+    step_drift = np.abs(np.diff(mom, axis=0)).max() / scale
+    total_drift = np.abs(mom[-1] - mom[0]).max() / scale
+    return dict(N=N, momentum_step_drift_max=float(step_drift), momentum_total_drift=float(total_drift),
+                temperature_mean=float(np.mean(temp)), temperature_std=float(np.std(temp)),
+                kinetic_energy_rel_change=float(abs(ekin[-1] - ekin[0]) / ekin[0]), vacf=vacf)
+
+
+def bulk_check(L=32, n_intervals=30, seed=7):
+    r32 = _bulk(L, A.FP32, seed, n_intervals)
+    r64 = _bulk(L, A.FP64, seed, n_intervals)
+    c32, c64 = np.array(r32.pop("vacf")), np.array(r64.pop("vacf"))
+    # statistical error of C(t) for N independent particles: ~ sqrt(1 + C^2) / sqrt(3 N)
+    err = np.sqrt((1 + c64 ** 2) / (3 * r64["N"]))
+    return dict(L=L, intervals=n_intervals, fp32=r32, fp64=r64,
+                temperature_rel_diff=(r32["temperature_mean"] - r64["temperature_mean"]) / r64["temperature_mean"],
+                vacf_max_abs_diff=float(np.abs(c32 - c64).max()), vacf_stat_err=float(err.max()),
+                vacf_fp64_first=[round(float(x), 5) for x in c64[:6]],
+                vacf_fp32_first=[round(float(x), 5) for x in c32[:6]])
+
+
+def _colloids(batch: DimerBatch, r: int):
+    d = batch.dimers[r]
+    call("rmpcd_dimer_batch_scatter", batch._h, int(r), None, d.colloids.handle, None, None, None)
+    pos = d.colloids.download("pos")
+    img = d.colloids.download("image")
+    return pos + img * d.edges
+
+
+def _propulsion(L, precision, replicas, n_intervals, skip, seed0):
+    dimers = [SingleDimerPBC(L=(L, L, L), rho=10, N_MD=100, seed=seed0 + k, list_capacity=4000,
+                             precision=precision) for k in range(replicas)]
+    b = DimerBatch(dimers)
+    prev = [_colloids(b, r) for r in range(replicas)]
+    per_rep = np.zeros((replicas, n_intervals))
+    for t in range(n_intervals):
+        b.run(1)
+        for r in range(replicas):
+            x = _colloids(b, r)
+            u = prev[r][0] - prev[r][1]
+            u = u / np.linalg.norm(u)
+            dcom = (x[0] + x[1]) / 2 - (prev[r][0] + prev[r][1]) / 2
+            per_rep[r, t] = float(dcom @ u)  # tau = 1
+            prev[r] = x
+    v = per_rep[:, skip:].mean(axis=1)
+    return dict(replicas=replicas, intervals=n_intervals, skipped=skip, v_prop=float(v.mean()),
+                v_prop_err=float(v.std(ddof=1) / np.sqrt(replicas)))
+
+
+def propulsion_check(L=32, replicas=32, n_intervals=60, skip=10, seed0=1000):
+    p32 = _propulsion(L, A.FP32, replicas, n_intervals, skip, seed0)
+    p64 = _propulsion(L, A.FP64, replicas, n_intervals, skip, seed0)
+    diff = p32["v_prop"] - p64["v_prop"]
+    err = float(np.hypot(p32["v_prop_err"], p64["v_prop_err"]))
+    return dict(L=L, fp32=p32, fp64=p64, diff=diff, diff_err=err,
+                rel_diff=diff / p64["v_prop"] if p64["v_prop"] else None,
+                rel_err=err / abs(p64["v_prop"]) if p64["v_prop"] else None)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--quick", action="store_true", help="small sizes (a minute)")
+    a = ap.parse_args(argv)
+    t0 = time.perf_counter()
+    if a.quick:
+        out = dict(bulk=bulk_check(L=24, n_intervals=20),
+                   propulsion=propulsion_check(L=16, replicas=16, n_intervals=30, skip=5))
+    else:
+        out = dict(bulk=bulk_check(L=48, n_intervals=50),
+                   propulsion=propulsion_check(L=32, replicas=64, n_intervals=200, skip=20))
+    out["seconds"] = round(time.perf_counter() - t0, 1)
+    print(json.dumps(out))
+    return out
+
+
+if __name__ == "__main__":
+    main()
