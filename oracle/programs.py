@@ -1,6 +1,7 @@
-"""Oracle twin of the program drivers (test infrastructure): the loop of
-programs/single_dimer_pbc.f90 over the oracle's C routines, consuming random
-steps in the same order as rmpcdmd_b200.programs.SingleDimerPBC."""
+"""Oracle twin of the program drivers (test infrastructure): the loops of
+programs/single_dimer_pbc.f90 and programs/n_colloids_pbc.f90 over the
+oracle's C routines, consuming random steps in the same order as
+rmpcdmd_b200.programs.SingleDimerPBC and NColloidsPBC."""
 from __future__ import annotations
 
 import numpy as np
@@ -108,3 +109,131 @@ class SingleDimerPBC:
             O.bulk_reaction(self.s, self.cells, 2, 1, self.bulk_rate, self.tau, self.seed, self._next())
         else:
             O.refuel(self.s, self.c, self.edges, int(self.L[0]))
+
+
+PI_3141 = float(np.float32(3.141))
+PI_3142 = float(np.float32(3.142))
+COLLOID_PLACE_STEP = 0xFFFFFFFFFFFFFFFF
+PLACE_STREAM = 5
+
+
+def place_colloids(seed, n, edges, min_dist):
+    """programs/n_colloids_pbc.f90:193-210 with the oracle's Philox draws."""
+    edges = np.asarray(edges, np.float64)
+    pos = np.zeros((n, 3))
+    i = k = 0
+    while i < n:
+        u0, u1 = O.rng_u2(seed, COLLOID_PLACE_STEP, k, PLACE_STREAM, 0)
+        u2, _ = O.rng_u2(seed, COLLOID_PLACE_STEP, k, PLACE_STREAM, 1)
+        k += 1
+        x = np.array([u0 * edges[0], u1 * edges[1], u2 * edges[2]])
+        ok = True
+        for j in range(i):
+            d = x - pos[j]
+            d = d - np.where(d < -edges / 2, -edges, 0) - np.where(d > edges / 2, edges, 0)
+            if float((d ** 2).sum()) < min_dist ** 2:
+                ok = False
+                break
+        if ok:
+            pos[i] = x
+            i += 1
+    return pos
+
+
+class NColloidsPBC:
+    def __init__(self, L=(32, 32, 32), rho=10, T=1.0 / 3.0, T_final=None, tau=1.0, N_MD=100, N_colloids=10,
+                 sigma=3.0, epsilon=1.0, epsilon_colloids=1.0, do_hydro=True, do_thermostat=False, seed=1,
+                 skin=0.8, list_capacity=None, volume_correction=True):
+        self.L = np.asarray(L, dtype=np.int32)
+        self.rho, self.T_init, self.tau, self.N_MD = rho, T, tau, N_MD
+        self.T_final = T if T_final is None else T_final
+        self.dt = tau / N_MD
+        self.do_hydro, self.do_thermostat = do_hydro, do_thermostat
+        self.skin, self.seed, self.step = skin, seed, 0
+        vol = int(rho * 4 * PI_3142 / 3 * sigma ** 3 * N_colloids) if volume_correction else 0
+        self.N = int(rho * int(self.L.prod())) - vol
+        self.mass = rho * sigma ** 3 * 4 * PI_3141 / 3
+        sigma_cut = sigma * 2.0 ** (1.0 / 6.0)
+        self.lj = O.LJParams([[epsilon]], [[sigma]], [[sigma_cut]])
+        self.clj = O.LJParams([[epsilon_colloids]], [[2 * sigma]], [[2 * (3 * sigma)]])
+        self.c = O.Particles(N_colloids, 1, [self.mass])
+        self.c.species[:] = 1
+        self.vv_mass = np.full(N_colloids, self.mass)
+        self.s = O.Particles(self.N, 1)
+        O.maxwell_velocities(self.s, T, seed)
+        self.s.species[:] = 1
+        self.cells = O.Cells(self.L, 1.0)
+        self.edges = self.cells.edges
+        self.c.pos[:] = place_colloids(seed, N_colloids, self.edges, 2 * sigma)
+        O.random_placement(self.s, self.edges, seed, self.c, self.lj)
+        self.s.sort(self.cells)
+        self.radius = sigma_cut + skin
+        cap = list_capacity if list_capacity is not None else int(250 * (sigma_cut + skin) ** 2)
+        self.nl = O.NeighborList(N_colloids, cap)
+        self.nl.make_stencil(self.cells, self.radius)
+        self.nl.update_list(self.c, self.s, self.radius, self.cells)
+        self.e1 = O.compute_force(self.c, self.s, self.nl, self.edges, self.lj)
+        self.e2 = O.compute_force_n2(self.c, self.edges, self.clj)
+        self.s.force_old[:] = self.s.force
+        self.c.force_old[:] = self.c.force
+        self.s.pos_old[:] = self.s.pos
+        self.c.pos_old[:] = self.c.pos
+        self.n_extra_sorting = 0
+        self.t = 0
+        self.last_sort = 0
+
+    def _next(self):
+        st = self.step
+        self.step += 1
+        return st
+
+    def _catch_up_and_sort(self):
+        s, c, dtl = self.s, self.c, (self.t - self.last_sort) * self.dt
+        O.cell_md_pos(self.cells, s, dtl, False)
+        O.cell_md_vel(self.cells, s, dtl, False)
+        O.apply_pbc(s, self.edges)
+        O.apply_pbc(c, self.edges)
+        s.sort(self.cells)
+        self.last_sort = self.t
+        self.nl.update_list(c, s, self.radius, self.cells)
+        s.pos_old[:] = s.pos
+        c.pos_old[:] = c.pos
+
+    def md_step(self):
+        s, c, dt = self.s, self.c, self.dt
+        self.t += 1
+        O.cell_md_pos(self.cells, s, dt, True)
+        O.colloid_vv_pos(c, dt, self.vv_mass)
+        so_max = O.cell_maximum_displacement(self.cells, s, dt * (self.t - self.last_sort))
+        co_max = c.maximum_displacement()
+        if (co_max >= self.skin * 0.1) or (so_max >= self.skin * 0.9):
+            self._catch_up_and_sort()
+            self.n_extra_sorting += 1
+        s.switch_force()
+        c.switch_force()
+        s.force[:] = 0
+        c.force[:] = 0
+        self.e1 = O.compute_force(c, s, self.nl, self.edges, self.lj)
+        self.e2 = O.compute_force_n2(c, self.edges, self.clj)
+        O.cell_md_vel(self.cells, s, dt, True)
+        O.colloid_vv_vel(c, dt, self.vv_mass)
+
+    def interval(self, thermostat, T, rescale=False):
+        for _ in range(self.N_MD):
+            self.md_step()
+        self.cells.random_shift(self.seed, self._next())
+        self._catch_up_and_sort()
+        O.simple_mpcd_step(self.s, self.cells, self.seed, self._next(), thermostat=thermostat, T=T,
+                           hydro=self.do_hydro)
+        if rescale:
+            O.rescale_cells(self.s, self.cells, self.T_init)
+
+    def thermalise(self, n_loops):
+        for i in range(1, n_loops + 1):
+            self.interval(True, self.T_init, rescale=(i % 10 == 0))
+        self.t = self.last_sort = 0
+
+    def run(self, n_loops):
+        for i in range(1, n_loops + 1):
+            T = self.T_init + (i - 1) * (self.T_final - self.T_init) / max(1, n_loops - 1)
+            self.interval(self.do_thermostat, T)

@@ -5,6 +5,7 @@ their modules:
   * :class:`SingleDimerPBC` -- programs/single_dimer_pbc.f90:108-445
   * :class:`DimerBatch`     -- that program's main loop for many replicas at
                                once (one launch per phase, graph-replayed)
+  * :class:`NColloidsPBC`   -- programs/n_colloids_pbc.f90:147-336
   * :func:`bulk_fluid`      -- the loop of test/setup_bulk_decay.f90:99-121
 
 The randomness differs from the reference only in its source (Philox keyed
@@ -226,6 +227,148 @@ class DimerBatch:
              d.neigh.handle, d.rng.ptr)
         d.n_extra_sorting = self._extra0[r] + int(self.n_extra_sorting()[r])
         return d
+
+
+PI_3141 = float(np.float32(3.141))  # default-real constants of n_colloids_pbc
+PI_3142 = float(np.float32(3.142))
+COLLOID_PLACE_STEP = 0xFFFFFFFFFFFFFFFF  # RNG step of the colloid placement draws
+PLACE_STREAM = 5
+
+
+def place_colloids(uniform2, seed, n, edges, min_dist):
+    """Uniform colloid positions with the program's rejection of pairs closer
+    than min_dist (programs/n_colloids_pbc.f90:193-210).  Attempt k draws
+    uniform2(seed, COLLOID_PLACE_STEP, k, PLACE, 0) for x, y and (.., 1) for z."""
+    edges = np.asarray(edges, np.float64)
+    pos = np.zeros((n, 3))
+    i = k = 0
+    while i < n:
+        u0, u1 = uniform2(seed, COLLOID_PLACE_STEP, k, PLACE_STREAM, 0)
+        u2, _ = uniform2(seed, COLLOID_PLACE_STEP, k, PLACE_STREAM, 1)
+        k += 1
+        x = np.array([u0 * edges[0], u1 * edges[1], u2 * edges[2]])
+        ok = True
+        for j in range(i):
+            d = x - pos[j]
+            d = d - np.where(d < -edges / 2, -edges, 0) - np.where(d > edges / 2, edges, 0)
+            if float((d ** 2).sum()) < min_dist ** 2:
+                ok = False
+                break
+        if ok:
+            pos[i] = x
+            i += 1
+    return pos
+
+
+class NColloidsPBC:
+    """programs/n_colloids_pbc.f90 on the GPU: passive LJ colloids in an SRD
+    fluid with lazy, cell-wise solvent streaming.  Only the solvent in cells
+    flagged by the neighbor list (is_md) is advanced every MD step; the other
+    cells are streamed in one step of the accumulated time before each sort.
+
+    ``volume_correction`` subtracts the colloid volume from the solvent count
+    as the program does (N = rho L^3 - int(rho 4*3.142/3 sigma^3 N_colloids)).
+    """
+
+    def __init__(self, L=(32, 32, 32), rho=10, T=1.0 / 3.0, T_final=None, tau=1.0, N_MD=100, N_colloids=10,
+                 sigma=3.0, epsilon=1.0, epsilon_colloids=1.0, do_hydro=True, do_thermostat=False, seed=1,
+                 skin=0.8, list_capacity=None, precision=A.FP64, volume_correction=True):
+        self.L = np.asarray(L, dtype=np.int32)
+        self.rho, self.T_init, self.tau, self.N_MD = rho, T, tau, N_MD
+        self.T_final = T if T_final is None else T_final
+        self.dt = tau / N_MD
+        self.do_hydro, self.do_thermostat = do_hydro, do_thermostat
+        self.skin = skin
+        vol = int(rho * 4 * PI_3142 / 3 * sigma ** 3 * N_colloids) if volume_correction else 0
+        self.N = int(rho * int(self.L.prod())) - vol
+        if self.N <= 0:
+            raise ValueError("Not enough volume available for solvent")
+        self.mass = rho * sigma ** 3 * 4 * PI_3141 / 3
+        sigma_cut = sigma * 2.0 ** (1.0 / 6.0)
+        self.solvent_colloid_lj = A.LJParams([[epsilon]], [[sigma]], [[sigma_cut]])
+        self.colloid_lj = A.LJParams([[epsilon_colloids]], [[2 * sigma]], [[2 * (3 * sigma)]])
+        self.rng = A.Rng(seed)
+        self.colloids = A.ParticleSystem(N_colloids, 1, [self.mass])
+        self.colloids.species = 1
+        self.vv_mass = np.full(N_colloids, self.mass)
+        self.solvent = A.ParticleSystem(self.N, 1, None, precision)
+        self.solvent.maxwell(T, seed)
+        self.solvent.species = 1
+        self.cells = A.CellSystem(self.L, 1.0)
+        self.edges = self.cells.edges
+        self.colloids.pos = place_colloids(A.rng_uniform2, seed, N_colloids, self.edges, 2 * sigma)
+        self.solvent.random_placement(self.edges, self.colloids, self.solvent_colloid_lj, seed)
+        self.solvent.sort(self.cells)
+        self.radius = sigma_cut + skin
+        cap = list_capacity if list_capacity is not None else int(250 * (sigma_cut + skin) ** 2)
+        self.neigh = A.NeighborList(N_colloids, cap)
+        self.neigh.make_stencil(self.cells, self.radius)
+        self.neigh.update_list(self.colloids, self.solvent, self.radius, self.cells)
+        self.e1 = A.compute_force(self.colloids, self.solvent, self.neigh, self.edges, self.solvent_colloid_lj)
+        self.e2 = A.compute_force_n2(self.colloids, self.edges, self.colloid_lj)
+        self.solvent.copy_force_old()
+        self.colloids.copy_force_old()
+        self.solvent.copy_pos_old()
+        self.colloids.copy_pos_old()
+        self.n_extra_sorting = 0
+        self.t = 0          # MD steps of the current loop (thermalisation or production)
+        self.last_sort = 0  # value of t at the last sort
+
+    def _catch_up_and_sort(self):
+        """Stream the non-MD cells over the time since the last sort, wrap,
+        sort, rebuild the list (programs/n_colloids_pbc.f90:230-241)."""
+        s, c, dtl = self.solvent, self.colloids, (self.t - self.last_sort) * self.dt
+        A.cell_md_pos(self.cells, s, dtl, False)
+        A.cell_md_vel(self.cells, s, dtl, False)
+        A.apply_pbc(s, self.edges)
+        A.apply_pbc(c, self.edges)
+        s.sort(self.cells)
+        self.last_sort = self.t
+        self.neigh.update_list(c, s, self.radius, self.cells)
+        s.copy_pos_old()
+        c.copy_pos_old()
+
+    def md_step(self):
+        """One pass of md_loop, programs/n_colloids_pbc.f90:221-254."""
+        s, c, dt = self.solvent, self.colloids, self.dt
+        self.t += 1
+        A.cell_md_pos(self.cells, s, dt, True)
+        A.colloid_vv_pos(c, dt, self.vv_mass)
+        so_max = A.cell_maximum_displacement(self.cells, s, dt * (self.t - self.last_sort))
+        co_max = c.maximum_displacement()
+        if (co_max >= self.skin * 0.1) or (so_max >= self.skin * 0.9):
+            self._catch_up_and_sort()
+            self.n_extra_sorting += 1
+        s.switch_force()
+        c.switch_force()
+        s.zero_force()
+        c.zero_force()
+        self.e1 = A.compute_force(c, s, self.neigh, self.edges, self.solvent_colloid_lj)
+        self.e2 = A.compute_force_n2(c, self.edges, self.colloid_lj)
+        A.cell_md_vel(self.cells, s, dt, True)
+        A.colloid_vv_vel(c, dt, self.vv_mass)
+
+    def interval(self, thermostat: bool, T: float, rescale: bool = False):
+        """md_loop followed by the MPCD part (programs/n_colloids_pbc.f90:256-276, :304-324)."""
+        for _ in range(self.N_MD):
+            self.md_step()
+        self.cells.random_shift(self.rng)
+        self._catch_up_and_sort()
+        A.simple_mpcd_step(self.solvent, self.cells, self.rng, thermostat=thermostat, T=T, hydro=self.do_hydro)
+        if rescale:
+            A.rescale_cells(self.solvent, self.cells, self.rng, self.T_init)
+
+    def thermalise(self, n_loops):
+        """The thermostatted loop: MPC-AT at T, cell rescaling every 10 intervals."""
+        for i in range(1, n_loops + 1):
+            self.interval(True, self.T_init, rescale=(i % 10 == 0))
+        self.t = self.last_sort = 0
+
+    def run(self, n_loops):
+        """The production loop with the temperature ramp T_init -> T_final."""
+        for i in range(1, n_loops + 1):
+            T = self.T_init + (i - 1) * (self.T_final - self.T_init) / max(1, n_loops - 1)
+            self.interval(self.do_thermostat, T)
 
 
 def bulk_fluid(L, rho=10, T=1.0 / 3.0, tau=1.0, n_intervals=200, seed=1, precision=A.FP64, alpha=None):

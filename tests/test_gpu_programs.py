@@ -72,3 +72,26 @@ def test_single_dimer_pbc_bit_exact(rm, oracle, n_int):
     assert_same(g.solvent, o.s, ("pos", "vel", "image", "id", "species", "flags", "force"))
     assert g.n_extra_sorting == o.n_extra_sorting
     assert g.rng.step == o.step
+
+
+def test_n_colloids_pbc_bit_exact(rm, oracle):
+    """programs/n_colloids_pbc.f90: thermalisation (MPC-AT + rescaling) and
+    production intervals with lazy cell-wise streaming, against the oracle."""
+    from oracle.programs import NColloidsPBC as OC
+    from rmpcdmd_b200.programs import NColloidsPBC as GC
+
+    kw = dict(L=(20, 20, 20), rho=10, N_MD=20, N_colloids=5, seed=31, T_final=0.4)
+    o = OC(**kw)
+    g = GC(**kw)
+    assert g.N == o.N
+    assert_same(g.colloids, o.c, ("pos",))
+    assert_same(g.solvent, o.s, ("pos", "vel", "species", "id"))
+    o.thermalise(2)
+    g.thermalise(2)
+    o.run(2)
+    g.run(2)
+    assert_same(g.colloids, o.c, ("pos", "vel", "force", "image"))
+    assert_same(g.solvent, o.s, ("pos", "vel", "image", "id", "species", "flags", "force"))
+    assert g.n_extra_sorting == o.n_extra_sorting
+    assert g.rng.step == o.step
+    assert np.array_equal(g.cells.origin, o.cells.origin)
