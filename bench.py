@@ -267,6 +267,23 @@ def run_dimer(rm, peak, peak_kind, local):
                                              "sample": "replicas 0-7, one interval each"}
     e["batched_over_sequential_fp64"] = round(e["value"] / e["fp64_plain_one_replica_at_a_time"]["value"], 3)
     out["batched_512_fp32"] = e
+    # n_colloids_pbc: 200 passive colloids (sigma 3) in 128^3, the program's
+    # loop call by call through the C ABI (lazy cell-wise streaming)
+    from rmpcdmd_b200.programs import NColloidsPBC
+    for prec in (64, 32):
+        g = NColloidsPBC(L=(128, 128, 128), rho=RHO, N_MD=DIMER_N_MD, N_colloids=200, seed=SEED,
+                         volume_correction=False, precision=prec)
+        g.interval(True, g.T_init)
+        rm.synchronize()
+        t0 = time.perf_counter()
+        g.interval(True, g.T_init)
+        rm.synchronize()
+        sec = time.perf_counter() - t0
+        out[f"n_colloids_128_fp{prec}_call_by_call"] = {
+            "value": g.N * DIMER_N_MD / sec, "us_per_md_step": round(sec * 1e6 / DIMER_N_MD, 2), "N": g.N,
+            "colloids": 200, "n_extra_sorting": g.n_extra_sorting,
+            "path": "one C-ABI call per module procedure (wall clock), thermostatted interval"}
+        del g
     return out
 
 
