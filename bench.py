@@ -487,6 +487,23 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def profile_dimer(args):
+    """A fixed engine workload for profilers: R replicas of the batched
+    dimer (cubic sides drawn from {16..48}), FP32 solvent, one interval with
+    the kernels launched one by one (profilers cannot see inside a graph that
+    holds conditional nodes).  Prints nothing but a line when done."""
+    import rmpcdmd_b200 as rm
+    from rmpcdmd_b200.programs import DimerBatch, SingleDimerPBC
+
+    boxes = dimer_boxes_batched()[: args.profile_dimer]
+    ds = [SingleDimerPBC(L=L, rho=RHO, N_MD=DIMER_N_MD, seed=k + 1, list_capacity=DIMER_LIST_CAPACITY,
+                         precision=32) for k, L in enumerate(boxes)]
+    b = DimerBatch(ds, use_graph=False)
+    b.run(1)
+    rm.synchronize()
+    print(f"profile_dimer: {len(ds)} replicas, {b.n_solvent} particles, 1 interval")
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -499,10 +516,14 @@ def main(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-dimer", action="store_true", help="skip the single-dimer engine configurations")
+    ap.add_argument("--profile-dimer", type=int, default=0, metavar="R",
+                    help="only run one interval of R batched dimer replicas (graph off), for profilers")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.profile_dimer:
+        profile_dimer(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
