@@ -328,8 +328,10 @@ class NColloidsPBC:
         s.copy_pos_old()
         c.copy_pos_old()
 
-    def md_step(self):
-        """One pass of md_loop, programs/n_colloids_pbc.f90:221-254."""
+    def md_step(self, want_energy=False):
+        """One pass of md_loop, programs/n_colloids_pbc.f90:221-254.  The
+        energies e1, e2 are only read after the last MD step of an interval
+        (the thermo output), so they are computed there only."""
         s, c, dt = self.solvent, self.colloids, self.dt
         self.t += 1
         A.cell_md_pos(self.cells, s, dt, True)
@@ -343,15 +345,17 @@ class NColloidsPBC:
         c.switch_force()
         s.zero_force()
         c.zero_force()
-        self.e1 = A.compute_force(c, s, self.neigh, self.edges, self.solvent_colloid_lj)
-        self.e2 = A.compute_force_n2(c, self.edges, self.colloid_lj)
+        e1 = A.compute_force(c, s, self.neigh, self.edges, self.solvent_colloid_lj, energy=want_energy)
+        e2 = A.compute_force_n2(c, self.edges, self.colloid_lj, energy=want_energy)
+        if want_energy:
+            self.e1, self.e2 = e1, e2
         A.cell_md_vel(self.cells, s, dt, True)
         A.colloid_vv_vel(c, dt, self.vv_mass)
 
     def interval(self, thermostat: bool, T: float, rescale: bool = False):
         """md_loop followed by the MPCD part (programs/n_colloids_pbc.f90:256-276, :304-324)."""
-        for _ in range(self.N_MD):
-            self.md_step()
+        for j in range(self.N_MD):
+            self.md_step(want_energy=(j == self.N_MD - 1))
         self.cells.random_shift(self.rng)
         self._catch_up_and_sort()
         A.simple_mpcd_step(self.solvent, self.cells, self.rng, thermostat=thermostat, T=T, hydro=self.do_hydro)
