@@ -307,6 +307,18 @@ int rmpcd_velocity_sums(rmpcd_particles *p, double out[4]);
  * uses rng step s+2i for the collision and s+2i+1 for the shift. */
 int rmpcd_bulk_run(rmpcd_particles *p, rmpcd_cells *cells, rmpcd_rng *rng,
                    double tau, int has_alpha, double alpha, int n_intervals);
+/* Tile shapes of the fused interval kernel (slots per block, resident
+ * blocks per SM).  All shapes give the same results bit for bit; one is in
+ * use per precision (shape 0 until set).  No counterpart in the reference. */
+int rmpcd_bulk_shapes(int precision, int *n_shapes, int *slots, int *min_blocks);
+int rmpcd_bulk_set_shape(int precision, int shape);
+int rmpcd_bulk_get_shape(int precision, int *shape);
+/* Autotuner: builds a synthetic bulk fluid of box L at density 10 (seeded
+ * placement, Maxwell kT = 1/3), times n_intervals intervals with every
+ * shape, puts the fastest in use for `precision` and returns its index in
+ * *best; ms_per_shape (may be NULL) receives each shape's time. */
+int rmpcd_bulk_autotune(const int L[3], int precision, double tau, int n_intervals, int *best,
+                        float *ms_per_shape);
 
 /* Batched single_dimer_pbc: the main loop of programs/single_dimer_pbc.f90
  * (:303-443: N_MD MD steps with the program's re-sort test, then

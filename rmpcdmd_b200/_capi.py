@@ -153,6 +153,10 @@ PROTOTYPES = {
                                           C.c_double, C.c_double, C.c_double, C.c_int, c_double_p],
     "rmpcd_velocity_sums": [PART_P, c_double_p],
     "rmpcd_bulk_run": [PART_P, CELLS_P, RNG_P, C.c_double, C.c_int, C.c_double, C.c_int],
+    "rmpcd_bulk_shapes": [C.c_int, c_int_p, c_int_p, c_int_p],
+    "rmpcd_bulk_set_shape": [C.c_int, C.c_int],
+    "rmpcd_bulk_get_shape": [C.c_int, c_int_p],
+    "rmpcd_bulk_autotune": [c_int_p, C.c_int, C.c_double, C.c_int, c_int_p, C.POINTER(C.c_float)],
     "rmpcd_dimer_batch_create": [C.POINTER(c_void_p), C.c_int, C.POINTER(c_void_p), C.POINTER(c_void_p),
                                  C.POINTER(c_void_p), C.POINTER(c_void_p), RNG_P, LJ_P, LJ_P,
                                  C.POINTER(DIMER_PARAMS)],

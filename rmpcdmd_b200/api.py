@@ -579,6 +579,37 @@ def bulk_run(particles: ParticleSystem, cells: CellSystem, state: Rng, tau: floa
          float(alpha or 0.0), int(n_intervals))
 
 
+def bulk_shapes(precision: int = FP32) -> list[tuple[int, int]]:
+    """(slots per block, blocks per SM) of every tile shape of the fused interval kernel."""
+    n = C.c_int()
+    sl = np.zeros(16, np.int32)
+    mb = np.zeros(16, np.int32)
+    call("rmpcd_bulk_shapes", int(precision), C.byref(n), _ip(sl), _ip(mb))
+    return [(int(sl[k]), int(mb[k])) for k in range(n.value)]
+
+
+def bulk_shape(precision: int = FP32) -> int:
+    s = C.c_int()
+    call("rmpcd_bulk_get_shape", int(precision), C.byref(s))
+    return s.value
+
+
+def set_bulk_shape(precision: int, shape: int) -> None:
+    call("rmpcd_bulk_set_shape", int(precision), int(shape))
+
+
+def bulk_autotune(L, precision: int = FP32, tau: float = 1.0, n_intervals: int = 5) -> tuple[int, list[float]]:
+    """Time every tile shape on a synthetic bulk fluid of box L; the fastest is put in use."""
+    n = len(bulk_shapes(precision))
+    ms = (C.c_float * n)()
+    best = C.c_int()
+    call("rmpcd_bulk_autotune", _ip(_i3(L)), int(precision), float(tau), int(n_intervals), C.byref(best), ms)
+    return best.value, [float(x) for x in ms]
+
+
+__all__ += ["bulk_shapes", "bulk_shape", "set_bulk_shape", "bulk_autotune"]
+
+
 class Timers:
     """Per-phase device timers (the reference's timer_t list)."""
 

@@ -71,22 +71,18 @@ struct Rec<double> {
     __device__ static double *pos(unsigned char *r) { return (double *)r + 4; }
 };
 
-// cells per block, staged-particle capacity and resident blocks per SM; the
-// capacity is > 7 standard deviations above the mean tile occupancy at
-// density 10 and an over-full tile takes the global-memory path
-template <typename R>
-struct FusedCfg;
-template <>
-struct FusedCfg<float> {
-    static constexpr int kSlots = 128;
-    static constexpr int kCap = 1792;
-    static constexpr int kMinBlocks = 4;
-};
-template <>
-struct FusedCfg<double> {
-    static constexpr int kSlots = 96;
-    static constexpr int kCap = 1408;
-    static constexpr int kMinBlocks = 4;
+// Tile shape of k_bulk_interval: slots (cells) per block, staged-particle
+// capacity and resident blocks per SM (launch bound).  The capacity is more
+// than 7 standard deviations above the mean tile occupancy at density 10; an
+// over-full tile takes the global-memory path.  Every shape gives the same
+// results bit for bit (the tile size changes only which block handles a
+// cell); the shape in use is chosen per precision, by default the first one,
+// or by rmpcd_bulk_autotune.
+template <int SL_, int CAP_, int MINB_>
+struct Shape {
+    static constexpr int kSlots = SL_;
+    static constexpr int kCap = CAP_;
+    static constexpr int kMinBlocks = MINB_;
 };
 
 template <typename R>
@@ -242,10 +238,10 @@ __device__ inline int stream_values(const FusedArgs<R> &A, R &x, R &y, R &z, R v
     return slot_of(A.g_next, (double)x, (double)y, (double)z);
 }
 
-template <typename R>
+template <typename R, typename S>
 constexpr size_t fused_smem()
 {
-    return (size_t)FusedCfg<R>::kCap * (Rec<R>::kVelBytes + sizeof(int));
+    return (size_t)S::kCap * (Rec<R>::kVelBytes + sizeof(int));
 }
 
 // the non-velocity part of a record, as loaded from global memory
@@ -305,11 +301,12 @@ __device__ inline int finish_particle(const FusedArgs<double> &A, const unsigned
     return key;
 }
 
-template <typename R>
-__global__ void __launch_bounds__(kFusedThreads, FusedCfg<R>::kMinBlocks) k_bulk_interval(FusedArgs<R> A)
+template <typename R, typename S>
+__global__ void __launch_bounds__(kFusedThreads, S::kMinBlocks) k_bulk_interval(FusedArgs<R> A)
 {
-    constexpr int SL = FusedCfg<R>::kSlots;
-    constexpr int CAP = FusedCfg<R>::kCap;
+    constexpr int SL = S::kSlots;
+    constexpr int CAP = S::kCap;
+    static_assert(SL <= kFusedThreads, "one thread per slot of the tile");
     constexpr int B = Rec<R>::kBytes;
     constexpr int VB = Rec<R>::kVelBytes;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -474,6 +471,62 @@ __global__ void k_rec_gather_to_soa(const unsigned char *rec, const int *perm, P
     }
 }
 
+// the shapes a precision can run with, and the one in use
+template <typename R>
+struct ShapeEntry {
+    void (*kernel)(FusedArgs<R>);
+    int slots;
+    size_t smem;
+    int min_blocks;
+};
+
+template <typename R, typename S>
+constexpr ShapeEntry<R> entry()
+{
+    return {k_bulk_interval<R, S>, S::kSlots, fused_smem<R, S>(), S::kMinBlocks};
+}
+
+template <typename R>
+struct Shapes;
+template <>
+struct Shapes<float> {
+    static constexpr ShapeEntry<float> list[] = {entry<float, Shape<128, 1792, 4>>(),
+                                                  entry<float, Shape<128, 1792, 5>>(),
+                                                  entry<float, Shape<96, 1408, 5>>(),
+                                                  entry<float, Shape<192, 2560, 3>>()};
+};
+template <>
+struct Shapes<double> {
+    static constexpr ShapeEntry<double> list[] = {entry<double, Shape<96, 1408, 4>>(),
+                                                   entry<double, Shape<64, 1024, 5>>(),
+                                                   entry<double, Shape<128, 1792, 3>>()};
+};
+template <typename R>
+constexpr int n_shapes()
+{
+    return (int)(sizeof(Shapes<R>::list) / sizeof(Shapes<R>::list[0]));
+}
+
+static int g_shape[2] = {0, 0};  // shape in use: [0] FP32, [1] FP64
+
+template <typename R>
+static const ShapeEntry<R> &shape_in_use()
+{
+    return Shapes<R>::list[g_shape[sizeof(R) == 8]];
+}
+
+template <typename R>
+static int prepare_shapes()
+{
+    static bool done[2] = {false, false};
+    if (done[sizeof(R) == 8]) return RMPCD_OK;
+    for (int k = 0; k < n_shapes<R>(); k++)
+        RMPCD_CUDA_TRY(cudaFuncSetAttribute(Shapes<R>::list[k].kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)Shapes<R>::list[k].smem));
+    done[sizeof(R) == 8] = true;
+    return RMPCD_OK;
+}
+
 template <typename R>
 static int ensure_records(rmpcd_particles *p)
 {
@@ -495,13 +548,10 @@ static int bulk_run_fused(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r, doub
                           double alpha, int n_intervals)
 {
     cudaStream_t st = stream();
-    static bool attr_set[2] = {false, false};
-    if (!attr_set[sizeof(R) == 8]) {
-        RMPCD_CUDA_TRY(cudaFuncSetAttribute(k_bulk_interval<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)fused_smem<R>()));
-        attr_set[sizeof(R) == 8] = true;
-    }
-    int rc = ensure_records<R>(p);
+    int rc = prepare_shapes<R>();
+    if (rc) return rc;
+    const ShapeEntry<R> &shape = shape_in_use<R>();
+    rc = ensure_records<R>(p);
     if (rc) return rc;
     double sin_a = 1, cos_a = 0;
     if (has_alpha) {
@@ -516,7 +566,7 @@ static int bulk_run_fused(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r, doub
     // image, flags and id stay in the current API arrays, addressed by idx
     const PView<R> side = cur<R>(p);
     int rb = 0;  // record buffer holding the current arrays
-    const int nblocks = (c->S + FusedCfg<R>::kSlots - 1) / FusedCfg<R>::kSlots;
+    const int nblocks = (c->S + shape.slots - 1) / shape.slots;
     int *perm = nullptr;  // identity for the first interval (data sorted on entry)
     for (int it = 0; it < n_intervals; it++) {
         uint64_t step_c = r->step;
@@ -553,7 +603,7 @@ static int bulk_run_fused(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r, doub
         A.axes = c->axes;
         {
             PhaseTimer t("interval_fused");
-            k_bulk_interval<R><<<nblocks, kFusedThreads, fused_smem<R>(), st>>>(A);
+            shape.kernel<<<nblocks, kFusedThreads, shape.smem, st>>>(A);
             RMPCD_CHECK_LAUNCH();
         }
         rb = 1 - rb;
@@ -589,6 +639,105 @@ static int bulk_run_fused(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r, doub
 }  // namespace rmpcd
 
 using namespace rmpcd;
+
+// species = 1 for a synthetic fluid
+__global__ void k_fill_int(int *a, long long n, int v)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        a[i] = v;
+}
+
+template <typename R>
+static int autotune_t(const int L[3], double tau, int n_intervals, int *best, float *ms_out)
+{
+    rmpcd_cells *c = nullptr;
+    rmpcd_particles *p = nullptr;
+    int rc = rmpcd_cells_init(&c, L, 1.0, 0);
+    long long N = 10LL * L[0] * L[1] * L[2];
+    if (!rc && N > 2000000000LL) rc = fail(RMPCD_ERR_CAPACITY, "rmpcd_bulk_autotune: box too large");
+    if (!rc) rc = rmpcd_particles_init(&p, (int)N, 1, nullptr, sizeof(R) == 4 ? RMPCD_FP32 : RMPCD_FP64);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (!rc) {
+        const double edges[3] = {c->edges[0], c->edges[1], c->edges[2]};
+        const uint64_t seed = 0x5eed;
+        rmpcd_rng r{seed, 0};
+        rc = rmpcd_particles_random_placement(p, edges, nullptr, nullptr, seed);
+        if (!rc) rc = rmpcd_particles_maxwell(p, 1.0 / 3.0, seed);
+        if (!rc) {
+            k_fill_int<<<grid_for(N, 256), 256, 0, stream()>>>(p->species[p->cur], N, 1);
+            rc = rmpcd_cells_random_shift(c, &r);
+        }
+        if (!rc) rc = rmpcd_particles_sort(p, c);
+        if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+            rc = fail(RMPCD_ERR_CUDA, "rmpcd_bulk_autotune: event creation failed");
+        const int keep = g_shape[sizeof(R) == 8];
+        float best_ms = 0;
+        int best_k = keep;
+        for (int k = 0; !rc && k < n_shapes<R>(); k++) {
+            g_shape[sizeof(R) == 8] = k;
+            rc = bulk_run_fused<R>(p, c, &r, tau, 0, 0.0, 1);
+            if (rc) break;
+            cudaEventRecord(e0, stream());
+            rc = bulk_run_fused<R>(p, c, &r, tau, 0, 0.0, n_intervals);
+            cudaEventRecord(e1, stream());
+            if (!rc) rc = sync();
+            float ms = 0;
+            if (!rc) cudaEventElapsedTime(&ms, e0, e1);
+            if (ms_out) ms_out[k] = ms;
+            if (!rc && (k == 0 || ms < best_ms)) {
+                best_ms = ms;
+                best_k = k;
+            }
+        }
+        g_shape[sizeof(R) == 8] = rc ? keep : best_k;
+        if (best) *best = g_shape[sizeof(R) == 8];
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    rmpcd_particles_destroy(p);
+    rmpcd_cells_destroy(c);
+    return rc;
+}
+
+extern "C" int rmpcd_bulk_shapes(int precision, int *n, int *slots, int *min_blocks)
+{
+    RMPCD_ARG(n, "null argument");
+    RMPCD_ARG(precision == RMPCD_FP32 || precision == RMPCD_FP64, "precision must be 32 or 64");
+    const bool f = precision == RMPCD_FP32;
+    *n = f ? n_shapes<float>() : n_shapes<double>();
+    for (int k = 0; k < *n; k++) {
+        if (slots) slots[k] = f ? Shapes<float>::list[k].slots : Shapes<double>::list[k].slots;
+        if (min_blocks) min_blocks[k] = f ? Shapes<float>::list[k].min_blocks : Shapes<double>::list[k].min_blocks;
+    }
+    return RMPCD_OK;
+}
+
+extern "C" int rmpcd_bulk_set_shape(int precision, int shape)
+{
+    RMPCD_ARG(precision == RMPCD_FP32 || precision == RMPCD_FP64, "precision must be 32 or 64");
+    const int n = precision == RMPCD_FP32 ? n_shapes<float>() : n_shapes<double>();
+    RMPCD_ARG(shape >= 0 && shape < n, "rmpcd_bulk_set_shape: no such shape");
+    g_shape[precision == RMPCD_FP64] = shape;
+    return RMPCD_OK;
+}
+
+extern "C" int rmpcd_bulk_get_shape(int precision, int *shape)
+{
+    RMPCD_ARG(shape, "null argument");
+    RMPCD_ARG(precision == RMPCD_FP32 || precision == RMPCD_FP64, "precision must be 32 or 64");
+    *shape = g_shape[precision == RMPCD_FP64];
+    return RMPCD_OK;
+}
+
+extern "C" int rmpcd_bulk_autotune(const int L[3], int precision, double tau, int n_intervals, int *best,
+                                   float *ms_per_shape)
+{
+    RMPCD_ARG(L && L[0] > 0 && L[1] > 0 && L[2] > 0, "rmpcd_bulk_autotune: box sides must be > 0");
+    RMPCD_ARG(n_intervals >= 1, "rmpcd_bulk_autotune: n_intervals must be >= 1");
+    RMPCD_ARG(precision == RMPCD_FP32 || precision == RMPCD_FP64, "precision must be 32 or 64");
+    if (precision == RMPCD_FP32) return autotune_t<float>(L, tau, n_intervals, best, ms_per_shape);
+    return autotune_t<double>(L, tau, n_intervals, best, ms_per_shape);
+}
 
 extern "C" int rmpcd_bulk_run(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r, double tau, int has_alpha,
                               double alpha, int n_intervals)

@@ -95,3 +95,27 @@ def test_n_colloids_pbc_bit_exact(rm, oracle):
     assert g.n_extra_sorting == o.n_extra_sorting
     assert g.rng.step == o.step
     assert np.array_equal(g.cells.origin, o.cells.origin)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_bulk_shapes_give_identical_results(rm, oracle, precision):
+    """Every tile shape of the fused interval (and the autotuner's choice)
+    produces the same arrays bit for bit."""
+    shapes = rm.bulk_shapes(precision)
+    assert len(shapes) >= 2
+    keep = rm.bulk_shape(precision)
+    outs = []
+    try:
+        for k in range(len(shapes)):
+            rm.set_bulk_shape(precision, k)
+            (_, _), (gc, gp) = make_pair(rm, oracle, [16, 12, 10], 19200, seed=8, precision=precision)
+            rm.bulk_run(gp, gc, rm.Rng(3, 0), 1.0, 3)
+            outs.append({f: gp.download(f) for f in ("pos", "vel", "image", "id")})
+        for o in outs[1:]:
+            for f in o:
+                assert np.array_equal(o[f], outs[0][f]), f
+        best, ms = rm.bulk_autotune([24, 24, 24], precision, 1.0, 2)
+        assert 0 <= best < len(shapes) and rm.bulk_shape(precision) == best
+        assert len(ms) == len(shapes) and all(m > 0 for m in ms)
+    finally:
+        rm.set_bulk_shape(precision, keep)
