@@ -493,13 +493,17 @@ struct Shapes<float> {
     static constexpr ShapeEntry<float> list[] = {entry<float, Shape<128, 1792, 4>>(),
                                                   entry<float, Shape<128, 1792, 5>>(),
                                                   entry<float, Shape<96, 1408, 5>>(),
+                                                  entry<float, Shape<64, 1024, 6>>(),
+                                                  entry<float, Shape<160, 2176, 4>>(),
                                                   entry<float, Shape<192, 2560, 3>>()};
 };
 template <>
 struct Shapes<double> {
     static constexpr ShapeEntry<double> list[] = {entry<double, Shape<96, 1408, 4>>(),
-                                                   entry<double, Shape<64, 1024, 5>>(),
-                                                   entry<double, Shape<128, 1792, 3>>()};
+                                                   entry<double, Shape<112, 1600, 3>>(),
+                                                   entry<double, Shape<128, 1792, 3>>(),
+                                                   entry<double, Shape<160, 2176, 2>>(),
+                                                   entry<double, Shape<192, 2560, 2>>()};
 };
 template <typename R>
 constexpr int n_shapes()
