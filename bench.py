@@ -511,6 +511,21 @@ def profile_dimer(args):
     print(f"profile_dimer: {len(ds)} replicas, {b.n_solvent} particles, 1 interval")
 
 
+def profile_ncolloids(args):
+    """A fixed n_colloids_pbc workload for profilers: 128^3, rho = 10,
+    args.profile_ncolloids colloids, FP32 solvent, one thermostatted interval
+    after one warm-up interval, call by call."""
+    import rmpcdmd_b200 as rm
+    from rmpcdmd_b200.programs import NColloidsPBC
+
+    g = NColloidsPBC(L=(128, 128, 128), rho=RHO, N_MD=DIMER_N_MD, N_colloids=args.profile_ncolloids, seed=SEED,
+                     volume_correction=False, precision=32)
+    g.interval(True, g.T_init)
+    g.interval(True, g.T_init)
+    rm.synchronize()
+    print(f"profile_ncolloids: {args.profile_ncolloids} colloids, {g.N} particles, 2 intervals")
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -523,6 +538,8 @@ def main(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-dimer", action="store_true", help="skip the single-dimer engine configurations")
+    ap.add_argument("--profile-ncolloids", type=int, default=0, metavar="C",
+                    help="only run two intervals of n_colloids_pbc with C colloids at 128^3, for profilers")
     ap.add_argument("--profile-dimer", type=int, default=0, metavar="R",
                     help="only run one interval of R batched dimer replicas (graph off), for profilers")
     args = ap.parse_args(argv)
@@ -530,6 +547,8 @@ def main(argv=None):
         args.warmup = 3
     if args.profile_dimer:
         profile_dimer(args)
+    elif args.profile_ncolloids:
+        profile_ncolloids(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

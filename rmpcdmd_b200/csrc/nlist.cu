@@ -58,24 +58,30 @@ __global__ void k_pair_forces(const double *cx, const double *cy, const double *
                          contrib, ncontrib, max_contrib);
 }
 
-// solvent force - f for particles with exactly one contribution
+// solvent force - f for particles with exactly one contribution; the others
+// are collected for k_apply_multi
 template <typename R>
 __global__ void k_apply_single(const int *list, const int *n, int Nmax, const unsigned char *contrib,
-                               const double *pf, const int *ncontrib, R *fx, R *fy, R *fz)
+                               const double *pf, const int *ncontrib, R *fx, R *fy, R *fz,
+                               unsigned long long *mkeys, int *m_count)
 {
     const int i = blockIdx.y;
     const int ni = n[i];
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ni; e += gridDim.x * blockDim.x)
-        apply_single_entry((size_t)i * Nmax + e, list, contrib, pf, ncontrib, fx, fy, fz);
+        apply_single_or_collect((size_t)i * Nmax + e, list, contrib, pf, ncontrib, fx, fy, fz, mkeys, m_count);
 }
 
 template <typename R>
 __global__ void k_apply_multi(const int *list, const int *n, int C, int Nmax, const unsigned char *contrib,
                               const double *pf, const int *ncontrib, const int *max_contrib, int serial,
-                              R *fx, R *fy, R *fz)
+                              R *fx, R *fy, R *fz, const unsigned long long *mkeys, int *m_count)
 {
     if (*max_contrib < 2) return;
-    apply_multi_block(list, n, C, Nmax, contrib, pf, ncontrib, serial, fx, fy, fz);
+    const int m = *m_count;
+    if (!apply_multi_sorted_block(mkeys, m, pf, fx, fy, fz))
+        apply_multi_block(list, n, C, Nmax, contrib, pf, ncontrib, serial, fx, fy, fz);
+    __syncthreads();
+    if (threadIdx.x == 0) *m_count = 0;
 }
 
 // f1 = sum of the pair forces in list order; force(:,i) = force(:,i) + f1
@@ -141,6 +147,8 @@ static int ensure_force_scratch(rmpcd_nlist *nl, int N2)
         RMPCD_CUDA_TRY(cudaMalloc(&nl->pair_e, ne * sizeof(double) + 8));
         RMPCD_CUDA_TRY(cudaMalloc(&nl->contrib, ne + 8));
         RMPCD_CUDA_TRY(cudaMalloc(&nl->d_status, (2 * nl->Npoints + 16 + ne) * sizeof(int)));
+        RMPCD_CUDA_TRY(cudaMalloc(&nl->mkeys, kMultiSortMax * sizeof(unsigned long long)));
+        RMPCD_CUDA_TRY(cudaMemsetAsync(nl->d_status, 0, 16 * sizeof(int), stream()));
     }
     if (nl->ncontrib_cap < N2) {
         cudaStreamSynchronize(stream());
@@ -190,6 +198,7 @@ int rmpcd_nlist_destroy(rmpcd_nlist *nl)
     cudaFree(nl->contrib);
     cudaFree(nl->ncontrib);
     cudaFree(nl->d_status);
+    cudaFree(nl->mkeys);
     delete nl;
     return RMPCD_OK;
 }
@@ -302,6 +311,7 @@ int rmpcd_compute_force(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist 
     int C = ps1->N;
     if (ps2->N > 0) k_flag_roll<<<grid_for(ps2->N, 256), 256, 0, s>>>(ps2->flags[ps2->cur], ps2->N);
     int *max_contrib = nl->d_status;
+    int *m_count = nl->d_status + 1;  // multi-contribution keys collected (reset by k_apply_multi)
     int *cn = nl->d_status + 16;
     int *clist = nl->d_status + 16 + 2 * nl->Npoints;
     double *e_out = (double *)ps1->d_sums;
@@ -325,9 +335,10 @@ int rmpcd_compute_force(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist 
                                                       L[1], L[2], ld, nl->pair_f, nl->pair_e, nl->contrib,
                                                       nl->ncontrib, max_contrib);
             k_apply_single<float><<<grid, 256, 0, s>>>(nl->list, nl->n, nl->Nmax, nl->contrib, nl->pair_f,
-                                                       nl->ncontrib, v.force.x, v.force.y, v.force.z);
-            k_apply_multi<float><<<1, 256, 0, s>>>(nl->list, nl->n, C, nl->Nmax, nl->contrib, nl->pair_f,
-                                                   nl->ncontrib, max_contrib, serial, v.force.x, v.force.y, v.force.z);
+                                                       nl->ncontrib, v.force.x, v.force.y, v.force.z, nl->mkeys, m_count);
+            k_apply_multi<float><<<1, 1024, 0, s>>>(nl->list, nl->n, C, nl->Nmax, nl->contrib, nl->pair_f,
+                                                   nl->ncontrib, max_contrib, serial, v.force.x, v.force.y, v.force.z, nl->mkeys,
+                                                   m_count);
         } else {
             PView<double> v = cur<double>(ps2);
             k_pair_forces<double><<<grid, 256, 0, s>>>(cv.pos.x, cv.pos.y, cv.pos.z, cv.species, v.pos.x, v.pos.y,
@@ -335,9 +346,10 @@ int rmpcd_compute_force(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist 
                                                        L[1], L[2], ld, nl->pair_f, nl->pair_e, nl->contrib,
                                                        nl->ncontrib, max_contrib);
             k_apply_single<double><<<grid, 256, 0, s>>>(nl->list, nl->n, nl->Nmax, nl->contrib, nl->pair_f,
-                                                        nl->ncontrib, v.force.x, v.force.y, v.force.z);
-            k_apply_multi<double><<<1, 256, 0, s>>>(nl->list, nl->n, C, nl->Nmax, nl->contrib, nl->pair_f,
-                                                    nl->ncontrib, max_contrib, serial, v.force.x, v.force.y, v.force.z);
+                                                        nl->ncontrib, v.force.x, v.force.y, v.force.z, nl->mkeys, m_count);
+            k_apply_multi<double><<<1, 1024, 0, s>>>(nl->list, nl->n, C, nl->Nmax, nl->contrib, nl->pair_f,
+                                                    nl->ncontrib, max_contrib, serial, v.force.x, v.force.y, v.force.z, nl->mkeys,
+                                                   m_count);
         }
         k_colloid_sum<<<C, kNlThreads, 0, s>>>(nl->n, nl->Nmax, nl->contrib, nl->pair_f, cv.force.x, cv.force.y,
                                                cv.force.z, clist, cn);

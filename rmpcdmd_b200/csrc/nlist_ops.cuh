@@ -224,6 +224,75 @@ __device__ inline void apply_single_entry(size_t q, const int *list, const unsig
     fz[idx] = fz[idx] - (R)pf[3 * q + 2];
 }
 
+// Particles with several contributions must receive their subtractions in
+// the reference's (colloid, entry) order.  The single-contribution pass
+// collects them as 64-bit keys (particle << 32 | entry index q, with
+// q = colloid * Nmax + entry increasing in that order); one block sorts the
+// keys and applies each particle's run in order.  Larger lists than the block
+// sorts take the colloid-by-colloid loop (apply_multi_block).
+constexpr int kMultiSortMax = 4096;
+
+template <typename R>
+__device__ inline void apply_single_or_collect(size_t q, const int *list, const unsigned char *contrib,
+                                               const double *pf, const int *ncontrib, R *fx, R *fy, R *fz,
+                                               unsigned long long *mkeys, int *m_count)
+{
+    if (!contrib[q]) return;
+    const int idx = list[q];
+    const int nc = ncontrib[idx];
+    if (nc == 1) {
+        fx[idx] = fx[idx] - (R)pf[3 * q];
+        fy[idx] = fy[idx] - (R)pf[3 * q + 1];
+        fz[idx] = fz[idx] - (R)pf[3 * q + 2];
+    } else if (nc > 1) {
+        const int k = atomicAdd(m_count, 1);
+        if (k < kMultiSortMax) mkeys[k] = ((unsigned long long)(unsigned)idx << 32) | (unsigned long long)q;
+    }
+}
+
+// one block: sort the collected keys and apply each particle's contributions
+// in (colloid, entry) order; returns false (nothing applied) when more keys
+// were collected than the block sorts
+template <typename R>
+__device__ inline bool apply_multi_sorted_block(const unsigned long long *mkeys, int m, const double *pf, R *fx,
+                                                R *fy, R *fz)
+{
+    __shared__ unsigned long long sk[kMultiSortMax];
+    if (m > kMultiSortMax) return false;
+    int n2 = 1;
+    while (n2 < m) n2 <<= 1;
+    for (int k = threadIdx.x; k < n2; k += blockDim.x) sk[k] = k < m ? mkeys[k] : ~0ull;
+    __syncthreads();
+    // bitonic sort of n2 keys (all distinct: q is unique)
+    for (int size = 2; size <= n2; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int k = threadIdx.x; k < n2; k += blockDim.x) {
+                const int o = k ^ stride;
+                if (o > k) {
+                    const bool up = (k & size) == 0;
+                    const unsigned long long a = sk[k], b = sk[o];
+                    if ((a > b) == up) {
+                        sk[k] = b;
+                        sk[o] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (int k = threadIdx.x; k < m; k += blockDim.x) {
+        const unsigned idx = (unsigned)(sk[k] >> 32);
+        if (k > 0 && (unsigned)(sk[k - 1] >> 32) == idx) continue;
+        for (int j = k; j < m && (unsigned)(sk[j] >> 32) == idx; j++) {
+            const size_t q = (size_t)(sk[j] & 0xffffffffull);
+            fx[idx] = fx[idx] - (R)pf[3 * q];
+            fy[idx] = fy[idx] - (R)pf[3 * q + 1];
+            fz[idx] = fz[idx] - (R)pf[3 * q + 2];
+        }
+    }
+    __syncthreads();
+    return true;
+}
+
 // particles with several contributions: colloid by colloid in order; inside
 // one colloid's list entries are distinct unless the stencil wraps the box,
 // in which case a single thread applies everything in order (one block)

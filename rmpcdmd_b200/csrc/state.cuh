@@ -91,6 +91,7 @@ struct rmpcd_nlist {
     int *ncontrib = nullptr;    // per solvent particle contribution counter
     int ncontrib_cap = 0;
     int *d_status = nullptr;
+    unsigned long long *mkeys = nullptr;  // multi-contribution keys (kMultiSortMax)
 };
 
 namespace rmpcd {
