@@ -247,7 +247,7 @@ int rmpcd_cell_md_pos(rmpcd_cells *c, rmpcd_particles *p, double dt, int md_flag
     RMPCD_ARG(c && p, "null argument");
     PhaseTimer t("md_pos");
     double dt_sq = dt * dt / 2;
-    int g = grid_for(c->S, 128);
+    int g = grid_full(c->S, 128);
     DISPATCH_R(p,
                (k_cell_md_pos<float><<<g, 128, 0, stream()>>>(c->count, c->start, c->is_md, c->S, cur<float>(p),
                                                                (float)dt, (float)dt_sq, md_flag)),
@@ -261,7 +261,7 @@ int rmpcd_cell_md_vel(rmpcd_cells *c, rmpcd_particles *p, double dt, int md_flag
 {
     RMPCD_ARG(c && p, "null argument");
     PhaseTimer t("md_vel");
-    int g = grid_for(c->S, 128);
+    int g = grid_full(c->S, 128);
     DISPATCH_R(p,
                (k_cell_md_vel<float><<<g, 128, 0, stream()>>>(c->count, c->start, c->is_md, c->S, cur<float>(p),
                                                                (float)dt, md_flag)),
@@ -276,7 +276,7 @@ static int cell_md_pos_wall(rmpcd_cells *c, rmpcd_particles *p, double dt, int m
     RMPCD_ARG(c && p, "null argument");
     PhaseTimer t("md_pos");
     double dt_sq = dt * dt / 2;
-    int g = grid_for(c->S, 128);
+    int g = grid_full(c->S, 128);
     DISPATCH_R(p,
                (k_cell_md_pos_wall<float><<<g, 128, 0, stream()>>>(c->count, c->start, c->is_md, c->S,
                                                                     cur<float>(p), (float)dt, (float)dt_sq,

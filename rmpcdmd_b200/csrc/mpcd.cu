@@ -415,7 +415,7 @@ int rmpcd_simple_mpcd_step(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r, int
     PhaseTimer t("step");
     SrdParams q = srd_params(p, c, r, has_alpha, alpha, thermostat, T, hydro);
     cudaStream_t s = stream();
-    int g = grid_for(c->S, 128);
+    int g = grid_full(c->S, 128);
     DISPATCH_R(p,
                ({ PView<float> v = cur<float>(p);
                   k_simple_mpcd<float><<<g, 128, 0, s>>>(c->count, c->start, c->S, v.vel.x, v.vel.y, v.vel.z, v.species, q); }),
@@ -442,7 +442,7 @@ int rmpcd_wall_mpcd_step(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r,
     double wt0 = all_present ? wall_temperature[0] : 0, wt1 = all_present ? wall_temperature[1] : 0;
     int wn0 = all_present ? wall_n[0] : 0, wn1 = all_present ? wall_n[1] : 0;
     cudaStream_t s = stream();
-    int g = grid_for(c->S, 128);
+    int g = grid_full(c->S, 128);
     PhaseTimer t("step");
     DISPATCH_R(p,
                ({ PView<float> v = cur<float>(p);
@@ -478,7 +478,7 @@ int rmpcd_rescale_cells(rmpcd_particles *p, rmpcd_cells *c, double T)
     RMPCD_ARG(p && c, "null argument");
     PhaseTimer t("step");
     cudaStream_t s = stream();
-    int g = grid_for(c->S, 128);
+    int g = grid_full(c->S, 128);
     DISPATCH_R(p,
                ({ PView<float> v = cur<float>(p);
                   k_rescale<float><<<g, 128, 0, s>>>(c->count, c->start, c->S, v.vel.x, v.vel.y, v.vel.z, v.species, T); }),
@@ -536,7 +536,7 @@ int rmpcd_bulk_reaction(rmpcd_particles *p, rmpcd_cells *c, int from, int to, do
                         rmpcd_rng *r)
 {
     RMPCD_ARG(p && c && r, "null argument");
-    k_bulk_reaction<<<grid_for(c->S, 128), 128, 0, stream()>>>(c->count, c->start, c->is_reac, c->S,
+    k_bulk_reaction<<<grid_full(c->S, 128), 128, 0, stream()>>>(c->count, c->start, c->is_reac, c->S,
                                                                p->species[p->cur], from, to, rate, tau,
                                                                r->seed, r->step);
     RMPCD_CHECK_LAUNCH();

@@ -111,12 +111,20 @@ __global__ void k_reset_contrib(const int *list, const int *n, int Nmax, const u
     }
 }
 
-// compute_force_n2, src/neighbor_list.f90:227-264
+// compute_force_n2, src/neighbor_list.f90:227-264: a thread per colloid for
+// a few colloids, a block per colloid for many
 __global__ void k_force_n2(const double *px, const double *py, const double *pz, const int *sp, int C,
                            double L0, double L1, double L2, LJDev lj, double *fx, double *fy, double *fz)
 {
     for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < C; m += gridDim.x * blockDim.x)
         force_n2_one(m, px, py, pz, sp, C, L0, L1, L2, lj, fx, fy, fz);
+}
+
+__global__ void __launch_bounds__(kNlBlockThreads)
+    k_force_n2_blocks(const double *px, const double *py, const double *pz, const int *sp, int C, double L0,
+                      double L1, double L2, LJDev lj, double *fx, double *fy, double *fz)
+{
+    force_n2_block(blockIdx.x, px, py, pz, sp, C, L0, L1, L2, lj, fx, fy, fz);
 }
 
 __global__ void k_energy_n2(const double *px, const double *py, const double *pz, const int *sp, int C,
@@ -382,8 +390,12 @@ int rmpcd_compute_force_n2(rmpcd_particles *ps, const double L[3], const rmpcd_l
         LJDev ld = lj_dev(lj);
         if (energy)
             k_energy_n2<<<1, 32, 0, s>>>(v.pos.x, v.pos.y, v.pos.z, v.species, C, L[0], L[1], L[2], ld, e_out);
-        k_force_n2<<<grid_for(C, 128), 128, 0, s>>>(v.pos.x, v.pos.y, v.pos.z, v.species, C, L[0], L[1], L[2], ld,
-                                                    v.force.x, v.force.y, v.force.z);
+        if (C <= 32)
+            k_force_n2<<<1, 32, 0, s>>>(v.pos.x, v.pos.y, v.pos.z, v.species, C, L[0], L[1], L[2], ld, v.force.x,
+                                        v.force.y, v.force.z);
+        else
+            k_force_n2_blocks<<<C, kNlBlockThreads, 0, s>>>(v.pos.x, v.pos.y, v.pos.z, v.species, C, L[0], L[1], L[2],
+                                                            ld, v.force.x, v.force.y, v.force.z);
         RMPCD_CHECK_LAUNCH();
     }
     if (energy) {

@@ -387,6 +387,66 @@ __device__ inline void colloid_sum_block(int i, const int *n, int Nmax, const un
     }
 }
 
+// compute_force_n2 for colloid m = blockIdx.x with the pair terms evaluated
+// by the whole block: term k (from colloid k != m) goes to shared memory in
+// chunks and thread 0 accumulates the chunk in k order, so the sum is the
+// sequential one of force_n2_one
+__device__ inline void force_n2_block(int m, const double *px, const double *py, const double *pz, const int *sp,
+                                      int C, double L0, double L1, double L2, const LJDev &lj, double *fx,
+                                      double *fy, double *fz)
+{
+    __shared__ double term[3][kNlBlockThreads];
+    __shared__ unsigned char has[kNlBlockThreads];
+    double a0 = 0, a1 = 0, a2 = 0;
+    if (threadIdx.x == 0) {
+        a0 = fx[m];
+        a1 = fy[m];
+        a2 = fz[m];
+    }
+    for (int k0 = 0; k0 < C; k0 += kNlBlockThreads) {
+        const int k = k0 + threadIdx.x;
+        unsigned char h = 0;
+        if (k < C && k != m) {
+            int i = k < m ? k : m, j = k < m ? m : k;
+            double d0 = min_image_d(px[i] - px[j], L0);
+            double d1 = min_image_d(py[i] - py[j], L1);
+            double d2 = min_image_d(pz[i] - pz[j], L2);
+            double r_sq = d0 * d0 + d1 * d1 + d2 * d2;
+            int s1 = sp[i], s2 = sp[j];
+            if (r_sq <= lj.cut_sq[(s1 - 1) + lj.n1 * (s2 - 1)]) {
+                int tt = (s2 - 1) + lj.n1 * (s1 - 1);
+                double fr = lj_force_over_r(r_sq, lj.epsilon[tt], lj.sigma[tt]);
+                term[0][threadIdx.x] = fr * d0;
+                term[1][threadIdx.x] = fr * d1;
+                term[2][threadIdx.x] = fr * d2;
+                h = k < m ? 1 : 2;
+            }
+        }
+        has[threadIdx.x] = h;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int n = min(kNlBlockThreads, C - k0);
+            for (int q = 0; q < n; q++) {
+                if (has[q] == 1) {
+                    a0 = a0 - term[0][q];
+                    a1 = a1 - term[1][q];
+                    a2 = a2 - term[2][q];
+                } else if (has[q] == 2) {
+                    a0 = a0 + term[0][q];
+                    a1 = a1 + term[1][q];
+                    a2 = a2 + term[2][q];
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        fx[m] = a0;
+        fy[m] = a1;
+        fz[m] = a2;
+    }
+}
+
 // compute_force_n2, src/neighbor_list.f90:227-264: colloid m receives, in the
 // sequential loop order, -f(k,m) for k < m and then +f(m,j) for j > m
 __device__ inline void force_n2_one(int m, const double *px, const double *py, const double *pz, const int *sp, int C,

@@ -63,8 +63,7 @@ __global__ void k_max_disp(Vec3<R> pos, Vec3<R> old, const int *species, int N,
         double r = disp_sq_one(pos, old, species, i);
         m = m > r ? m : r;
     }
-    m = warp_max(m);
-    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out, m);
+    warp_max_into(out, m);
 }
 
 // cell_maximum_displacement, src/particle_system.f90:380-410
@@ -87,8 +86,7 @@ __global__ void k_cell_max_disp(const int *count, const int *start, const unsign
             }
         }
     }
-    m = warp_max(m);
-    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out, m);
+    warp_max_into(out, m);
 }
 
 // random_placement, src/particle_system.f90:250-302: uniform positions,
@@ -473,11 +471,11 @@ int rmpcd_cell_maximum_displacement(rmpcd_cells *c, rmpcd_particles *p, double d
     RMPCD_CUDA_TRY(cudaMemsetAsync(p->d_max, 0, 8, s));
     if (p->precision == RMPCD_FP32) {
         PView<float> a = cur<float>(p), b = alt<float>(p);
-        k_cell_max_disp<float><<<grid_for(c->S, 256), 256, 0, s>>>(c->count, c->start, c->is_md, c->S,
+        k_cell_max_disp<float><<<grid_full(c->S, 256), 256, 0, s>>>(c->count, c->start, c->is_md, c->S,
                                                                    a.pos, b.pos, a.species, p->d_max);
     } else {
         PView<double> a = cur<double>(p), b = alt<double>(p);
-        k_cell_max_disp<double><<<grid_for(c->S, 256), 256, 0, s>>>(c->count, c->start, c->is_md, c->S,
+        k_cell_max_disp<double><<<grid_full(c->S, 256), 256, 0, s>>>(c->count, c->start, c->is_md, c->S,
                                                                     a.pos, b.pos, a.species, p->d_max);
     }
     unsigned long long bits = 0;

@@ -60,6 +60,16 @@ unsigned *dev_error_word();
 int check_dev_error(unsigned *bits_out);
 
 int sm_count();
+// one thread per item for kernels whose items carry serial inner loops
+// (cells): no cap, so every cell's loop runs in its own thread
+inline int grid_full(long long n, int block)
+{
+    long long g = (n + block - 1) / block;
+    if (g > 0x7fffffffLL) g = 0x7fffffffLL;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
 inline int grid_for(long long n, int block)
 {
     long long g = (n + block - 1) / block;
@@ -120,6 +130,11 @@ __device__ inline void atomic_max_nonneg(unsigned long long *addr, double v)
     atomicMax(addr, (unsigned long long)__double_as_longlong(v));
 }
 
+// warp maximum of non-negative r^2 values into *addr: one atomic per warp,
+// skipped when it cannot raise the stored maximum (keeps a single hot
+// address from serialising thousands of atomics)
+__device__ inline void warp_max_into(unsigned long long *addr, double m);
+
 template <typename T>
 __device__ inline T warp_max(T v)
 {
@@ -128,6 +143,13 @@ __device__ inline T warp_max(T v)
         v = v > w ? v : w;
     }
     return v;
+}
+
+__device__ inline void warp_max_into(unsigned long long *addr, double m)
+{
+    m = warp_max(m);
+    if ((threadIdx.x & 31) == 0 && m > 0 && m > __longlong_as_double((long long)__ldcg(addr)))
+        atomic_max_nonneg(addr, m);
 }
 
 }  // namespace rmpcd

@@ -212,7 +212,7 @@ int sort_perm_segments(rmpcd_cells *c, rmpcd_particles *p)
     // big-segment queue lives in cursor[] (free once perm is built) plus a counter
     int *n_big = p->d_ints;
     RMPCD_CUDA_TRY(cudaMemsetAsync(n_big, 0, sizeof(int), st));
-    k_segsort_small<<<grid_for(c->S, 256), 256, 0, st>>>(c->start, c->count, c->S, p->perm,
+    k_segsort_small<<<grid_full(c->S, 256), 256, 0, st>>>(c->start, c->count, c->S, p->perm,
                                                          c->cursor, n_big);
     k_segsort_big<<<64, 512, 0, st>>>(c->start, c->count, c->cursor, n_big, p->perm, p->key);
     RMPCD_CHECK_LAUNCH();
