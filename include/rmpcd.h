@@ -320,6 +320,37 @@ int rmpcd_bulk_get_shape(int precision, int *shape);
 int rmpcd_bulk_autotune(const int L[3], int precision, double tau, int n_intervals, int *best,
                         float *ms_per_shape);
 
+/* The main loops of programs/n_colloids_pbc.f90 (:221-276, :304-324) in one
+ * call: n_intervals intervals of N_MD MD steps with lazy cell-wise solvent
+ * streaming (cell_md_pos/vel on is_md cells, catch-up of the other cells
+ * before each sort), the program's re-sort test, velocity-Verlet colloids,
+ * then random_shift, catch-up + sort, simple_mpcd_step(thermostat, T[k],
+ * do_hydro) and, for interval numbers i = first_interval + k divisible by
+ * rescale_every (> 0), rescale_cells(T_rescale).  The calls and their order
+ * are those of the program, so the results equal the same calls made one by
+ * one; the loop state (MD step counters, re-sort count, the energies e1, e2
+ * of each interval's last MD step) is carried in *state.  No module
+ * counterpart in the reference. */
+typedef struct rmpcd_ncolloids_params {
+    double tau;          /* dt = tau / N_MD */
+    int N_MD;
+    double skin;         /* re-sort when a colloid moved >= skin/10 or the solvent >= 0.9 skin */
+    double list_radius;  /* update_list radius: cut + skin */
+    double mass;         /* colloid mass of the velocity-Verlet halves */
+    int do_hydro;
+} rmpcd_ncolloids_params;
+typedef struct rmpcd_ncolloids_state {
+    int t;               /* MD steps of the current loop */
+    int last_sort;       /* t at the last sort */
+    int n_extra_sorting;
+    double e1, e2;       /* compute_force / compute_force_n2 energies */
+} rmpcd_ncolloids_state;
+int rmpcd_ncolloids_run(rmpcd_particles *solvent, rmpcd_particles *colloids, rmpcd_cells *cells,
+                        rmpcd_nlist *nlist, const rmpcd_lj *solvent_colloid, const rmpcd_lj *colloid_colloid,
+                        rmpcd_rng *rng, const rmpcd_ncolloids_params *params, int n_intervals, int thermostat,
+                        const double *T, int first_interval, int rescale_every, double T_rescale,
+                        rmpcd_ncolloids_state *state);
+
 /* Batched single_dimer_pbc: the main loop of programs/single_dimer_pbc.f90
  * (:303-443: N_MD MD steps with the program's re-sort test, then
  * random_shift, re-sort, simple_mpcd_step and refuel) for R independent

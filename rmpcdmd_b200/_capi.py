@@ -59,6 +59,20 @@ class DIMER_PARAMS(C.Structure):
     ]
 
 
+class NCOLLOIDS_PARAMS(C.Structure):
+    """rmpcd_ncolloids_params: the constants of the n_colloids_pbc loops."""
+
+    _fields_ = [("tau", C.c_double), ("N_MD", C.c_int), ("skin", C.c_double), ("list_radius", C.c_double),
+                ("mass", C.c_double), ("do_hydro", C.c_int)]
+
+
+class NCOLLOIDS_STATE(C.Structure):
+    """rmpcd_ncolloids_state: the loop counters carried between calls."""
+
+    _fields_ = [("t", C.c_int), ("last_sort", C.c_int), ("n_extra_sorting", C.c_int), ("e1", C.c_double),
+                ("e2", C.c_double)]
+
+
 CELLS_P = c_void_p
 PART_P = c_void_p
 NL_P = c_void_p
@@ -157,6 +171,9 @@ PROTOTYPES = {
     "rmpcd_bulk_set_shape": [C.c_int, C.c_int],
     "rmpcd_bulk_get_shape": [C.c_int, c_int_p],
     "rmpcd_bulk_autotune": [c_int_p, C.c_int, C.c_double, C.c_int, c_int_p, C.POINTER(C.c_float)],
+    "rmpcd_ncolloids_run": [PART_P, PART_P, CELLS_P, NL_P, LJ_P, LJ_P, RNG_P, C.POINTER(NCOLLOIDS_PARAMS),
+                            C.c_int, C.c_int, c_double_p, C.c_int, C.c_int, C.c_double,
+                            C.POINTER(NCOLLOIDS_STATE)],
     "rmpcd_dimer_batch_create": [C.POINTER(c_void_p), C.c_int, C.POINTER(c_void_p), C.POINTER(c_void_p),
                                  C.POINTER(c_void_p), C.POINTER(c_void_p), RNG_P, LJ_P, LJ_P,
                                  C.POINTER(DIMER_PARAMS)],

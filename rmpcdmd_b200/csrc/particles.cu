@@ -172,6 +172,40 @@ int fixed_order_sum(const double *a, int N, double *d_out)
     return RMPCD_OK;
 }
 
+int launch_max_disp(rmpcd_particles *p)
+{
+    cudaStream_t s = stream();
+    RMPCD_CUDA_TRY(cudaMemsetAsync(p->d_max, 0, 8, s));
+    if (p->N > 0) {
+        if (p->precision == RMPCD_FP32) {
+            PView<float> a = cur<float>(p), b = alt<float>(p);
+            k_max_disp<float><<<grid_for(p->N, 256), 256, 0, s>>>(a.pos, b.pos, a.species, p->N, p->d_max);
+        } else {
+            PView<double> a = cur<double>(p), b = alt<double>(p);
+            k_max_disp<double><<<grid_for(p->N, 256), 256, 0, s>>>(a.pos, b.pos, a.species, p->N, p->d_max);
+        }
+        RMPCD_CHECK_LAUNCH();
+    }
+    return RMPCD_OK;
+}
+
+int launch_cell_max_disp(rmpcd_cells *c, rmpcd_particles *p)
+{
+    cudaStream_t s = stream();
+    RMPCD_CUDA_TRY(cudaMemsetAsync(p->d_max, 0, 8, s));
+    if (p->precision == RMPCD_FP32) {
+        PView<float> a = cur<float>(p), b = alt<float>(p);
+        k_cell_max_disp<float><<<grid_full(c->S, 256), 256, 0, s>>>(c->count, c->start, c->is_md, c->S, a.pos,
+                                                                   b.pos, a.species, p->d_max);
+    } else {
+        PView<double> a = cur<double>(p), b = alt<double>(p);
+        k_cell_max_disp<double><<<grid_full(c->S, 256), 256, 0, s>>>(c->count, c->start, c->is_md, c->S, a.pos,
+                                                                    b.pos, a.species, p->d_max);
+    }
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
 }  // namespace rmpcd
 
 using namespace rmpcd;
@@ -444,16 +478,8 @@ int rmpcd_particles_maximum_displacement(rmpcd_particles *p, double *r)
     RMPCD_ARG(p && r, "null argument");
     PhaseTimer t("maximum disp");
     cudaStream_t s = stream();
-    RMPCD_CUDA_TRY(cudaMemsetAsync(p->d_max, 0, 8, s));
-    if (p->N > 0) {
-        if (p->precision == RMPCD_FP32) {
-            PView<float> a = cur<float>(p), b = alt<float>(p);
-            k_max_disp<float><<<grid_for(p->N, 256), 256, 0, s>>>(a.pos, b.pos, a.species, p->N, p->d_max);
-        } else {
-            PView<double> a = cur<double>(p), b = alt<double>(p);
-            k_max_disp<double><<<grid_for(p->N, 256), 256, 0, s>>>(a.pos, b.pos, a.species, p->N, p->d_max);
-        }
-    }
+    int rc0 = launch_max_disp(p);
+    if (rc0) return rc0;
     unsigned long long bits = 0;
     RMPCD_CUDA_TRY(cudaMemcpyAsync(&bits, p->d_max, 8, cudaMemcpyDeviceToHost, s));
     int rc = sync();
@@ -468,16 +494,8 @@ int rmpcd_cell_maximum_displacement(rmpcd_cells *c, rmpcd_particles *p, double d
 {
     RMPCD_ARG(c && p && r, "null argument");
     cudaStream_t s = stream();
-    RMPCD_CUDA_TRY(cudaMemsetAsync(p->d_max, 0, 8, s));
-    if (p->precision == RMPCD_FP32) {
-        PView<float> a = cur<float>(p), b = alt<float>(p);
-        k_cell_max_disp<float><<<grid_full(c->S, 256), 256, 0, s>>>(c->count, c->start, c->is_md, c->S,
-                                                                   a.pos, b.pos, a.species, p->d_max);
-    } else {
-        PView<double> a = cur<double>(p), b = alt<double>(p);
-        k_cell_max_disp<double><<<grid_full(c->S, 256), 256, 0, s>>>(c->count, c->start, c->is_md, c->S,
-                                                                    a.pos, b.pos, a.species, p->d_max);
-    }
+    int rc0 = launch_cell_max_disp(c, p);
+    if (rc0) return rc0;
     unsigned long long bits = 0;
     RMPCD_CUDA_TRY(cudaMemcpyAsync(&bits, p->d_max, 8, cudaMemcpyDeviceToHost, s));
     int rc = sync();

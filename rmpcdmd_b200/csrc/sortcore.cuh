@@ -33,6 +33,11 @@ int sort_particles(rmpcd_cells *c, rmpcd_particles *p);
 // particles (tmp: scratch of the extent of perm)
 void launch_segsort_big(const int *start, const int *count, const int *big, const int *n_big, int *perm,
                         int *tmp, cudaStream_t st);
+// maximum-displacement reductions into p->d_max (r^2 as ordered bits), no
+// synchronisation: maximum_displacement over all particles, and over the
+// particles of is_md cells (src/particle_system.f90:357-410)
+int launch_max_disp(rmpcd_particles *p);
+int launch_cell_max_disp(rmpcd_cells *c, rmpcd_particles *p);
 // largest cell handled by sort_segment; larger ones go to launch_segsort_big
 constexpr int kSmallSegmentMax = 64;
 

@@ -20,7 +20,7 @@ import ctypes as C
 import numpy as np
 
 from . import api as A
-from ._capi import DIMER_PARAMS, RNG, call, lib
+from ._capi import DIMER_PARAMS, NCOLLOIDS_PARAMS, NCOLLOIDS_STATE, RNG, call, lib
 
 PI_SP = float(np.float32(3.14159265))  # the default-real constant of the program
 TWO_SIXTH = 2.0 ** (1.0 / 6.0)
@@ -362,17 +362,35 @@ class NColloidsPBC:
         if rescale:
             A.rescale_cells(self.solvent, self.cells, self.rng, self.T_init)
 
-    def thermalise(self, n_loops):
+    def _native(self, n, thermostat, Ts, rescale_every):
+        """n intervals through rmpcd_ncolloids_run (the same calls, in C)."""
+        prm = NCOLLOIDS_PARAMS(self.tau, self.N_MD, self.skin, self.radius, self.mass, int(bool(self.do_hydro)))
+        st = NCOLLOIDS_STATE(self.t, self.last_sort, self.n_extra_sorting, self.e1 or 0.0, self.e2 or 0.0)
+        T = np.ascontiguousarray(Ts, dtype=np.float64)
+        call("rmpcd_ncolloids_run", self.solvent.handle, self.colloids.handle, self.cells.handle, self.neigh.handle,
+             C.byref(self.solvent_colloid_lj.struct), C.byref(self.colloid_lj.struct), self.rng.ptr, C.byref(prm),
+             int(n), int(bool(thermostat)), T.ctypes.data_as(C.POINTER(C.c_double)), 1, int(rescale_every),
+             float(self.T_init), C.byref(st))
+        self.t, self.last_sort, self.n_extra_sorting = st.t, st.last_sort, st.n_extra_sorting
+        self.e1, self.e2 = st.e1, st.e2
+
+    def thermalise(self, n_loops, native=True):
         """The thermostatted loop: MPC-AT at T, cell rescaling every 10 intervals."""
-        for i in range(1, n_loops + 1):
-            self.interval(True, self.T_init, rescale=(i % 10 == 0))
+        if native:
+            self._native(n_loops, True, [self.T_init] * max(1, n_loops), 10)
+        else:
+            for i in range(1, n_loops + 1):
+                self.interval(True, self.T_init, rescale=(i % 10 == 0))
         self.t = self.last_sort = 0
 
-    def run(self, n_loops):
+    def run(self, n_loops, native=True):
         """The production loop with the temperature ramp T_init -> T_final."""
-        for i in range(1, n_loops + 1):
-            T = self.T_init + (i - 1) * (self.T_final - self.T_init) / max(1, n_loops - 1)
-            self.interval(self.do_thermostat, T)
+        Ts = [self.T_init + (i - 1) * (self.T_final - self.T_init) / max(1, n_loops - 1) for i in range(1, n_loops + 1)]
+        if native:
+            self._native(n_loops, self.do_thermostat, Ts or [self.T_init], 0)
+        else:
+            for T in Ts:
+                self.interval(self.do_thermostat, T)
 
 
 def bulk_fluid(L, rho=10, T=1.0 / 3.0, tau=1.0, n_intervals=200, seed=1, precision=A.FP64, alpha=None):

@@ -119,3 +119,24 @@ def test_bulk_shapes_give_identical_results(rm, oracle, precision):
         assert len(ms) == len(shapes) and all(m > 0 for m in ms)
     finally:
         rm.set_bulk_shape(precision, keep)
+
+
+def test_n_colloids_native_loop_matches_call_by_call(rm):
+    """rmpcd_ncolloids_run issues the program's calls in C; the state after
+    thermalisation (with the 10th-interval rescaling) and a temperature ramp
+    equals the Python loop making the same calls one by one."""
+    from rmpcdmd_b200.programs import NColloidsPBC
+
+    kw = dict(L=(24, 24, 24), rho=10, N_MD=10, N_colloids=8, seed=77, T_final=0.5)
+    a = NColloidsPBC(**kw)
+    b = NColloidsPBC(**kw)
+    a.thermalise(10, native=False)
+    b.thermalise(10, native=True)
+    a.run(3, native=False)
+    b.run(3, native=True)
+    for f in ("pos", "vel", "image", "id", "flags", "force", "force_old"):
+        assert np.array_equal(a.solvent.download(f), b.solvent.download(f)), f
+    for f in ("pos", "vel", "force", "image"):
+        assert np.array_equal(a.colloids.download(f), b.colloids.download(f)), f
+    assert (a.t, a.last_sort, a.n_extra_sorting, a.rng.step) == (b.t, b.last_sort, b.n_extra_sorting, b.rng.step)
+    assert a.e1 == b.e1 and a.e2 == b.e2
