@@ -42,7 +42,7 @@
 
 namespace rmpcd {
 
-constexpr int kTile = 1024;  // particles or slots per tile
+constexpr int kTile = 1024;  // slots per slot tile; most particles per particle tile
 constexpr int kBT = 256;     // threads per tile block
 
 struct BTile {
@@ -1061,6 +1061,12 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
     b->ms.n = col[0]->n_species;
     for (int s = 0; s < RMPCD_MAX_SPECIES; s++) b->ms.m[s] = col[0]->mass[s];
     // replica layout and tiles
+    // particle tiles: 1024 particles, smaller for small batches so that the
+    // per-MD-step kernels still fill the GPU (at least ~16 tiles per SM)
+    long long n_total = 0;
+    for (int r = 0; r < R; r++) n_total += sol[r]->N;
+    long long ptile = 1024;
+    while (ptile > kBT && n_total / ptile < 16LL * sm_count()) ptile /= 2;
     std::vector<BTile> pt, stl;
     std::vector<int> sfirst(R), scount(R), pfirst(R), pcount(R);
     std::map<std::vector<int>, int *> lut_of;
@@ -1095,7 +1101,7 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
         }
         p.g.lut = lut_of[key];
         pfirst[r] = (int)pt.size();
-        for (long long t = 0; t < p.n; t += kTile) pt.push_back({r, 0, off + t, off + (t + kTile < p.n ? t + kTile : p.n)});
+        for (long long t = 0; t < p.n; t += ptile) pt.push_back({r, 0, off + t, off + (t + ptile < p.n ? t + ptile : p.n)});
         pcount[r] = (int)pt.size() - pfirst[r];
         sfirst[r] = (int)stl.size();
         for (long long t = 0; t < p.S; t += kTile) stl.push_back({r, 0, soff + t, soff + (t + kTile < p.S ? t + kTile : p.S)});

@@ -371,8 +371,10 @@ __device__ inline void colloid_sum_block(int i, const int *n, int Nmax, const un
         }
         __syncthreads();
         const int cnt = s_cnt;
-        if (t < 3)
+        if (t < 3) {
+#pragma unroll 8
             for (int k = 0; k < cnt; k++) acc = acc + vals[t][k];
+        }
         for (int k = t; k < cnt; k += kNlBlockThreads) clist[(size_t)i * Nmax + total + k] = idxs[k];
         total += cnt;
         __syncthreads();
