@@ -1,10 +1,17 @@
 // The main loops of programs/n_colloids_pbc.f90 (:221-276 thermalisation,
 // :304-324 production) as one native call: passive LJ colloids in an SRD
-// fluid with lazy, cell-wise solvent streaming.  The loop issues the same
-// module entry points, in the same order, as a program calling them one by
-// one (and as rmpcdmd_b200.programs.NColloidsPBC.interval does), so the
-// results are identical; it removes the per-call host overhead and reads the
-// two displacement maxima of each MD step with a single synchronisation.
+// fluid with lazy, cell-wise solvent streaming.  The loop performs the
+// program's steps in the program's order, so the results are those of the
+// module entry points called one by one (rmpcdmd_b200.programs.NColloidsPBC
+// .interval does exactly that); it differs in how the work is issued:
+//   * the MD cells (is_md) are listed once per neighbor-list update, and the
+//     per-MD-step cell_md_pos / cell_md_vel / cell_maximum_displacement run
+//     over that list instead of over every slot;
+//   * zero_force of the solvent and the PAST_MD/MD roll of compute_force are
+//     one pass that clears only the force entries that can be non-zero
+//     (particles with MD or PAST_MD set: every other entry is exactly zero);
+//   * the two displacement maxima of an MD step are read with one
+//     synchronisation, and there is no per-call host overhead.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -12,9 +19,117 @@
 #include "rmpcd_common.cuh"
 #include "sortcore.cuh"
 #include "state.cuh"
+#include "stepops.cuh"
 #include "timers.cuh"
 
 namespace rmpcd {
+
+// the is_md slots, in any order (one atomic per warp)
+__global__ void k_md_slot_list(const unsigned char *is_md, int S, int *list, int *n_list)
+{
+    const int lane = threadIdx.x & 31;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < S; base += (long long)gridDim.x * blockDim.x) {
+        const long long s = base + threadIdx.x;
+        const bool md = s < S && is_md[s];
+        const unsigned bal = __ballot_sync(0xffffffffu, md);
+        int b = 0;
+        if (lane == 0 && bal) b = atomicAdd(n_list, __popc(bal));
+        b = __shfl_sync(0xffffffffu, b, 0);
+        if (md) list[b + __popc(bal & ((1u << lane) - 1u))] = (int)s;
+    }
+}
+
+// cell_md_pos / cell_md_vel with md_flag = .true. (src/md.f90:79-102,
+// :239-263), one thread per listed cell
+template <typename R>
+__global__ void k_md_cells_pos(const int *list, const int *n_list, const int *count, const int *start, PView<R> v,
+                               R dt, R dt_sq)
+{
+    const int n = *n_list;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int s = list[k], a = start[s], c = count[s];
+#pragma unroll 4
+        for (int i = a; i < a + c; i++) md_pos_one(v, i, dt, dt_sq);
+    }
+}
+
+template <typename R>
+__global__ void k_md_cells_vel(const int *list, const int *n_list, const int *count, const int *start, PView<R> v,
+                               R dt)
+{
+    const int n = *n_list;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int s = list[k], a = start[s], c = count[s];
+#pragma unroll 4
+        for (int i = a; i < a + c; i++) md_vel_one(v, i, dt);
+    }
+}
+
+// the catch-up of cell_md_pos / cell_md_vel with md_flag = .false. over every
+// non-MD cell, eight lanes per cell so that a cell's particles are read
+// together
+constexpr int kLanesPerCell = 8;
+
+template <typename R>
+__global__ void k_other_cells_pos(const int *count, const int *start, const unsigned char *is_md, int S, PView<R> v,
+                                  R dt, R dt_sq)
+{
+    const long long nthreads = (long long)gridDim.x * blockDim.x;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < (long long)S * kLanesPerCell;
+         q += nthreads) {
+        const int s = (int)(q / kLanesPerCell), g = (int)(q % kLanesPerCell);
+        if (is_md[s]) continue;
+        const int a = start[s], c = count[s];
+        for (int i = a + g; i < a + c; i += kLanesPerCell) md_pos_one(v, i, dt, dt_sq);
+    }
+}
+
+template <typename R>
+__global__ void k_other_cells_vel(const int *count, const int *start, const unsigned char *is_md, int S, PView<R> v,
+                                  R dt)
+{
+    const long long nthreads = (long long)gridDim.x * blockDim.x;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < (long long)S * kLanesPerCell;
+         q += nthreads) {
+        const int s = (int)(q / kLanesPerCell), g = (int)(q % kLanesPerCell);
+        if (is_md[s]) continue;
+        const int a = start[s], c = count[s];
+        for (int i = a + g; i < a + c; i += kLanesPerCell) md_vel_one(v, i, dt);
+    }
+}
+
+// cell_maximum_displacement over the listed cells (src/particle_system.f90:380-410)
+template <typename R>
+__global__ void k_md_cells_max_disp(const int *list, const int *n_list, const int *count, const int *start,
+                                    Vec3<R> pos, Vec3<R> old, const int *species, unsigned long long *out)
+{
+    const int n = *n_list;
+    double m = 0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int s = list[k], a = start[s], c = count[s];
+        for (int i = a; i < a + c; i++) {
+            const double r = disp_sq_one(pos, old, species, i);
+            m = m > r ? m : r;
+        }
+    }
+    warp_max_into(out, m);
+}
+
+// zero_force of the solvent fused with the PAST_MD/MD roll: only entries of
+// particles with MD or PAST_MD set can be non-zero
+template <typename R>
+__global__ void k_roll_clear(int *flags, Vec3<R> force, long long N)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        const int f = flags[i];
+        if (f & ((1 << MD_BIT) | (1 << PAST_MD_BIT))) {
+            force.x[i] = 0;
+            force.y[i] = 0;
+            force.z[i] = 0;
+            flag_roll_one(flags, i);
+        }
+    }
+}
 
 struct NcLoop {
     rmpcd_particles *s, *c;
@@ -26,16 +141,84 @@ struct NcLoop {
     rmpcd_ncolloids_state *st;
     std::vector<double> vv_mass;
     double dt;
+    int *md_list = nullptr;  // is_md slots
+    int *n_md = nullptr;     // their number (device)
+    unsigned long long *h_max = nullptr;  // page-locked landing of the two maxima
 };
+
+// list the MD cells after a neighbor-list update
+static int list_md_cells(NcLoop &L)
+{
+    cudaStream_t st = stream();
+    RMPCD_CUDA_TRY(cudaMemsetAsync(L.n_md, 0, sizeof(int), st));
+    k_md_slot_list<<<grid_for(L.cells->S, 256), 256, 0, st>>>(L.cells->is_md, L.cells->S, L.md_list, L.n_md);
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+template <typename R>
+static int md_cells_pos_t(NcLoop &L)
+{
+    const R dt = (R)L.dt, dt_sq = (R)(L.dt * L.dt / 2);
+    k_md_cells_pos<R><<<sm_count() * 8, 128, 0, stream()>>>(L.md_list, L.n_md, L.cells->count,
+                                                                       L.cells->start, cur<R>(L.s), dt, dt_sq);
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+template <typename R>
+static int md_cells_vel_t(NcLoop &L)
+{
+    k_md_cells_vel<R><<<sm_count() * 8, 128, 0, stream()>>>(L.md_list, L.n_md, L.cells->count,
+                                                                       L.cells->start, cur<R>(L.s), (R)L.dt);
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+template <typename R>
+static int md_cells_max_disp_t(NcLoop &L)
+{
+    cudaStream_t st = stream();
+    RMPCD_CUDA_TRY(cudaMemsetAsync(L.s->d_max, 0, 8, st));
+    PView<R> a = cur<R>(L.s), b = alt<R>(L.s);
+    k_md_cells_max_disp<R><<<sm_count() * 4, 256, 0, st>>>(L.md_list, L.n_md, L.cells->count,
+                                                                      L.cells->start, a.pos, b.pos, a.species,
+                                                                      L.s->d_max);
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+template <typename R>
+static int roll_clear_t(NcLoop &L)
+{
+    PView<R> v = cur<R>(L.s);
+    if (L.s->N > 0) k_roll_clear<R><<<grid_for(L.s->N, 256), 256, 0, stream()>>>(v.flags, v.force, L.s->N);
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+template <typename R>
+static int other_cells_t(NcLoop &L, double dtl)
+{
+    const double dt_sq = dtl * dtl / 2;
+    const int g = grid_full((long long)L.cells->S * kLanesPerCell, 256);
+    rmpcd_cells *c = L.cells;
+    k_other_cells_pos<R><<<g, 256, 0, stream()>>>(c->count, c->start, c->is_md, c->S, cur<R>(L.s), (R)dtl, (R)dt_sq);
+    k_other_cells_vel<R><<<g, 256, 0, stream()>>>(c->count, c->start, c->is_md, c->S, cur<R>(L.s), (R)dtl);
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+#define NC_DISPATCH(L, fn) ((L).s->precision == RMPCD_FP32 ? fn<float>(L) : fn<double>(L))
 
 // the displacement maxima of the MD step: solvent over is_md cells (floored
 // at max_v * delta_t) and colloids, read with one synchronisation
 static int displacements(NcLoop &L, double delta_t, double *so_max, double *co_max)
 {
-    int rc = launch_cell_max_disp(L.cells, L.s);
+    int rc = NC_DISPATCH(L, md_cells_max_disp_t);
     if (!rc) rc = launch_max_disp(L.c);
     if (rc) return rc;
-    unsigned long long bits[2] = {0, 0};
+    unsigned long long *bits = L.h_max;
     RMPCD_CUDA_TRY(cudaMemcpyAsync(bits, L.s->d_max, 8, cudaMemcpyDeviceToHost, stream()));
     RMPCD_CUDA_TRY(cudaMemcpyAsync(bits + 1, L.c->d_max, 8, cudaMemcpyDeviceToHost, stream()));
     rc = sync();
@@ -54,13 +237,13 @@ static int displacements(NcLoop &L, double delta_t, double *so_max, double *co_m
 static int catch_up_and_sort(NcLoop &L)
 {
     const double dtl = (L.st->t - L.st->last_sort) * L.dt;
-    int rc = rmpcd_cell_md_pos(L.cells, L.s, dtl, 0);
-    if (!rc) rc = rmpcd_cell_md_vel(L.cells, L.s, dtl, 0);
+    int rc = L.s->precision == RMPCD_FP32 ? other_cells_t<float>(L, dtl) : other_cells_t<double>(L, dtl);
     if (!rc) rc = rmpcd_apply_pbc(L.s, L.cells->edges);
     if (!rc) rc = rmpcd_apply_pbc(L.c, L.cells->edges);
     if (!rc) rc = rmpcd_particles_sort(L.s, L.cells);
     L.st->last_sort = L.st->t;
     if (!rc) rc = rmpcd_nlist_update(L.nl, L.c, L.s, L.prm->list_radius, L.cells, nullptr);
+    if (!rc) rc = list_md_cells(L);
     if (!rc) rc = rmpcd_particles_copy_pos_old(L.s);
     if (!rc) rc = rmpcd_particles_copy_pos_old(L.c);
     return rc;
@@ -71,7 +254,7 @@ static int md_step(NcLoop &L, bool want_energy)
 {
     const double dt = L.dt;
     L.st->t += 1;
-    int rc = rmpcd_cell_md_pos(L.cells, L.s, dt, 1);
+    int rc = NC_DISPATCH(L, md_cells_pos_t);
     if (!rc) rc = rmpcd_colloid_vv_pos(L.c, dt, L.vv_mass.data());
     double so_max = 0, co_max = 0;
     if (!rc) rc = displacements(L, dt * (L.st->t - L.st->last_sort), &so_max, &co_max);
@@ -83,16 +266,16 @@ static int md_step(NcLoop &L, bool want_energy)
     }
     rc = rmpcd_particles_switch_force(L.s);
     if (!rc) rc = rmpcd_particles_switch_force(L.c);
-    if (!rc) rc = rmpcd_particles_zero_force(L.s);
+    if (!rc) rc = NC_DISPATCH(L, roll_clear_t);
     if (!rc) rc = rmpcd_particles_zero_force(L.c);
     double e1 = 0, e2 = 0;
-    if (!rc) rc = rmpcd_compute_force(L.c, L.s, L.nl, L.cells->edges, L.lj_sc, want_energy ? &e1 : nullptr);
+    if (!rc) rc = compute_force_impl(L.c, L.s, L.nl, L.cells->edges, L.lj_sc, want_energy ? &e1 : nullptr, false);
     if (!rc) rc = rmpcd_compute_force_n2(L.c, L.cells->edges, L.lj_cc, want_energy ? &e2 : nullptr);
     if (!rc && want_energy) {
         L.st->e1 = e1;
         L.st->e2 = e2;
     }
-    if (!rc) rc = rmpcd_cell_md_vel(L.cells, L.s, dt, 1);
+    if (!rc) rc = NC_DISPATCH(L, md_cells_vel_t);
     if (!rc) rc = rmpcd_colloid_vv_vel(L.c, dt, L.vv_mass.data());
     return rc;
 }
@@ -125,18 +308,29 @@ extern "C" int rmpcd_ncolloids_run(rmpcd_particles *solvent, rmpcd_particles *co
     L.vv_mass.assign((size_t)colloids->N, params->mass);
     L.dt = params->tau / params->N_MD;
     PhaseTimer timer("ncolloids_run");
-    for (int k = 0; k < n_intervals; k++) {
+    RMPCD_CUDA_TRY(cudaMalloc(&L.md_list, (size_t)(cells->S > 0 ? cells->S : 1) * sizeof(int)));
+    if (cudaMalloc(&L.n_md, sizeof(int)) != cudaSuccess ||
+        cudaHostAlloc(&L.h_max, 2 * sizeof(unsigned long long), cudaHostAllocDefault) != cudaSuccess) {
+        cudaFree(L.md_list);
+        cudaFree(L.n_md);
+        return fail(RMPCD_ERR_CUDA, "rmpcd_ncolloids_run: allocation failed");
+    }
+    int rc0 = list_md_cells(L);
+    for (int k = 0; !rc0 && k < n_intervals; k++) {
         const int i = first_interval + k;
-        for (int j = 0; j < params->N_MD; j++) {
-            int rc = md_step(L, j == params->N_MD - 1);
-            if (rc) return rc;
-        }
-        int rc = rmpcd_cells_random_shift(cells, rng);
+        int rc = 0;
+        for (int j = 0; !rc && j < params->N_MD; j++) rc = md_step(L, j == params->N_MD - 1);
+        if (!rc) rc = rmpcd_cells_random_shift(cells, rng);
         if (!rc) rc = catch_up_and_sort(L);
         if (!rc)
             rc = rmpcd_simple_mpcd_step(solvent, cells, rng, 0, 0.0, thermostat, T ? T[k] : 0.0, params->do_hydro);
         if (!rc && rescale_every > 0 && i % rescale_every == 0) rc = rmpcd_rescale_cells(solvent, cells, T_rescale);
-        if (rc) return rc;
+        rc0 = rc;
     }
+    cudaStreamSynchronize(stream());
+    cudaFree(L.md_list);
+    cudaFree(L.n_md);
+    cudaFreeHost(L.h_max);
+    if (rc0) return rc0;
     return check_dev_error(nullptr);
 }

@@ -13,6 +13,7 @@
 
 #include "keys.cuh"
 #include "nlist_ops.cuh"
+#include "sortcore.cuh"
 #include "rmpcd_common.cuh"
 #include "state.cuh"
 #include "stepops.cuh"
@@ -309,6 +310,16 @@ int rmpcd_nlist_download(const rmpcd_nlist *nl, int *list, int *n)
 int rmpcd_compute_force(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist *nl, const double L[3],
                         const rmpcd_lj *lj, double *energy)
 {
+    return compute_force_impl(ps1, ps2, nl, L, lj, energy, true);
+}
+
+}  // extern "C"
+
+namespace rmpcd {
+
+int compute_force_impl(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist *nl, const double L[3],
+                       const rmpcd_lj *lj, double *energy, bool roll_flags)
+{
     RMPCD_ARG(ps1 && ps2 && nl && L && lj, "null argument");
     RMPCD_ARG(ps1->precision == RMPCD_FP64, "compute_force: ps1 (colloids) must be FP64");
     RMPCD_ARG(ps1->N == nl->Npoints, "compute_force: ps1 size differs from Npoints");
@@ -317,7 +328,7 @@ int rmpcd_compute_force(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist 
     PhaseTimer tm("neigh list force");
     cudaStream_t s = stream();
     int C = ps1->N;
-    if (ps2->N > 0) k_flag_roll<<<grid_for(ps2->N, 256), 256, 0, s>>>(ps2->flags[ps2->cur], ps2->N);
+    if (roll_flags && ps2->N > 0) k_flag_roll<<<grid_for(ps2->N, 256), 256, 0, s>>>(ps2->flags[ps2->cur], ps2->N);
     int *max_contrib = nl->d_status;
     int *m_count = nl->d_status + 1;  // multi-contribution keys collected (reset by k_apply_multi)
     int *cn = nl->d_status + 16;
@@ -374,6 +385,10 @@ int rmpcd_compute_force(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist 
     }
     return RMPCD_OK;
 }
+
+}  // namespace rmpcd
+
+extern "C" {
 
 // compute_force_n2, src/neighbor_list.f90:227-264
 int rmpcd_compute_force_n2(rmpcd_particles *ps, const double L[3], const rmpcd_lj *lj, double *energy)

@@ -38,6 +38,10 @@ void launch_segsort_big(const int *start, const int *count, const int *big, cons
 // particles of is_md cells (src/particle_system.f90:357-410)
 int launch_max_disp(rmpcd_particles *p);
 int launch_cell_max_disp(rmpcd_cells *c, rmpcd_particles *p);
+// compute_force (src/neighbor_list.f90:159-225); roll_flags = false leaves
+// the PAST_MD/MD roll to the caller (which must then have done it)
+int compute_force_impl(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist *nl, const double L[3],
+                       const rmpcd_lj *lj, double *energy, bool roll_flags);
 // largest cell handled by sort_segment; larger ones go to launch_segsort_big
 constexpr int kSmallSegmentMax = 64;
 
