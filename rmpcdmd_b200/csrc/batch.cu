@@ -257,7 +257,7 @@ struct ResortLists {
 // re-sort test, lists the tiles of the replicas to re-sort and raises the
 // graph's re-sort condition when there are any
 template <typename R>
-__global__ void __launch_bounds__(kBT, 6)
+__global__ void __launch_bounds__(kBT, 4)
     kb_step_begin(const BTile *tiles, const BRep *rep, PView<R> v, Vec3<R> old, Vec3<R> next, R dt, R dt_sq,
                   unsigned long long *so_max, unsigned *done, int *resort, int *n_extra, ColloidStep cs,
                   ResortLists rl, cudaGraphConditionalHandle cond, int use_cond, unsigned *err)
@@ -267,26 +267,48 @@ __global__ void __launch_bounds__(kBT, 6)
     __shared__ double s_max[kBT / 32];
     const BTile t = tiles[blockIdx.x];
     double m = 0;
-    for (long long i = t.begin + threadIdx.x; i < t.end; i += blockDim.x) {
-        const int f = v.flags[i];
-        const int sp = v.species[i];
-        R px = v.pos.x[i], py = v.pos.y[i], pz = v.pos.z[i];
-        const R vx = v.vel.x[i], vy = v.vel.y[i], vz = v.vel.z[i];
-        const R ox = old.x[i], oy = old.y[i], oz = old.z[i];
-        const bool md = (f >> MD_BIT) & 1, past = (f >> PAST_MD_BIT) & 1;
-        const R fx = flagged(v.force.x, i, md), fy = flagged(v.force.y, i, md), fz = flagged(v.force.z, i, md);
-        px = px + dt * vx + dt_sq * fx;
-        py = py + dt * vy + dt_sq * fy;
-        pz = pz + dt * vz + dt_sq * fz;
-        v.pos.x[i] = px;
-        v.pos.y[i] = py;
-        v.pos.z[i] = pz;
-        if (past) next.x[i] = next.y[i] = next.z[i] = 0;
-        if (md || past) flag_roll_one(v.flags, i);
-        if (sp >= 0) {
-            double d0 = (double)px - (double)ox, d1 = (double)py - (double)oy, d2 = (double)pz - (double)oz;
-            double r = d0 * d0 + d1 * d1 + d2 * d2;
-            m = m > r ? m : r;
+    // K particles per thread and pass, all loads issued before any use
+    constexpr int K = sizeof(R) == 4 ? 4 : 2;
+    for (long long base = t.begin + threadIdx.x; base < t.end; base += (long long)K * blockDim.x) {
+        int f[K], sp[K];
+        R px[K], py[K], pz[K], vx[K], vy[K], vz[K], ox[K], oy[K], oz[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const long long i = base + (long long)k * blockDim.x;
+            if (i < t.end) {
+                f[k] = v.flags[i];
+                sp[k] = v.species[i];
+                px[k] = v.pos.x[i];
+                py[k] = v.pos.y[i];
+                pz[k] = v.pos.z[i];
+                vx[k] = v.vel.x[i];
+                vy[k] = v.vel.y[i];
+                vz[k] = v.vel.z[i];
+                ox[k] = old.x[i];
+                oy[k] = old.y[i];
+                oz[k] = old.z[i];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const long long i = base + (long long)k * blockDim.x;
+            if (i >= t.end) continue;
+            const bool md = (f[k] >> MD_BIT) & 1, past = (f[k] >> PAST_MD_BIT) & 1;
+            const R fx = flagged(v.force.x, i, md), fy = flagged(v.force.y, i, md), fz = flagged(v.force.z, i, md);
+            const R qx = px[k] + dt * vx[k] + dt_sq * fx;
+            const R qy = py[k] + dt * vy[k] + dt_sq * fy;
+            const R qz = pz[k] + dt * vz[k] + dt_sq * fz;
+            v.pos.x[i] = qx;
+            v.pos.y[i] = qy;
+            v.pos.z[i] = qz;
+            if (past) next.x[i] = next.y[i] = next.z[i] = 0;
+            if (md || past) flag_roll_one(v.flags, i);
+            if (sp[k] >= 0) {
+                double d0 = (double)qx - (double)ox[k], d1 = (double)qy - (double)oy[k],
+                       d2 = (double)qz - (double)oz[k];
+                double r = d0 * d0 + d1 * d1 + d2 * d2;
+                m = m > r ? m : r;
+            }
         }
     }
     m = warp_max(m);
@@ -383,7 +405,7 @@ __global__ void kb_apply_sum(const BRep *rep, int R_, int gx, const int *list, c
 // RATTLE's velocity correction per replica (src/neighbor_list.f90:227-264,
 // programs/single_dimer_pbc.f90:356-359, src/md.f90:298-319)
 template <typename R>
-__global__ void __launch_bounds__(kBT, 6)
+__global__ void __launch_bounds__(kBT, 4)
     kb_step_end(const BTile *tiles, int n_tiles, int gx, const BRep *rep, PView<R> v, PView<double> c, R dt,
                 double cut_c, double cut_n, double prob, const uint64_t *d_step, int step_off, const int *list,
                 const int *n, int Nmax, const unsigned char *contrib, int *ncontrib, int *max_contrib,
@@ -399,9 +421,26 @@ __global__ void __launch_bounds__(kBT, 6)
         const uint64_t step = *d_step + (uint64_t)step_off;
         const uint64_t seed = rp.seed;
         const long long off = rp.off;
-        for (long long i = t.begin + threadIdx.x; i < t.end; i += blockDim.x) {
-            int f = v.flags[i];
-            const R vx = v.vel.x[i], vy = v.vel.y[i], vz = v.vel.z[i];
+        constexpr int K = 4;
+        for (long long base = t.begin + threadIdx.x; base < t.end; base += (long long)K * blockDim.x) {
+          int fk[K];
+          R vxk[K], vyk[K], vzk[K];
+#pragma unroll
+          for (int k = 0; k < K; k++) {
+            const long long i = base + (long long)k * blockDim.x;
+            if (i < t.end) {
+                fk[k] = v.flags[i];
+                vxk[k] = v.vel.x[i];
+                vyk[k] = v.vel.y[i];
+                vzk[k] = v.vel.z[i];
+            }
+          }
+#pragma unroll
+          for (int k = 0; k < K; k++) {
+            const long long i = base + (long long)k * blockDim.x;
+            if (i >= t.end) continue;
+            int f = fk[k];
+            const R vx = vxk[k], vy = vyk[k], vz = vzk[k];
             if (!((f >> WALL_BIT) & 1)) {
                 const bool md = (f >> MD_BIT) & 1, past = (f >> PAST_MD_BIT) & 1;
                 if (md || past) {
@@ -428,6 +467,7 @@ __global__ void __launch_bounds__(kBT, 6)
             }
             if ((f >> REAC_BIT) & 1)
                 change_species_one(v, i, i - off, a, bb, L0, L1, L2, cut_c, cut_n, prob, seed, step);
+          }
         }
         return;
     }
