@@ -270,7 +270,7 @@ def run_dimer(rm, peak, peak_kind, local):
     # n_colloids_pbc: 200 passive colloids (sigma 3) in 128^3, the program's
     # loop call by call through the C ABI (lazy cell-wise streaming)
     from rmpcdmd_b200.programs import NColloidsPBC
-    for prec in (64, 32):
+    for prec in (32, 64):
         g = NColloidsPBC(L=(128, 128, 128), rho=RHO, N_MD=DIMER_N_MD, N_colloids=200, seed=SEED,
                          volume_correction=False, precision=prec)
         g.thermalise(1)
