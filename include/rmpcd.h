@@ -218,6 +218,10 @@ int rmpcd_mpcd_stream_nogravity_zwall(rmpcd_particles *p, rmpcd_cells *cells, do
 /* bulk_reaction, src/mpcd.f90:605-643 */
 int rmpcd_bulk_reaction(rmpcd_particles *p, rmpcd_cells *cells, int from, int to,
                         double rate, double tau, rmpcd_rng *rng);
+/* bulk_reaction_endothermic, src/mpcd.f90:645-700 (the reaction also needs the
+ * cell's relative kinetic energy to exceed delta_u, and removes delta_u from it) */
+int rmpcd_bulk_reaction_endothermic(rmpcd_particles *p, rmpcd_cells *cells, int from, int to,
+                                    double rate, double tau, double delta_u, rmpcd_rng *rng);
 
 /* ------------------------------------------------------------------ */
 /* MD, src/md.f90                                                       */

@@ -274,6 +274,12 @@ def bulk_reaction(p: Particles, c: Cells, frm, to, rate, tau, seed, step):
                             C.c_uint64(step))
 
 
+def bulk_reaction_endothermic(p: Particles, c: Cells, frm, to, rate, tau, delta_u, seed, step):
+    lib().orc_bulk_reaction_endothermic(C.byref(c.g), p.N, ip(c.cell_count), ip(c.cell_start), up(c.is_reac),
+                                        ip(p.species), dp(p.vel), int(frm), int(to), C.c_double(rate),
+                                        C.c_double(tau), C.c_double(delta_u), C.c_uint64(seed), C.c_uint64(step))
+
+
 def md_pos(p: Particles, dt):
     lib().orc_md_pos(p.N, dp(p.pos), dp(p.vel), dp(p.force), C.c_double(dt))
 

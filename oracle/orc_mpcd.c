@@ -411,3 +411,54 @@ void orc_bulk_reaction(const orc_grid *g, int N, const int *cell_count,
         if (u[0] < (1 - exp(-local_rate * tau)) && pick >= 0) species[pick] = to;
     }
 }
+
+/* bulk_reaction_endothermic, src/mpcd.f90:645-700.  com_v is the plain mean of
+ * the cell's velocities (:675-682), kin the sum of |v - com_v|^2 / 2 (:684-688),
+ * with sum() over the three components taken left to right; the uniform is
+ * drawn only when the cell can react (:690-692), and the rescale is
+ * v = com_v + factor (v - com_v) with factor = sqrt((kin - delta_u) / kin)
+ * (:693-698). */
+void orc_bulk_reaction_endothermic(const orc_grid *g, int N, const int *cell_count,
+                                   const int *cell_start, const unsigned char *is_reac,
+                                   int *species, double *vel, int from, int to,
+                                   double rate, double tau, double delta_u,
+                                   uint64_t seed, uint64_t step)
+{
+    (void)N;
+    for (int s = 0; s < g->S; s++) {
+        if ((cell_count[s] <= 1) || !is_reac[s]) continue;
+        int start = cell_start[s] - 1;
+        int n = cell_count[s];
+        double local_rate = 0;
+        int pick = -1;
+        double com_v[3] = {0, 0, 0};
+        for (int i = start; i < start + n; i++) {
+            if (species[i] == from) {
+                local_rate = local_rate + 1;
+                pick = i;
+            }
+            for (int k = 0; k < 3; k++) com_v[k] = com_v[k] + vel[3 * (size_t)i + k];
+        }
+        for (int k = 0; k < 3; k++) com_v[k] = com_v[k] / n;
+        double kin = 0;
+        for (int i = start; i < start + n; i++) {
+            double d0 = vel[3 * (size_t)i] - com_v[0];
+            double d1 = vel[3 * (size_t)i + 1] - com_v[1];
+            double d2 = vel[3 * (size_t)i + 2] - com_v[2];
+            kin = kin + ((d0 * d0 + d1 * d1) + d2 * d2);
+        }
+        kin = kin / 2;
+        if ((local_rate > 0) && (kin > delta_u)) {
+            local_rate = local_rate * rate;
+            double u[2];
+            orc_rng_u2(seed, step, (uint32_t)s, ORC_RNG_BULK, 0, u);
+            if (u[0] < (1 - exp(-local_rate * tau))) {
+                species[pick] = to;
+                double factor = sqrt((kin - delta_u) / kin);
+                for (int i = start; i < start + n; i++)
+                    for (int k = 0; k < 3; k++)
+                        vel[3 * (size_t)i + k] = com_v[k] + factor * (vel[3 * (size_t)i + k] - com_v[k]);
+            }
+        }
+    }
+}

@@ -146,6 +146,12 @@ void orc_bulk_reaction(const orc_grid *g, int N, const int *cell_count,
                        const int *cell_start, const unsigned char *is_reac,
                        int *species, int from, int to, double rate, double tau,
                        uint64_t seed, uint64_t step);
+/* bulk_reaction_endothermic, src/mpcd.f90:645-700 */
+void orc_bulk_reaction_endothermic(const orc_grid *g, int N, const int *cell_count,
+                                   const int *cell_start, const unsigned char *is_reac,
+                                   int *species, double *vel, int from, int to,
+                                   double rate, double tau, double delta_u,
+                                   uint64_t seed, uint64_t step);
 
 /* ---------------- MD (src/md.f90) ---------------- */
 void orc_md_pos(int N, double *pos, const double *vel, const double *force, double dt);

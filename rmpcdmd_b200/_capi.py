@@ -138,6 +138,8 @@ PROTOTYPES = {
     "rmpcd_mpcd_stream_xforce_yzwall": [PART_P, CELLS_P, C.c_double, C.c_double],
     "rmpcd_mpcd_stream_nogravity_zwall": [PART_P, CELLS_P, C.c_double],
     "rmpcd_bulk_reaction": [PART_P, CELLS_P, C.c_int, C.c_int, C.c_double, C.c_double, RNG_P],
+    "rmpcd_bulk_reaction_endothermic": [PART_P, CELLS_P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                        RNG_P],
     "rmpcd_md_pos": [PART_P, C.c_double],
     "rmpcd_md_vel": [PART_P, C.c_double],
     "rmpcd_cell_md_pos": [CELLS_P, PART_P, C.c_double, C.c_int],

@@ -37,7 +37,7 @@ __all__ = [
     "PAST_MD_BIT", "CATALYZED_BIT", "RmpcdError", "Rng", "LJParams", "CellSystem", "ParticleSystem",
     "NeighborList", "compact_p_to_h", "compact_h_to_p", "simple_mpcd_step", "wall_mpcd_step",
     "compute_temperature", "rescale_cells", "mpcd_stream_periodic", "mpcd_stream_xforce_yzwall",
-    "mpcd_stream_nogravity_zwall", "bulk_reaction", "md_pos", "md_vel", "cell_md_pos", "cell_md_vel",
+    "mpcd_stream_nogravity_zwall", "bulk_reaction", "bulk_reaction_endothermic", "md_pos", "md_vel", "cell_md_pos", "cell_md_vel",
     "cell_md_pos_ywall", "cell_md_pos_zwall", "apply_pbc", "rattle_dimer_pos", "rattle_dimer_vel",
     "colloid_vv_pos", "colloid_vv_vel", "compute_force", "compute_force_n2", "flag_particles_nl",
     "change_species", "refuel", "n_solvent", "cylindrical_shell_histogram", "velocity_sums",
@@ -472,6 +472,13 @@ def mpcd_stream_nogravity_zwall(particles: ParticleSystem, cells: CellSystem, dt
 
 def bulk_reaction(p: ParticleSystem, c: CellSystem, frm: int, to: int, rate: float, tau: float, state: Rng) -> None:
     call("rmpcd_bulk_reaction", p.handle, c.handle, int(frm), int(to), float(rate), float(tau), state.ptr)
+
+
+def bulk_reaction_endothermic(p: ParticleSystem, c: CellSystem, frm: int, to: int, rate: float, tau: float,
+                              state: Rng, delta_u: float) -> None:
+    """src/mpcd.f90:645-700 (argument order of the reference: ..., state, delta_u)."""
+    call("rmpcd_bulk_reaction_endothermic", p.handle, c.handle, int(frm), int(to), float(rate), float(tau),
+         float(delta_u), state.ptr)
 
 
 def md_pos(particles: ParticleSystem, dt: float) -> None:

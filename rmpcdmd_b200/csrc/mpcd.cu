@@ -371,6 +371,57 @@ __global__ void k_bulk_reaction(const int *__restrict__ count, const int *__rest
     }
 }
 
+// bulk_reaction_endothermic, src/mpcd.f90:645-700: the reaction needs
+// kin = sum |v - com_v|^2 / 2 > delta_u in the cell and, when it fires, takes
+// delta_u from the cell's relative kinetic energy by scaling v - com_v.  Sums
+// run in the cell's particle order, as the reference's per-cell loop does.
+template <typename R>
+__global__ void k_bulk_reaction_endo(const int *__restrict__ count, const int *__restrict__ start,
+                                     const unsigned char *__restrict__ is_reac, int S, PView<R> v, int from,
+                                     int to, double rate, double tau, double delta_u, uint64_t seed,
+                                     uint64_t step)
+{
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
+        if ((count[s] <= 1) || !is_reac[s]) continue;
+        int a = start[s], n = count[s];
+        double local_rate = 0;
+        int pick = -1;
+        double cx = 0, cy = 0, cz = 0;
+        for (int i = a; i < a + n; i++) {
+            if (v.species[i] == from) {
+                local_rate = local_rate + 1;
+                pick = i;
+            }
+            cx = cx + (double)v.vel.x[i];
+            cy = cy + (double)v.vel.y[i];
+            cz = cz + (double)v.vel.z[i];
+        }
+        cx = cx / n;
+        cy = cy / n;
+        cz = cz / n;
+        double kin = 0;
+        for (int i = a; i < a + n; i++) {
+            double dx = (double)v.vel.x[i] - cx, dy = (double)v.vel.y[i] - cy, dz = (double)v.vel.z[i] - cz;
+            kin = kin + ((dx * dx + dy * dy) + dz * dz);
+        }
+        kin = kin / 2;
+        if ((local_rate > 0) && (kin > delta_u)) {
+            local_rate = local_rate * rate;
+            double u0, u1;
+            rng::uniform2(seed, step, (uint32_t)s, rng::BULK, 0, u0, u1);
+            if (u0 < (1 - exp(-local_rate * tau))) {
+                v.species[pick] = to;
+                double factor = sqrt((kin - delta_u) / kin);
+                for (int i = a; i < a + n; i++) {
+                    v.vel.x[i] = (R)(cx + factor * ((double)v.vel.x[i] - cx));
+                    v.vel.y[i] = (R)(cy + factor * ((double)v.vel.y[i] - cy));
+                    v.vel.z[i] = (R)(cz + factor * ((double)v.vel.z[i] - cz));
+                }
+            }
+        }
+    }
+}
+
 static SrdParams srd_params(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r, int has_alpha,
                             double alpha, int thermostat, double T, int hydro)
 {
@@ -539,6 +590,23 @@ int rmpcd_bulk_reaction(rmpcd_particles *p, rmpcd_cells *c, int from, int to, do
     k_bulk_reaction<<<grid_full(c->S, 128), 128, 0, stream()>>>(c->count, c->start, c->is_reac, c->S,
                                                                p->species[p->cur], from, to, rate, tau,
                                                                r->seed, r->step);
+    RMPCD_CHECK_LAUNCH();
+    r->step++;
+    return RMPCD_OK;
+}
+
+int rmpcd_bulk_reaction_endothermic(rmpcd_particles *p, rmpcd_cells *c, int from, int to, double rate,
+                                    double tau, double delta_u, rmpcd_rng *r)
+{
+    RMPCD_ARG(p && c && r, "null argument");
+    int gr = grid_full(c->S, 128);
+    cudaStream_t s = stream();
+    DISPATCH_R(p,
+               (k_bulk_reaction_endo<float><<<gr, 128, 0, s>>>(c->count, c->start, c->is_reac, c->S, cur<float>(p),
+                                                               from, to, rate, tau, delta_u, r->seed, r->step)),
+               (k_bulk_reaction_endo<double><<<gr, 128, 0, s>>>(c->count, c->start, c->is_reac, c->S,
+                                                                cur<double>(p), from, to, rate, tau, delta_u,
+                                                                r->seed, r->step)));
     RMPCD_CHECK_LAUNCH();
     r->step++;
     return RMPCD_OK;

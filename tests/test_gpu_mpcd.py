@@ -126,6 +126,45 @@ def test_bulk_reaction(rm, oracle):
     assert_same(gp, op, ("species",))
 
 
+@pytest.mark.parametrize("precision", [64, 32])
+@pytest.mark.parametrize("delta_u", [0.5, 3.0])
+def test_bulk_reaction_endothermic(rm, oracle, precision, delta_u):
+    # delta_u = 3.0 is above the relative kinetic energy of many cells (10
+    # particles at kT = 1/3 hold ~1.5), so both sides of the kin > delta_u
+    # test occur
+    L, N = [10, 10, 10], 9000
+    sp = np.random.default_rng(14).choice([1, 2], size=N).astype(np.int32)
+    (oc, op), (gc, gp) = make_pair(rm, oracle, L, N, seed=15, species=sp, precision=precision)
+    reac = (np.arange(oc.S) % 3 != 0).astype(np.uint8)
+    oc.is_reac[:] = reac
+    gc.is_reac = reac
+    if precision == 32:
+        op.vel[:] = gp.download("vel")  # the FP32 form starts from the rounded velocities
+    sp0, v0 = op.species.copy(), op.vel.copy()
+    oracle.bulk_reaction_endothermic(op, oc, 2, 1, 0.3, 1.0, delta_u, 21, 5)
+    st = rm.Rng(21, 5)
+    rm.bulk_reaction_endothermic(gp, gc, 2, 1, 0.3, 1.0, st, delta_u)
+    assert st.step == 6
+    fired = np.nonzero(op.species != sp0)[0]
+    assert fired.size > 0 and np.all(op.species[fired] == 1)
+    assert_same(gp, op, ("species",))
+    if precision == 64:
+        assert_same(gp, op, ("vel",))
+    else:
+        # velocities computed in FP64 from the same FP32 inputs and rounded once
+        assert_same(gp, op, ("vel",), exact=False, rtol=0, atol=4e-7 * np.abs(op.vel).max())
+    # each reacting cell lost exactly delta_u of relative kinetic energy and kept its momentum
+    starts, counts = oc.cell_start - 1, oc.cell_count
+    cells = np.searchsorted(starts, fired, side="right") - 1
+    for c in cells[:20]:
+        a, n = starts[c], counts[c]
+        vb, va = v0[a:a + n], op.vel[a:a + n]
+        kin = lambda v: 0.5 * ((v - v.mean(0)) ** 2).sum()
+        assert kin(vb) > delta_u
+        assert abs(kin(vb) - kin(va) - delta_u) < 1e-9
+        np.testing.assert_allclose(va.sum(0), vb.sum(0), atol=1e-9)
+
+
 @pytest.mark.parametrize("thermostat", [False, True])
 def test_wall_mpcd_step(rm, oracle, thermostat):
     L, N = [6, 6, 6], 2000

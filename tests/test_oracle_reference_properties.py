@@ -143,3 +143,34 @@ def test_srd_conserves_cell_momentum_and_energy(oracle):
         a, n = c.cell_start[s] - 1, c.cell_count[s]
         assert np.allclose(v0[a:a + n].sum(0), p.vel[a:a + n].sum(0), atol=1e-12)
         assert np.isclose((v0[a:a + n] ** 2).sum(), (p.vel[a:a + n] ** 2).sum(), rtol=1e-12)
+
+
+def test_bulk_reaction_endothermic_energy_and_pick(oracle):
+    # src/mpcd.f90:645-700: a reacting cell turns its LAST particle of species
+    # `from` into `to`, keeps its momentum and loses exactly delta_u of
+    # relative kinetic energy; cells with kin <= delta_u never react
+    N, du = 9000, 3.0
+    rng = np.random.default_rng(15)
+    c = oracle.Cells([10, 10, 10])
+    p = oracle.Particles(N)
+    p.pos[:] = rng.random((N, 3)) * 10
+    p.vel[:] = rng.normal(size=(N, 3)) * np.sqrt(1 / 3)
+    p.species[:] = rng.choice([1, 2], size=N)
+    p.sort(c)
+    c.is_reac[:] = 1
+    sp0, v0 = p.species.copy(), p.vel.copy()
+    oracle.bulk_reaction_endothermic(p, c, 2, 1, 0.3, 1.0, du, 21, 5)
+    kin = lambda v: 0.5 * ((v - v.mean(0)) ** 2).sum()
+    n_fired = 0
+    for s in np.nonzero(c.cell_count > 1)[0]:
+        a, n = c.cell_start[s] - 1, c.cell_count[s]
+        changed = np.nonzero(p.species[a:a + n] != sp0[a:a + n])[0]
+        if changed.size == 0:
+            assert np.array_equal(p.vel[a:a + n], v0[a:a + n])
+            continue
+        n_fired += 1
+        assert changed.size == 1 and changed[0] == np.nonzero(sp0[a:a + n] == 2)[0][-1]
+        assert kin(v0[a:a + n]) > du
+        assert abs(kin(v0[a:a + n]) - kin(p.vel[a:a + n]) - du) < 1e-9
+        assert np.allclose(v0[a:a + n].sum(0), p.vel[a:a + n].sum(0), atol=1e-12)
+    assert n_fired > 100
