@@ -42,6 +42,13 @@ SEED = 20241203
 # next key; see the traffic table in DESIGN.md)
 BYTES_PER_PARTICLE = {32: 72, 64: 120}
 BYTES_PER_SLOT = 12
+# Minimum bytes of one whole interval (stream + sort + collide) over the
+# reference's particle state kept as separate arrays (FP32: pos 12, vel 12,
+# image 12, species/flags 4, id 4 = 44 B; FP64: 72 B): key pass reads pos+vel
+# and writes a key, the permutation reads the key and moves the state, the
+# collision reads vel+species and writes vel; 16 B per slot for counts/starts.
+INTERVAL_BYTES_PER_PARTICLE = {32: 148, 64: 252}
+INTERVAL_BYTES_PER_SLOT = 16
 
 
 def peaks():
@@ -425,6 +432,16 @@ def run_ours(args):
                      "parallelism": f"replicas x{world} (independent systems, no collective)",
                      "l2": "inputs larger than L2 (>= 1 GB of particle arrays per copy); no flush"}
     out["roofline"] = r32["roofline"]
+    out["interval_roofline"] = {}
+    for prec, r in ((32, r32), (64, r64)):
+        alg = N * INTERVAL_BYTES_PER_PARTICLE[prec] + r32["cells"].N * INTERVAL_BYTES_PER_SLOT
+        ach = alg * args.steps / (r["ms"] * 1e-3) / 1e9
+        out["interval_roofline"][f"fp{prec}"] = {
+            "bound": "hbm", "achieved": round(ach, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+            "frac": round(ach / peak, 4), "algorithmic_bytes_per_interval": int(alg),
+            "note": "minimum bytes of stream+sort+collide over the SoA particle state "
+                    f"({INTERVAL_BYTES_PER_PARTICLE[prec]} B/particle + {INTERVAL_BYTES_PER_SLOT} B/slot) "
+                    "over the whole device time of an interval"}
     out["autotune"] = tuned
     out["clocks"] = r32["clocks"]
     fp64_value = world * N * args.steps / (r64["ms"] * 1e-3)
@@ -522,14 +539,14 @@ def profile_dimer(args):
 def profile_ncolloids(args):
     """A fixed n_colloids_pbc workload for profilers: 128^3, rho = 10,
     args.profile_ncolloids colloids, FP32 solvent, one thermostatted interval
-    after one warm-up interval, call by call."""
+    of the native loop (rmpcd_ncolloids_run) after one warm-up interval."""
     import rmpcdmd_b200 as rm
     from rmpcdmd_b200.programs import NColloidsPBC
 
     g = NColloidsPBC(L=(128, 128, 128), rho=RHO, N_MD=DIMER_N_MD, N_colloids=args.profile_ncolloids, seed=SEED,
                      volume_correction=False, precision=32)
-    g.interval(True, g.T_init)
-    g.interval(True, g.T_init)
+    g._native(1, True, [g.T_init], 10)
+    g._native(1, True, [g.T_init], 10)
     rm.synchronize()
     print(f"profile_ncolloids: {args.profile_ncolloids} colloids, {g.N} particles, 2 intervals")
 

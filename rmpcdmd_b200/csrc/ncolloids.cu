@@ -9,7 +9,9 @@
 //     over that list instead of over every slot;
 //   * zero_force of the solvent and the PAST_MD/MD roll of compute_force are
 //     one pass that clears only the force entries that can be non-zero
-//     (particles with MD or PAST_MD set: every other entry is exactly zero);
+//     (particles with MD or PAST_MD set: every other entry is exactly zero),
+//     over all N for the first two MD steps after a sort and over the MD
+//     cells after that;
 //   * the two displacement maxima of an MD step are read with one
 //     synchronisation, and there is no per-call host overhead.
 #include <cmath>
@@ -36,32 +38,6 @@ __global__ void k_md_slot_list(const unsigned char *is_md, int S, int *list, int
         if (lane == 0 && bal) b = atomicAdd(n_list, __popc(bal));
         b = __shfl_sync(0xffffffffu, b, 0);
         if (md) list[b + __popc(bal & ((1u << lane) - 1u))] = (int)s;
-    }
-}
-
-// cell_md_pos / cell_md_vel with md_flag = .true. (src/md.f90:79-102,
-// :239-263), one thread per listed cell
-template <typename R>
-__global__ void k_md_cells_pos(const int *list, const int *n_list, const int *count, const int *start, PView<R> v,
-                               R dt, R dt_sq)
-{
-    const int n = *n_list;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const int s = list[k], a = start[s], c = count[s];
-#pragma unroll 4
-        for (int i = a; i < a + c; i++) md_pos_one(v, i, dt, dt_sq);
-    }
-}
-
-template <typename R>
-__global__ void k_md_cells_vel(const int *list, const int *n_list, const int *count, const int *start, PView<R> v,
-                               R dt)
-{
-    const int n = *n_list;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const int s = list[k], a = start[s], c = count[s];
-#pragma unroll 4
-        for (int i = a; i < a + c; i++) md_vel_one(v, i, dt);
     }
 }
 
@@ -98,21 +74,75 @@ __global__ void k_other_cells_vel(const int *count, const int *start, const unsi
     }
 }
 
+// cell_md_pos / cell_md_vel with md_flag = .true. (src/md.f90:79-102,
+// :239-263) over the listed MD cells, eight lanes per cell
+template <typename R>
+__global__ void k_md_cells_pos(const int *list, const int *n_list, const int *count, const int *start, PView<R> v,
+                               R dt, R dt_sq)
+{
+    const long long n = (long long)*n_list * kLanesPerCell;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int s = list[q / kLanesPerCell], g = (int)(q % kLanesPerCell);
+        const int a = start[s], c = count[s];
+        for (int i = a + g; i < a + c; i += kLanesPerCell) md_pos_one(v, i, dt, dt_sq);
+    }
+}
+
+template <typename R>
+__global__ void k_md_cells_vel(const int *list, const int *n_list, const int *count, const int *start, PView<R> v,
+                               R dt)
+{
+    const long long n = (long long)*n_list * kLanesPerCell;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int s = list[q / kLanesPerCell], g = (int)(q % kLanesPerCell);
+        const int a = start[s], c = count[s];
+        for (int i = a + g; i < a + c; i += kLanesPerCell) md_vel_one(v, i, dt);
+    }
+}
+
 // cell_maximum_displacement over the listed cells (src/particle_system.f90:380-410)
 template <typename R>
 __global__ void k_md_cells_max_disp(const int *list, const int *n_list, const int *count, const int *start,
                                     Vec3<R> pos, Vec3<R> old, const int *species, unsigned long long *out)
 {
-    const int n = *n_list;
+    const long long n = (long long)*n_list * kLanesPerCell;
     double m = 0;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const int s = list[k], a = start[s], c = count[s];
-        for (int i = a; i < a + c; i++) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int s = list[q / kLanesPerCell], g = (int)(q % kLanesPerCell);
+        const int a = start[s], c = count[s];
+        for (int i = a + g; i < a + c; i += kLanesPerCell) {
             const double r = disp_sq_one(pos, old, species, i);
             m = m > r ? m : r;
         }
     }
     warp_max_into(out, m);
+}
+
+// the roll + clear below restricted to the listed MD cells.  Between two
+// sorts the list is fixed and compute_force flags only list entries, which
+// lie in MD cells; so once two rolls have run over every particle after a
+// sort (the first turns flags carried through the sort into PAST_MD, the
+// second clears them), no particle outside the MD cells has MD or PAST_MD
+// set or a non-zero force entry, and rolling the MD cells alone gives the
+// same flags and forces as rolling all N.
+template <typename R>
+__global__ void k_md_cells_roll_clear(const int *list, const int *n_list, const int *count, const int *start,
+                                      int *flags, Vec3<R> force)
+{
+    const long long n = (long long)*n_list * kLanesPerCell;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int s = list[q / kLanesPerCell], g = (int)(q % kLanesPerCell);
+        const int a = start[s], c = count[s];
+        for (int i = a + g; i < a + c; i += kLanesPerCell) {
+            const int f = flags[i];
+            if (f & ((1 << MD_BIT) | (1 << PAST_MD_BIT))) {
+                force.x[i] = 0;
+                force.y[i] = 0;
+                force.z[i] = 0;
+                flag_roll_one(flags, i);
+            }
+        }
+    }
 }
 
 // zero_force of the solvent fused with the PAST_MD/MD roll: only entries of
@@ -144,7 +174,11 @@ struct NcLoop {
     int *md_list = nullptr;  // is_md slots
     int *n_md = nullptr;     // their number (device)
     unsigned long long *h_max = nullptr;  // page-locked landing of the two maxima
+    int full_rolls = 2;  // rolls over all N still due since the last sort
 };
+
+// fixed grid of the MD-cell kernels (their item count is on the device)
+static inline int md_cells_grid() { return sm_count() * 16; }
 
 // list the MD cells after a neighbor-list update
 static int list_md_cells(NcLoop &L)
@@ -160,7 +194,7 @@ template <typename R>
 static int md_cells_pos_t(NcLoop &L)
 {
     const R dt = (R)L.dt, dt_sq = (R)(L.dt * L.dt / 2);
-    k_md_cells_pos<R><<<sm_count() * 8, 128, 0, stream()>>>(L.md_list, L.n_md, L.cells->count,
+    k_md_cells_pos<R><<<md_cells_grid(), 256, 0, stream()>>>(L.md_list, L.n_md, L.cells->count,
                                                                        L.cells->start, cur<R>(L.s), dt, dt_sq);
     RMPCD_CHECK_LAUNCH();
     return RMPCD_OK;
@@ -169,7 +203,7 @@ static int md_cells_pos_t(NcLoop &L)
 template <typename R>
 static int md_cells_vel_t(NcLoop &L)
 {
-    k_md_cells_vel<R><<<sm_count() * 8, 128, 0, stream()>>>(L.md_list, L.n_md, L.cells->count,
+    k_md_cells_vel<R><<<md_cells_grid(), 256, 0, stream()>>>(L.md_list, L.n_md, L.cells->count,
                                                                        L.cells->start, cur<R>(L.s), (R)L.dt);
     RMPCD_CHECK_LAUNCH();
     return RMPCD_OK;
@@ -181,7 +215,7 @@ static int md_cells_max_disp_t(NcLoop &L)
     cudaStream_t st = stream();
     RMPCD_CUDA_TRY(cudaMemsetAsync(L.s->d_max, 0, 8, st));
     PView<R> a = cur<R>(L.s), b = alt<R>(L.s);
-    k_md_cells_max_disp<R><<<sm_count() * 4, 256, 0, st>>>(L.md_list, L.n_md, L.cells->count,
+    k_md_cells_max_disp<R><<<md_cells_grid(), 256, 0, st>>>(L.md_list, L.n_md, L.cells->count,
                                                                       L.cells->start, a.pos, b.pos, a.species,
                                                                       L.s->d_max);
     RMPCD_CHECK_LAUNCH();
@@ -192,7 +226,13 @@ template <typename R>
 static int roll_clear_t(NcLoop &L)
 {
     PView<R> v = cur<R>(L.s);
-    if (L.s->N > 0) k_roll_clear<R><<<grid_for(L.s->N, 256), 256, 0, stream()>>>(v.flags, v.force, L.s->N);
+    if (L.full_rolls > 0) {
+        if (L.s->N > 0) k_roll_clear<R><<<grid_for(L.s->N, 256), 256, 0, stream()>>>(v.flags, v.force, L.s->N);
+        L.full_rolls--;
+    } else {
+        k_md_cells_roll_clear<R><<<md_cells_grid(), 256, 0, stream()>>>(L.md_list, L.n_md, L.cells->count,
+                                                                        L.cells->start, v.flags, v.force);
+    }
     RMPCD_CHECK_LAUNCH();
     return RMPCD_OK;
 }
@@ -242,6 +282,7 @@ static int catch_up_and_sort(NcLoop &L)
     if (!rc) rc = rmpcd_apply_pbc(L.c, L.cells->edges);
     if (!rc) rc = rmpcd_particles_sort(L.s, L.cells);
     L.st->last_sort = L.st->t;
+    L.full_rolls = 2;
     if (!rc) rc = rmpcd_nlist_update(L.nl, L.c, L.s, L.prm->list_radius, L.cells, nullptr);
     if (!rc) rc = list_md_cells(L);
     if (!rc) rc = rmpcd_particles_copy_pos_old(L.s);

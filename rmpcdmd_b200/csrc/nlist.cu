@@ -92,14 +92,91 @@ __global__ void k_colloid_sum(const int *n, int Nmax, const unsigned char *contr
     colloid_sum_block(blockIdx.x, n, Nmax, contrib, pf, cfx, cfy, cfz, clist, cn);
 }
 
-// e = sum of pair energies in (colloid, entry) order
-__global__ void k_energy(const int *cn, const int *clist, int C, int Nmax, const double *pe, double *out)
+// Sequential sum e = (((0 + t_0) + t_1) + ...) of `total` terms, one block:
+// thread 0 adds a chunk held in shared memory while warps 1.. load the next
+// chunk, so the add chain never waits on a global load.
+constexpr int kSumChunk = 2048;
+
+template <typename Get>
+__device__ void ordered_sum_block(Get get, long long total, double *out)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    __shared__ double buf[2][kSumChunk];
+    const int t = threadIdx.x, nt = blockDim.x;
+    const long long nch = (total + kSumChunk - 1) / kSumChunk;
+    auto load = [&](long long c, double *dst, int t0, int nthr) {
+        const long long b = c * kSumChunk;
+        const int m = (int)(total - b < kSumChunk ? total - b : kSumChunk);
+        for (int j = t0; j < m; j += nthr) dst[j] = get(b + j);
+    };
     double e = 0;
-    for (int i = 0; i < C; i++)
-        for (int k = 0; k < cn[i]; k++) e = e + pe[(size_t)i * Nmax + clist[(size_t)i * Nmax + k]];
-    *out = e;
+    if (nch > 0) load(0, buf[0], t, nt);
+    __syncthreads();
+    for (long long c = 0; c < nch; c++) {
+        if (t == 0) {
+            const long long b = c * kSumChunk;
+            const int m = (int)(total - b < kSumChunk ? total - b : kSumChunk);
+            const double *x = buf[c & 1];
+#pragma unroll 8
+            for (int j = 0; j < m; j++) e = e + x[j];
+        } else if (t >= 32 && c + 1 < nch) {
+            load(c + 1, buf[(c + 1) & 1], t - 32, nt - 32);
+        }
+        __syncthreads();
+    }
+    if (t == 0) *out = e;
+}
+
+// e = sum of pair energies in (colloid, entry) order: the contributing
+// entries of colloid i are clist[i*Nmax + 0 .. cn[i]-1]; an exclusive scan of
+// cn (into pre, C + 1 ints) turns a position in that order into (i, k).
+__global__ void __launch_bounds__(1024) k_energy(const int *cn, const int *clist, int C, int Nmax, const double *pe,
+                                                 int *pre, double *out)
+{
+    __shared__ int wsum[32];
+    __shared__ int carry;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    if (t == 0) carry = 0;
+    __syncthreads();
+    for (int b = 0; b < C; b += blockDim.x) {
+        const int i = b + t;
+        const int v = i < C ? cn[i] : 0;
+        int x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            int z = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, z, o);
+                if (lane >= o) z += y;
+            }
+            wsum[lane] = z;
+        }
+        __syncthreads();
+        const int incl = x + (w > 0 ? wsum[w - 1] : 0) + carry;
+        if (i < C) pre[i] = incl - v;
+        __syncthreads();
+        if (t == (int)blockDim.x - 1) carry = incl;
+        __syncthreads();
+    }
+    if (t == 0) pre[C] = carry;
+    __syncthreads();
+    const long long total = pre[C];
+    ordered_sum_block(
+        [&](long long f) {
+            int lo = 0, hi = C;  // largest i with pre[i] <= f
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (pre[mid] <= f) lo = mid;
+                else hi = mid;
+            }
+            const size_t q = (size_t)lo * Nmax;
+            return pe[q + clist[q + (f - pre[lo])]];
+        },
+        total, out);
 }
 
 __global__ void k_reset_contrib(const int *list, const int *n, int Nmax, const unsigned char *contrib,
@@ -128,6 +205,35 @@ __global__ void __launch_bounds__(kNlBlockThreads)
     force_n2_block(blockIdx.x, px, py, pz, sp, C, L0, L1, L2, lj, fx, fy, fz);
 }
 
+// the pair energies of compute_force_n2 in the reference's (i, j > i) order,
+// 0 for pairs beyond the cut (adding +0.0 leaves the sum unchanged: a
+// round-to-nearest sum starting at +0.0 is never -0.0), block i writes row i
+__global__ void k_energy_n2_terms(const double *px, const double *py, const double *pz, const int *sp, int C,
+                                  double L0, double L1, double L2, LJDev lj, double *terms)
+{
+    const int i = blockIdx.x;
+    const long long row = (long long)i * C - (long long)i * (i + 1) / 2;
+    for (int j = i + 1 + threadIdx.x; j < C; j += blockDim.x) {
+        double d0 = min_image_d(px[i] - px[j], L0);
+        double d1 = min_image_d(py[i] - py[j], L1);
+        double d2 = min_image_d(pz[i] - pz[j], L2);
+        double r_sq = d0 * d0 + d1 * d1 + d2 * d2;
+        int s1 = sp[i], s2 = sp[j];
+        double e = 0;
+        if (r_sq <= lj.cut_sq[(s1 - 1) + lj.n1 * (s2 - 1)]) {
+            int tt = (s2 - 1) + lj.n1 * (s1 - 1);
+            e = lj_energy(r_sq, lj.epsilon[tt], lj.sigma[tt], lj.cut_energy[tt]);
+        }
+        terms[row + (j - i - 1)] = e;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_energy_sum(const double *terms, long long total, double *out)
+{
+    ordered_sum_block([&](long long f) { return terms[f]; }, total, out);
+}
+
+// a single thread for a few colloids
 __global__ void k_energy_n2(const double *px, const double *py, const double *pz, const int *sp, int C,
                             double L0, double L1, double L2, LJDev lj, double *out)
 {
@@ -157,6 +263,7 @@ static int ensure_force_scratch(rmpcd_nlist *nl, int N2)
         RMPCD_CUDA_TRY(cudaMalloc(&nl->contrib, ne + 8));
         RMPCD_CUDA_TRY(cudaMalloc(&nl->d_status, (2 * nl->Npoints + 16 + ne) * sizeof(int)));
         RMPCD_CUDA_TRY(cudaMalloc(&nl->mkeys, kMultiSortMax * sizeof(unsigned long long)));
+        RMPCD_CUDA_TRY(cudaMalloc(&nl->e_pre, ((size_t)nl->Npoints + 1) * sizeof(int)));
         RMPCD_CUDA_TRY(cudaMemsetAsync(nl->d_status, 0, 16 * sizeof(int), stream()));
     }
     if (nl->ncontrib_cap < N2) {
@@ -208,6 +315,7 @@ int rmpcd_nlist_destroy(rmpcd_nlist *nl)
     cudaFree(nl->ncontrib);
     cudaFree(nl->d_status);
     cudaFree(nl->mkeys);
+    cudaFree(nl->e_pre);
     delete nl;
     return RMPCD_OK;
 }
@@ -373,7 +481,7 @@ int compute_force_impl(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist *
         k_colloid_sum<<<C, kNlThreads, 0, s>>>(nl->n, nl->Nmax, nl->contrib, nl->pair_f, cv.force.x, cv.force.y,
                                                cv.force.z, clist, cn);
         k_reset_contrib<<<grid, 256, 0, s>>>(nl->list, nl->n, nl->Nmax, nl->contrib, nl->ncontrib);
-        if (energy) k_energy<<<1, 32, 0, s>>>(cn, clist, C, nl->Nmax, nl->pair_e, e_out);
+        if (energy) k_energy<<<1, 1024, 0, s>>>(cn, clist, C, nl->Nmax, nl->pair_e, nl->e_pre, e_out);
         RMPCD_CHECK_LAUNCH();
     }
     if (energy) {
@@ -403,8 +511,22 @@ int rmpcd_compute_force_n2(rmpcd_particles *ps, const double L[3], const rmpcd_l
     if (C > 0) {
         PView<double> v = cur<double>(ps);
         LJDev ld = lj_dev(lj);
-        if (energy)
+        if (energy && C <= 32) {
             k_energy_n2<<<1, 32, 0, s>>>(v.pos.x, v.pos.y, v.pos.z, v.species, C, L[0], L[1], L[2], ld, e_out);
+        } else if (energy) {
+            const long long np = (long long)C * (C - 1) / 2;
+            if (ps->n2_cap < np) {
+                cudaStreamSynchronize(s);
+                cudaFree(ps->n2_terms);
+                ps->n2_terms = nullptr;
+                ps->n2_cap = 0;
+                RMPCD_CUDA_TRY(cudaMalloc(&ps->n2_terms, (size_t)np * sizeof(double)));
+                ps->n2_cap = np;
+            }
+            k_energy_n2_terms<<<C, 128, 0, s>>>(v.pos.x, v.pos.y, v.pos.z, v.species, C, L[0], L[1], L[2], ld,
+                                                ps->n2_terms);
+            k_energy_sum<<<1, 1024, 0, s>>>(ps->n2_terms, np, e_out);
+        }
         if (C <= 32)
             k_force_n2<<<1, 32, 0, s>>>(v.pos.x, v.pos.y, v.pos.z, v.species, C, L[0], L[1], L[2], ld, v.force.x,
                                         v.force.y, v.force.z);

@@ -236,6 +236,7 @@ static void free_particles(rmpcd_particles *p)
     cudaFree(p->stage);
     cudaFree(p->rec[0]);
     cudaFree(p->rec[1]);
+    cudaFree(p->n2_terms);
     delete p;
 }
 

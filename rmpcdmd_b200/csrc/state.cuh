@@ -73,6 +73,8 @@ struct rmpcd_particles {
     // permuting them (a permutation of zeros is zeros)
     bool force_zero = true;
     bool force_old_zero = true;
+    double *n2_terms = nullptr;  // pair energies of compute_force_n2, C (C - 1) / 2
+    long long n2_cap = 0;
 };
 
 struct rmpcd_nlist {
@@ -92,6 +94,7 @@ struct rmpcd_nlist {
     int ncontrib_cap = 0;
     int *d_status = nullptr;
     unsigned long long *mkeys = nullptr;  // multi-contribution keys (kMultiSortMax)
+    int *e_pre = nullptr;       // Npoints + 1, offsets of the energy terms per point
 };
 
 namespace rmpcd {

@@ -115,19 +115,22 @@ def test_neighbor_list_many_colloids_small_box(rm, oracle):
         assert_same(gcol, ocol, ("force",))
 
 
-def test_compute_force_n2(rm, oracle):
-    C = 200
+@pytest.mark.parametrize("C,box", [(200, 20.0), (300, 70.0), (20, 30.0)])
+def test_compute_force_n2(rm, oracle, C, box):
+    # box 20: every pair inside the cut; box 70: most pairs beyond it; C = 20:
+    # the single-thread path
     r = np.random.default_rng(5)
     ocol = oracle.Particles(C, 1, [100.0])
     gcol = rm.ParticleSystem(C, 1, [100.0])
     ocol.species[:] = 1
-    ocol.pos[:] = r.random((C, 3)) * 20
+    ocol.pos[:] = r.random((C, 3)) * box
     ocol.force[:] = r.normal(size=(C, 3))
     upload(gcol, ocol, ("pos", "species", "force"))
     lj_o = oracle.LJParams([[1.0]], [[6.0]], [[18.0]])
     lj_g = rm.LJParams([[1.0]], [[6.0]], [[18.0]])
-    e_o = oracle.compute_force_n2(ocol, [20.0] * 3, lj_o)
-    e_g = rm.compute_force_n2(gcol, [20.0] * 3, lj_g)
+    e_o = oracle.compute_force_n2(ocol, [box] * 3, lj_o)
+    e_g = rm.compute_force_n2(gcol, [box] * 3, lj_g)
+    assert e_o != 0
     assert e_g == e_o
     assert_same(gcol, ocol, ("force",))
 

@@ -95,6 +95,7 @@ def test_n_colloids_pbc_bit_exact(rm, oracle):
     assert g.n_extra_sorting == o.n_extra_sorting
     assert g.rng.step == o.step
     assert np.array_equal(g.cells.origin, o.cells.origin)
+    assert g.e1 == o.e1 and g.e2 == o.e2
 
 
 @pytest.mark.parametrize("precision", [64, 32])
@@ -121,13 +122,16 @@ def test_bulk_shapes_give_identical_results(rm, oracle, precision):
         rm.set_bulk_shape(precision, keep)
 
 
-def test_n_colloids_native_loop_matches_call_by_call(rm):
+@pytest.mark.parametrize("precision", [64, 32])
+def test_n_colloids_native_loop_matches_call_by_call(rm, precision):
     """rmpcd_ncolloids_run issues the program's calls in C; the state after
     thermalisation (with the 10th-interval rescaling) and a temperature ramp
-    equals the Python loop making the same calls one by one."""
+    equals the Python loop making the same calls one by one (flags and both
+    force buffers included: the native loop rolls flags over the MD cells
+    only, from the third MD step after a sort on)."""
     from rmpcdmd_b200.programs import NColloidsPBC
 
-    kw = dict(L=(24, 24, 24), rho=10, N_MD=10, N_colloids=8, seed=77, T_final=0.5)
+    kw = dict(L=(24, 24, 24), rho=10, N_MD=10, N_colloids=8, seed=77, T_final=0.5, precision=precision)
     a = NColloidsPBC(**kw)
     b = NColloidsPBC(**kw)
     a.thermalise(10, native=False)
@@ -139,4 +143,5 @@ def test_n_colloids_native_loop_matches_call_by_call(rm):
     for f in ("pos", "vel", "force", "image"):
         assert np.array_equal(a.colloids.download(f), b.colloids.download(f)), f
     assert (a.t, a.last_sort, a.n_extra_sorting, a.rng.step) == (b.t, b.last_sort, b.n_extra_sorting, b.rng.step)
+    assert b.n_extra_sorting > 0  # sorts inside MD steps occurred
     assert a.e1 == b.e1 and a.e2 == b.e2
