@@ -354,6 +354,10 @@ int rmpcd_ncolloids_run(rmpcd_particles *solvent, rmpcd_particles *colloids, rmp
                         rmpcd_rng *rng, const rmpcd_ncolloids_params *params, int n_intervals, int thermostat,
                         const double *T, int first_interval, int rescale_every, double T_rescale,
                         rmpcd_ncolloids_state *state);
+/* Whether rmpcd_ncolloids_run replays its MD steps as CUDA graphs (default
+ * on; the results are the same either way).  No counterpart in the
+ * reference. */
+int rmpcd_ncolloids_set_graphs(int on);
 
 /* Batched single_dimer_pbc: the main loop of programs/single_dimer_pbc.f90
  * (:303-443: N_MD MD steps with the program's re-sort test, then

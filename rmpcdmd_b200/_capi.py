@@ -173,6 +173,7 @@ PROTOTYPES = {
     "rmpcd_bulk_set_shape": [C.c_int, C.c_int],
     "rmpcd_bulk_get_shape": [C.c_int, c_int_p],
     "rmpcd_bulk_autotune": [c_int_p, C.c_int, C.c_double, C.c_int, c_int_p, C.POINTER(C.c_float)],
+    "rmpcd_ncolloids_set_graphs": [C.c_int],
     "rmpcd_ncolloids_run": [PART_P, PART_P, CELLS_P, NL_P, LJ_P, LJ_P, RNG_P, C.POINTER(NCOLLOIDS_PARAMS),
                             C.c_int, C.c_int, c_double_p, C.c_int, C.c_int, C.c_double,
                             C.POINTER(NCOLLOIDS_STATE)],

@@ -139,6 +139,8 @@ static void drain(TimerSlot &t)
     t.pending.clear();
 }
 
+bool timers_on() { return g_timers_on; }
+
 PhaseTimer::PhaseTimer(const char *name)
 {
     if (!g_timers_on) return;

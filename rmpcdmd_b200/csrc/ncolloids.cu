@@ -13,9 +13,15 @@
 //     over all N for the first two MD steps after a sort and over the MD
 //     cells after that;
 //   * the two displacement maxima of an MD step are read with one
-//     synchronisation, and there is no per-call host overhead.
+//     synchronisation, and there is no per-call host overhead;
+//   * an MD step without energies is two replayed CUDA graphs: the part up
+//     to the displacement maxima, and the part after the re-sort decision
+//     (flag roll, forces, velocity updates), each captured once per set of
+//     buffers it touches (the sort and the force switch exchange buffers).
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <tuple>
 #include <vector>
 
 #include "rmpcd_common.cuh"
@@ -41,28 +47,60 @@ __global__ void k_md_slot_list(const unsigned char *is_md, int S, int *list, int
     }
 }
 
-// the catch-up of cell_md_pos / cell_md_vel with md_flag = .false. over every
-// non-MD cell, eight lanes per cell so that a cell's particles are read
-// together
 constexpr int kLanesPerCell = 8;
 
+// In this program a solvent particle with neither MD nor PAST_MD set has zero
+// force and force_old: compute_force writes a force only together with the
+// MD bit, the roll moves MD to PAST_MD as the force moves to force_old, and
+// entries are cleared when both bits go.  So the force arrays are read only
+// for flagged particles and a zero takes their place otherwise; the
+// arithmetic is that of md_pos / md_vel with the zero entry, bit for bit.
+constexpr int kForceFlags = (1 << MD_BIT) | (1 << PAST_MD_BIT);
+
+// md_pos of one particle (src/md.f90:61-77 form)
 template <typename R>
-__global__ void k_other_cells_pos(const int *count, const int *start, const unsigned char *is_md, int S, PView<R> v,
-                                  R dt, R dt_sq)
+__device__ inline void stream_pos_gated(const PView<R> &v, long long i, int f, R dt, R dt_sq)
 {
-    const long long nthreads = (long long)gridDim.x * blockDim.x;
-    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < (long long)S * kLanesPerCell;
-         q += nthreads) {
-        const int s = (int)(q / kLanesPerCell), g = (int)(q % kLanesPerCell);
-        if (is_md[s]) continue;
-        const int a = start[s], c = count[s];
-        for (int i = a + g; i < a + c; i += kLanesPerCell) md_pos_one(v, i, dt, dt_sq);
+    R fx = 0, fy = 0, fz = 0;
+    if (f & kForceFlags) {
+        fx = v.force.x[i];
+        fy = v.force.y[i];
+        fz = v.force.z[i];
+    }
+    v.pos.x[i] = v.pos.x[i] + dt * v.vel.x[i] + dt_sq * fx;
+    v.pos.y[i] = v.pos.y[i] + dt * v.vel.y[i] + dt_sq * fy;
+    v.pos.z[i] = v.pos.z[i] + dt * v.vel.z[i] + dt_sq * fz;
+}
+
+// md_vel of one particle (src/md.f90:219-237 form)
+template <typename R>
+__device__ inline void stream_vel_gated(const PView<R> &v, long long i, int f, R dt)
+{
+    if (!((f >> WALL_BIT) & 1)) {
+        R fx = 0, fy = 0, fz = 0, ox = 0, oy = 0, oz = 0;
+        if (f & kForceFlags) {
+            fx = v.force.x[i];
+            fy = v.force.y[i];
+            fz = v.force.z[i];
+            ox = v.force_old.x[i];
+            oy = v.force_old.y[i];
+            oz = v.force_old.z[i];
+        }
+        v.vel.x[i] = v.vel.x[i] + dt * (fx + ox) / 2;
+        v.vel.y[i] = v.vel.y[i] + dt * (fy + oy) / 2;
+        v.vel.z[i] = v.vel.z[i] + dt * (fz + oz) / 2;
+    } else {
+        v.flags[i] = f & ~(1 << WALL_BIT);
     }
 }
 
+// the catch-up of cell_md_pos then cell_md_vel with md_flag = .false.
+// (src/md.f90:79-102, :239-263) over every non-MD cell in one pass (both are
+// per particle, the position step reading the velocity before its update),
+// eight lanes per cell so that a cell's particles are read together
 template <typename R>
-__global__ void k_other_cells_vel(const int *count, const int *start, const unsigned char *is_md, int S, PView<R> v,
-                                  R dt)
+__global__ void k_other_cells_stream(const int *count, const int *start, const unsigned char *is_md, int S,
+                                     PView<R> v, R dt, R dt_sq)
 {
     const long long nthreads = (long long)gridDim.x * blockDim.x;
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < (long long)S * kLanesPerCell;
@@ -70,7 +108,11 @@ __global__ void k_other_cells_vel(const int *count, const int *start, const unsi
         const int s = (int)(q / kLanesPerCell), g = (int)(q % kLanesPerCell);
         if (is_md[s]) continue;
         const int a = start[s], c = count[s];
-        for (int i = a + g; i < a + c; i += kLanesPerCell) md_vel_one(v, i, dt);
+        for (int i = a + g; i < a + c; i += kLanesPerCell) {
+            const int f = v.flags[i];
+            stream_pos_gated(v, i, f, dt, dt_sq);
+            stream_vel_gated(v, i, f, dt);
+        }
     }
 }
 
@@ -84,7 +126,7 @@ __global__ void k_md_cells_pos(const int *list, const int *n_list, const int *co
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
         const int s = list[q / kLanesPerCell], g = (int)(q % kLanesPerCell);
         const int a = start[s], c = count[s];
-        for (int i = a + g; i < a + c; i += kLanesPerCell) md_pos_one(v, i, dt, dt_sq);
+        for (int i = a + g; i < a + c; i += kLanesPerCell) stream_pos_gated(v, i, v.flags[i], dt, dt_sq);
     }
 }
 
@@ -96,7 +138,26 @@ __global__ void k_md_cells_vel(const int *list, const int *n_list, const int *co
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
         const int s = list[q / kLanesPerCell], g = (int)(q % kLanesPerCell);
         const int a = start[s], c = count[s];
-        for (int i = a + g; i < a + c; i += kLanesPerCell) md_vel_one(v, i, dt);
+        for (int i = a + g; i < a + c; i += kLanesPerCell) stream_vel_gated(v, i, v.flags[i], dt);
+    }
+}
+
+// pos_old = pos over the listed cells: inside the loop only the MD cells'
+// pos_old is read (cell_maximum_displacement) before the next sort rewrites
+// the buffer
+template <typename R>
+__global__ void k_md_cells_copy_pos(const int *list, const int *n_list, const int *count, const int *start,
+                                    Vec3<R> pos, Vec3<R> old)
+{
+    const long long n = (long long)*n_list * kLanesPerCell;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int s = list[q / kLanesPerCell], g = (int)(q % kLanesPerCell);
+        const int a = start[s], c = count[s];
+        for (int i = a + g; i < a + c; i += kLanesPerCell) {
+            old.x[i] = pos.x[i];
+            old.y[i] = pos.y[i];
+            old.z[i] = pos.z[i];
+        }
     }
 }
 
@@ -175,7 +236,45 @@ struct NcLoop {
     int *n_md = nullptr;     // their number (device)
     unsigned long long *h_max = nullptr;  // page-locked landing of the two maxima
     int full_rolls = 2;  // rolls over all N still due since the last sort
+    // replayed parts of an MD step, keyed by the buffers they use
+    using Key = std::tuple<const void *, const void *, const void *, int>;
+    std::map<Key, cudaGraphExec_t> part_a, part_b;
+    bool graphs = false;
+
+    ~NcLoop()
+    {
+        for (auto &kv : part_a) cudaGraphExecDestroy(kv.second);
+        for (auto &kv : part_b) cudaGraphExecDestroy(kv.second);
+    }
 };
+
+// run issue() once under stream capture the first time `key` is seen, then
+// replay the instantiated graph
+template <typename F>
+static int replay(std::map<NcLoop::Key, cudaGraphExec_t> &cache, const NcLoop::Key &key, F issue)
+{
+    cudaStream_t st = stream();
+    auto it = cache.find(key);
+    if (it == cache.end()) {
+        RMPCD_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const int rc = issue();
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (e != cudaSuccess) return fail(RMPCD_ERR_CUDA, "n_colloids step capture: %s", cudaGetErrorString(e));
+        cudaGraphExec_t x = nullptr;
+        const cudaError_t ei = cudaGraphInstantiate(&x, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess)
+            return fail(RMPCD_ERR_CUDA, "n_colloids step instantiate: %s", cudaGetErrorString(ei));
+        it = cache.emplace(key, x).first;
+    }
+    RMPCD_CUDA_TRY(cudaGraphLaunch(it->second, st));
+    return RMPCD_OK;
+}
 
 // fixed grid of the MD-cell kernels (their item count is on the device)
 static inline int md_cells_grid() { return sm_count() * 16; }
@@ -243,8 +342,18 @@ static int other_cells_t(NcLoop &L, double dtl)
     const double dt_sq = dtl * dtl / 2;
     const int g = grid_full((long long)L.cells->S * kLanesPerCell, 256);
     rmpcd_cells *c = L.cells;
-    k_other_cells_pos<R><<<g, 256, 0, stream()>>>(c->count, c->start, c->is_md, c->S, cur<R>(L.s), (R)dtl, (R)dt_sq);
-    k_other_cells_vel<R><<<g, 256, 0, stream()>>>(c->count, c->start, c->is_md, c->S, cur<R>(L.s), (R)dtl);
+    k_other_cells_stream<R><<<g, 256, 0, stream()>>>(c->count, c->start, c->is_md, c->S, cur<R>(L.s), (R)dtl,
+                                                     (R)dt_sq);
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+template <typename R>
+static int md_cells_copy_pos_t(NcLoop &L)
+{
+    PView<R> a = cur<R>(L.s), b = alt<R>(L.s);
+    k_md_cells_copy_pos<R><<<md_cells_grid(), 256, 0, stream()>>>(L.md_list, L.n_md, L.cells->count,
+                                                                  L.cells->start, a.pos, b.pos);
     RMPCD_CHECK_LAUNCH();
     return RMPCD_OK;
 }
@@ -253,7 +362,7 @@ static int other_cells_t(NcLoop &L, double dtl)
 
 // the displacement maxima of the MD step: solvent over is_md cells (floored
 // at max_v * delta_t) and colloids, read with one synchronisation
-static int displacements(NcLoop &L, double delta_t, double *so_max, double *co_max)
+static int launch_displacements(NcLoop &L)
 {
     int rc = NC_DISPATCH(L, md_cells_max_disp_t);
     if (!rc) rc = launch_max_disp(L.c);
@@ -261,8 +370,14 @@ static int displacements(NcLoop &L, double delta_t, double *so_max, double *co_m
     unsigned long long *bits = L.h_max;
     RMPCD_CUDA_TRY(cudaMemcpyAsync(bits, L.s->d_max, 8, cudaMemcpyDeviceToHost, stream()));
     RMPCD_CUDA_TRY(cudaMemcpyAsync(bits + 1, L.c->d_max, 8, cudaMemcpyDeviceToHost, stream()));
-    rc = sync();
+    return RMPCD_OK;
+}
+
+static int read_displacements(NcLoop &L, double delta_t, double *so_max, double *co_max)
+{
+    int rc = sync();
     if (rc) return rc;
+    unsigned long long *bits = L.h_max;
     double m0, m1;
     memcpy(&m0, bits, 8);
     memcpy(&m1, bits + 1, 8);
@@ -273,20 +388,43 @@ static int displacements(NcLoop &L, double delta_t, double *so_max, double *co_m
 }
 
 // stream the non-MD cells over the time since the last sort, wrap, sort,
-// rebuild the list (programs/n_colloids_pbc.f90:230-241)
-static int catch_up_and_sort(NcLoop &L)
+// rebuild the list (programs/n_colloids_pbc.f90:230-241).  The solvent's
+// pos_old is copied for the MD cells only, except on the call's last sort
+// (after which the caller may read any of it).
+static int catch_up_and_sort(NcLoop &L, bool full_pos_old)
 {
     const double dtl = (L.st->t - L.st->last_sort) * L.dt;
     int rc = L.s->precision == RMPCD_FP32 ? other_cells_t<float>(L, dtl) : other_cells_t<double>(L, dtl);
-    if (!rc) rc = rmpcd_apply_pbc(L.s, L.cells->edges);
     if (!rc) rc = rmpcd_apply_pbc(L.c, L.cells->edges);
-    if (!rc) rc = rmpcd_particles_sort(L.s, L.cells);
+    if (!rc) rc = sort_particles_flagged(L.cells, L.s, L.cells->edges);  // apply_pbc of the solvent + sort
     L.st->last_sort = L.st->t;
     L.full_rolls = 2;
     if (!rc) rc = rmpcd_nlist_update(L.nl, L.c, L.s, L.prm->list_radius, L.cells, nullptr);
     if (!rc) rc = list_md_cells(L);
-    if (!rc) rc = rmpcd_particles_copy_pos_old(L.s);
+    if (!rc) rc = full_pos_old ? rmpcd_particles_copy_pos_old(L.s) : NC_DISPATCH(L, md_cells_copy_pos_t);
     if (!rc) rc = rmpcd_particles_copy_pos_old(L.c);
+    return rc;
+}
+
+// md_loop up to the displacement maxima (programs/n_colloids_pbc.f90:221-229)
+static int issue_part_a(NcLoop &L)
+{
+    int rc = NC_DISPATCH(L, md_cells_pos_t);
+    if (!rc) rc = rmpcd_colloid_vv_pos(L.c, L.dt, L.vv_mass.data());
+    if (!rc) rc = launch_displacements(L);
+    return rc;
+}
+
+// md_loop after the re-sort test (programs/n_colloids_pbc.f90:243-254), the
+// force switch done; energies only when asked for (they synchronise)
+static int issue_part_b(NcLoop &L, double *e1, double *e2)
+{
+    int rc = NC_DISPATCH(L, roll_clear_t);
+    if (!rc) rc = rmpcd_particles_zero_force(L.c);
+    if (!rc) rc = compute_force_impl(L.c, L.s, L.nl, L.cells->edges, L.lj_sc, e1, false);
+    if (!rc) rc = rmpcd_compute_force_n2(L.c, L.cells->edges, L.lj_cc, e2);
+    if (!rc) rc = NC_DISPATCH(L, md_cells_vel_t);
+    if (!rc) rc = rmpcd_colloid_vv_vel(L.c, L.dt, L.vv_mass.data());
     return rc;
 }
 
@@ -295,35 +433,56 @@ static int md_step(NcLoop &L, bool want_energy)
 {
     const double dt = L.dt;
     L.st->t += 1;
-    int rc = NC_DISPATCH(L, md_cells_pos_t);
-    if (!rc) rc = rmpcd_colloid_vv_pos(L.c, dt, L.vv_mass.data());
+    int rc;
+    if (L.graphs) {
+        const NcLoop::Key ka{L.s->pos[L.s->cur][0], L.s->force[L.s->cur][0], L.c->force[L.c->cur][0], 0};
+        rc = replay(L.part_a, ka, [&] { return issue_part_a(L); });
+    } else {
+        rc = issue_part_a(L);
+    }
     double so_max = 0, co_max = 0;
-    if (!rc) rc = displacements(L, dt * (L.st->t - L.st->last_sort), &so_max, &co_max);
+    if (!rc) rc = read_displacements(L, dt * (L.st->t - L.st->last_sort), &so_max, &co_max);
     if (rc) return rc;
     if ((co_max >= L.prm->skin * 0.1) || (so_max >= L.prm->skin * 0.9)) {
-        rc = catch_up_and_sort(L);
+        rc = catch_up_and_sort(L, false);
         if (rc) return rc;
         L.st->n_extra_sorting += 1;
     }
     rc = rmpcd_particles_switch_force(L.s);
     if (!rc) rc = rmpcd_particles_switch_force(L.c);
-    if (!rc) rc = NC_DISPATCH(L, roll_clear_t);
-    if (!rc) rc = rmpcd_particles_zero_force(L.c);
+    if (rc) return rc;
+    if (L.graphs && !want_energy) {
+        // the roll over all N or over the MD cells is part of the key; the
+        // host-side bookkeeping of the captured calls is redone after a replay
+        const int full = L.full_rolls > 0;
+        const NcLoop::Key kb{L.s->pos[L.s->cur][0], L.s->force[L.s->cur][0], L.c->force[L.c->cur][0], full};
+        const int before = L.full_rolls;
+        rc = replay(L.part_b, kb, [&] { return issue_part_b(L, nullptr, nullptr); });
+        L.full_rolls = before > 0 ? before - 1 : 0;
+        L.s->force_zero = false;
+        L.c->force_zero = false;
+        return rc;
+    }
     double e1 = 0, e2 = 0;
-    if (!rc) rc = compute_force_impl(L.c, L.s, L.nl, L.cells->edges, L.lj_sc, want_energy ? &e1 : nullptr, false);
-    if (!rc) rc = rmpcd_compute_force_n2(L.c, L.cells->edges, L.lj_cc, want_energy ? &e2 : nullptr);
+    rc = issue_part_b(L, want_energy ? &e1 : nullptr, want_energy ? &e2 : nullptr);
     if (!rc && want_energy) {
         L.st->e1 = e1;
         L.st->e2 = e2;
     }
-    if (!rc) rc = NC_DISPATCH(L, md_cells_vel_t);
-    if (!rc) rc = rmpcd_colloid_vv_vel(L.c, dt, L.vv_mass.data());
     return rc;
 }
 
 }  // namespace rmpcd
 
 using namespace rmpcd;
+
+static bool g_nc_graphs = true;
+
+extern "C" int rmpcd_ncolloids_set_graphs(int on)
+{
+    g_nc_graphs = on != 0;
+    return RMPCD_OK;
+}
 
 extern "C" int rmpcd_ncolloids_run(rmpcd_particles *solvent, rmpcd_particles *colloids, rmpcd_cells *cells,
                                    rmpcd_nlist *nl, const rmpcd_lj *solvent_colloid, const rmpcd_lj *colloid_colloid,
@@ -360,9 +519,14 @@ extern "C" int rmpcd_ncolloids_run(rmpcd_particles *solvent, rmpcd_particles *co
     for (int k = 0; !rc0 && k < n_intervals; k++) {
         const int i = first_interval + k;
         int rc = 0;
-        for (int j = 0; !rc && j < params->N_MD; j++) rc = md_step(L, j == params->N_MD - 1);
+        for (int j = 0; !rc && j < params->N_MD; j++) {
+            rc = md_step(L, j == params->N_MD - 1);
+            // the first MD step runs uncaptured (it allocates the force
+            // scratch on a first use); graphs stay off while phase timers run
+            L.graphs = g_nc_graphs && !timers_on();
+        }
         if (!rc) rc = rmpcd_cells_random_shift(cells, rng);
-        if (!rc) rc = catch_up_and_sort(L);
+        if (!rc) rc = catch_up_and_sort(L, k == n_intervals - 1);
         if (!rc)
             rc = rmpcd_simple_mpcd_step(solvent, cells, rng, 0, 0.0, thermostat, T ? T[k] : 0.0, params->do_hydro);
         if (!rc && rescale_every > 0 && i % rescale_every == 0) rc = rmpcd_rescale_cells(solvent, cells, T_rescale);

@@ -30,6 +30,46 @@ __global__ void k_key_count(Grid g, const R *__restrict__ x, const R *__restrict
     }
 }
 
+// the same with apply_pbc (src/md.f90:202-217) done on each particle first:
+// the wrapped position is the one keyed, and pos / image are written only
+// for particles that wrap
+template <typename R>
+__global__ void k_pbc_key_count(Grid g, PView<R> v, double e0, double e1, double e2, int N,
+                                int *__restrict__ key, int *__restrict__ count)
+{
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < N; base += stride) {
+        long long i = base + threadIdx.x;
+        bool ok = i < N;
+        int s = -1;
+        if (ok) {
+            R x = v.pos.x[i], y = v.pos.y[i], z = v.pos.z[i];
+            const int jx = floor_div_edge((double)x, e0), jy = floor_div_edge((double)y, e1),
+                      jz = floor_div_edge((double)z, e2);
+            if (jx) {
+                v.ix[i] += jx;
+                x = x - (R)(jx * e0);
+                v.pos.x[i] = x;
+            }
+            if (jy) {
+                v.iy[i] += jy;
+                y = y - (R)(jy * e1);
+                v.pos.y[i] = y;
+            }
+            if (jz) {
+                v.iz[i] += jz;
+                z = z - (R)(jz * e2);
+                v.pos.z[i] = z;
+            }
+            s = slot_of(g, (double)x, (double)y, (double)z);
+            key[i] = s;
+        }
+        unsigned peers = __match_any_sync(0xffffffffu, s);
+        if (ok && lane == __ffs(peers) - 1) atomicAdd(count + s, __popc(peers));
+    }
+}
+
 // place every particle inside its cell; the order inside a cell is fixed
 // afterwards by k_segsort.  Each warp handles kPermRounds groups of 32
 // consecutive particles and issues all their cursor atomics before using any
@@ -134,10 +174,13 @@ __global__ void k_segsort_big(const int *__restrict__ start, const int *__restri
     }
 }
 
+// gated != 0: a particle with neither MD nor PAST_MD set is known to have
+// zero force and force_old, so those are written as zeros without a read
 template <typename R>
 __global__ void k_gather(PView<R> s, PView<R> d, const int *__restrict__ perm, int N,
-                         int with_force, int with_force_old)
+                         int with_force, int with_force_old, int gated)
 {
+    const int fmask = (1 << MD_BIT) | (1 << PAST_MD_BIT);
     for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < N;
          j += (long long)gridDim.x * blockDim.x) {
         const int i = perm[j];
@@ -158,15 +201,16 @@ __global__ void k_gather(PView<R> s, PView<R> d, const int *__restrict__ perm, i
         d.id[j] = id;
         d.species[j] = sp;
         d.flags[j] = fl;
+        const bool live = !gated || (fl & fmask);
         if (with_force) {
-            d.force.x[j] = s.force.x[i];
-            d.force.y[j] = s.force.y[i];
-            d.force.z[j] = s.force.z[i];
+            d.force.x[j] = live ? s.force.x[i] : (R)0;
+            d.force.y[j] = live ? s.force.y[i] : (R)0;
+            d.force.z[j] = live ? s.force.z[i] : (R)0;
         }
         if (with_force_old) {
-            d.force_old.x[j] = s.force_old.x[i];
-            d.force_old.y[j] = s.force_old.y[i];
-            d.force_old.z[j] = s.force_old.z[i];
+            d.force_old.x[j] = live ? s.force_old.x[i] : (R)0;
+            d.force_old.y[j] = live ? s.force_old.y[i] : (R)0;
+            d.force_old.z[j] = live ? s.force_old.z[i] : (R)0;
         }
     }
 }
@@ -220,11 +264,11 @@ int sort_perm_segments(rmpcd_cells *c, rmpcd_particles *p)
 }
 
 template <typename R>
-static int gather_t(rmpcd_particles *p)
+static int gather_t(rmpcd_particles *p, bool gated = false)
 {
     if (p->N > 0) {
         k_gather<R><<<grid_for(p->N, 256), 256, 0, stream()>>>(
-            cur<R>(p), alt<R>(p), p->perm, p->N, p->force_zero ? 0 : 1, p->force_old_zero ? 0 : 1);
+            cur<R>(p), alt<R>(p), p->perm, p->N, p->force_zero ? 0 : 1, p->force_old_zero ? 0 : 1, gated ? 1 : 0);
         RMPCD_CHECK_LAUNCH();
     }
     p->cur = 1 - p->cur;
@@ -255,6 +299,32 @@ int gather_all(rmpcd_particles *p)
 {
     if (p->precision == RMPCD_FP32) return gather_t<float>(p);
     return gather_t<double>(p);
+}
+
+template <typename R>
+static int sort_particles_flagged_t(rmpcd_cells *c, rmpcd_particles *p, const double edges[3])
+{
+    {
+        PhaseTimer t("count");
+        cudaStream_t st = stream();
+        RMPCD_CUDA_TRY(cudaMemsetAsync(c->count, 0, (size_t)c->S * sizeof(int), st));
+        if (p->N > 0)
+            k_pbc_key_count<R><<<grid_for(p->N, 256), 256, 0, st>>>(grid_of(c), cur<R>(p), edges[0], edges[1],
+                                                                   edges[2], p->N, p->key, c->count);
+        RMPCD_CHECK_LAUNCH();
+        int rc = exclusive_scan(c->count, c->start, c->cursor, c->S, c->scan_tmp, false, st);
+        if (rc) return rc;
+    }
+    PhaseTimer t("sort");
+    int rc = build_perm(c, p);
+    if (rc) return rc;
+    return gather_t<R>(p, true);
+}
+
+int sort_particles_flagged(rmpcd_cells *c, rmpcd_particles *p, const double edges[3])
+{
+    if (p->precision == RMPCD_FP32) return sort_particles_flagged_t<float>(c, p, edges);
+    return sort_particles_flagged_t<double>(c, p, edges);
 }
 
 int sort_particles(rmpcd_cells *c, rmpcd_particles *p)

@@ -29,6 +29,11 @@ int build_perm(rmpcd_cells *c, rmpcd_particles *p);
 int gather_all(rmpcd_particles *p);
 // full sort
 int sort_particles(rmpcd_cells *c, rmpcd_particles *p);
+// apply_pbc with the given edges, then the full sort, for a system in which a
+// particle with neither MD nor PAST_MD set has zero force and force_old (the
+// state compute_force and its flag roll maintain): those entries are written
+// as zeros instead of being gathered
+int sort_particles_flagged(rmpcd_cells *c, rmpcd_particles *p, const double edges[3]);
 // ascending merge sort of the *n_big queued cells big[] of more than 64
 // particles (tmp: scratch of the extent of perm)
 void launch_segsort_big(const int *start, const int *count, const int *big, const int *n_big, int *perm,

@@ -7,6 +7,10 @@
 
 namespace rmpcd {
 
+// whether phase timers are on (their event records must not be captured
+// into CUDA graphs)
+bool timers_on();
+
 class PhaseTimer {
   public:
     explicit PhaseTimer(const char *name);

@@ -122,23 +122,31 @@ def test_bulk_shapes_give_identical_results(rm, oracle, precision):
         rm.set_bulk_shape(precision, keep)
 
 
-@pytest.mark.parametrize("precision", [64, 32])
-def test_n_colloids_native_loop_matches_call_by_call(rm, precision):
+@pytest.mark.parametrize("precision,graphs", [(64, True), (32, True), (64, False)])
+def test_n_colloids_native_loop_matches_call_by_call(rm, precision, graphs):
     """rmpcd_ncolloids_run issues the program's calls in C; the state after
     thermalisation (with the 10th-interval rescaling) and a temperature ramp
-    equals the Python loop making the same calls one by one (flags and both
-    force buffers included: the native loop rolls flags over the MD cells
-    only, from the third MD step after a sort on)."""
+    equals the Python loop making the same calls one by one (flags, pos_old
+    and both force buffers included: the native loop rolls flags over the MD
+    cells only from the third MD step after a sort on, reads force entries of
+    flagged particles only, and copies pos_old of the MD cells only except
+    at its last sort)."""
     from rmpcdmd_b200.programs import NColloidsPBC
 
     kw = dict(L=(24, 24, 24), rho=10, N_MD=10, N_colloids=8, seed=77, T_final=0.5, precision=precision)
     a = NColloidsPBC(**kw)
     b = NColloidsPBC(**kw)
-    a.thermalise(10, native=False)
-    b.thermalise(10, native=True)
-    a.run(3, native=False)
-    b.run(3, native=True)
-    for f in ("pos", "vel", "image", "id", "flags", "force", "force_old"):
+    from rmpcdmd_b200._capi import call
+
+    call("rmpcd_ncolloids_set_graphs", int(graphs))
+    try:
+        a.thermalise(10, native=False)
+        b.thermalise(10, native=True)
+        a.run(3, native=False)
+        b.run(3, native=True)
+    finally:
+        call("rmpcd_ncolloids_set_graphs", 1)
+    for f in ("pos", "pos_old", "vel", "image", "id", "flags", "force", "force_old"):
         assert np.array_equal(a.solvent.download(f), b.solvent.download(f)), f
     for f in ("pos", "vel", "force", "image"):
         assert np.array_equal(a.colloids.download(f), b.colloids.download(f)), f
