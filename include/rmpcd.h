@@ -235,6 +235,52 @@ int rmpcd_cell_md_pos_zwall(rmpcd_cells *c, rmpcd_particles *p, double dt, int m
 int rmpcd_apply_pbc(rmpcd_particles *p, const double edges[3]);  /* :202-217 */
 int rmpcd_rattle_dimer_pos(rmpcd_particles *p, double d, double dt, const double edges[3]); /* :265-296 */
 int rmpcd_rattle_dimer_vel(rmpcd_particles *p, double d, double dt, const double edges[3]); /* :298-319 */
+
+/* ------------------------------------------------------------------ */
+/* Rigid-body colloids (programs/single_body.f90), FP64 systems.        */
+/* links: n_link pairs of 1-based particle numbers, the reference's     */
+/* links(2, n_link); distances: n_link target lengths.                   */
+/* ------------------------------------------------------------------ */
+/* rattle_body_pos, src/md.f90:321-408.  Needs pos_rattle (which is left
+ * unwrapped relative to particle 1, as the reference leaves it).
+ * *iterations = the reference's rattle_i at exit: the sweep that converged,
+ * or 1001 when 1000 sweeps did not (the reference warns when it is 1000). */
+int rmpcd_rattle_body_pos(rmpcd_particles *p, const int *links, const double *distances, int n_link,
+                          double dt, const double edges[3], double precision, int *iterations);
+/* rattle_body_vel, src/md.f90:410-480 */
+int rmpcd_rattle_body_vel(rmpcd_particles *p, const int *links, const double *distances, int n_link,
+                          double dt, const double edges[3], double precision, int *iterations);
+/* elastic_network, src/md.f90:516-544: adds the harmonic link forces to
+ * force and returns the energy */
+int rmpcd_elastic_network(rmpcd_particles *p, const int *links, const double *distances, int n_link,
+                          double k, const double edges[3], double *energy);
+
+/* rigid_body_t, src/md.f90:40-58: the body's scalar state (device
+ * resident; read and written with rmpcd_rigid_body_get / _set).  q is
+ * (s, x, y, z). */
+typedef struct rmpcd_rigid_body_state {
+    double mass;
+    double pos[3], vel[3], force[3];
+    double q[4];
+    double L[3], torque[3];
+    double I_body[3], omega_body[3];
+} rmpcd_rigid_body_state;
+typedef struct rmpcd_rigid_body rmpcd_rigid_body;
+/* rigid_body_init, src/md.f90:547-588 (beads i_start..i_stop, 1-based) */
+int rmpcd_rigid_body_init(rmpcd_rigid_body **rb, rmpcd_particles *p, int i_start, int i_stop,
+                          const double edges[3]);
+int rmpcd_rigid_body_destroy(rmpcd_rigid_body *rb);
+/* rigid_body_compute_force_torque, src/md.f90:591-607 */
+int rmpcd_rigid_body_compute_force_torque(rmpcd_rigid_body *rb, rmpcd_particles *p);
+/* rigid_body_vv1, src/md.f90:613-673 (the quaternion iteration, unbounded
+ * in the reference, stops after 100000 rounds with RMPCD_ERR_DEVICE) */
+int rmpcd_rigid_body_vv1(rmpcd_rigid_body *rb, rmpcd_particles *p, double dt, double treshold,
+                         const double edges[3]);
+/* rigid_body_vv2, src/md.f90:679-700 */
+int rmpcd_rigid_body_vv2(rmpcd_rigid_body *rb, rmpcd_particles *p, double dt);
+/* state (and, if pos_body is not null, the 3 x n_beads body-frame positions) */
+int rmpcd_rigid_body_get(const rmpcd_rigid_body *rb, rmpcd_rigid_body_state *state, double *pos_body);
+int rmpcd_rigid_body_set(rmpcd_rigid_body *rb, const rmpcd_rigid_body_state *state);
 /* colloid velocity-Verlet halves written inline in the programs
  * (programs/single_dimer_pbc.f90:312-315,356-359); mass[k] per particle */
 int rmpcd_colloid_vv_pos(rmpcd_particles *p, double dt, const double *mass);

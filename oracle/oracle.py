@@ -58,6 +58,7 @@ def lib():
         _lib.orc_compute_force_n2.restype = C.c_double
         _lib.orc_normal.restype = C.c_double
         _lib.orc_lj_energy.restype = C.c_double
+        _lib.orc_elastic_network.restype = C.c_double
         _lib.orc_rng_u2.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32,
                                     C.POINTER(C.c_double)]
         _lib.orc_rand_sphere.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(C.c_double)]
@@ -443,3 +444,68 @@ def bulk_run(p: Particles, c: Cells, n_intervals, tau, seed, step_base, alpha=No
                        dp(p.vel), ip(p.id), ip(p.species), ip(p.flags), ip(c.cell_count), ip(c.cell_start),
                        dp(out))
     c.origin = out
+
+
+# ---------------------------------------------------------------------------
+# rigid-body colloids (src/md.f90:321-700)
+# ---------------------------------------------------------------------------
+def _links(links, distances):
+    lk = np.ascontiguousarray(links, np.int32).reshape(-1, 2)
+    d = np.ascontiguousarray(distances, np.float64).reshape(-1)
+    assert len(lk) == len(d)
+    return lk, d
+
+
+def rattle_body_pos(p: Particles, links, distances, dt, edges, precision):
+    """rattle_body_pos; returns the reference's rattle_i at exit."""
+    lk, d = _links(links, distances)
+    e = np.ascontiguousarray(edges, np.float64)
+    im = np.zeros(6 * p.N, np.int32)
+    return int(lib().orc_rattle_body_pos(p.N, dp(p.pos), dp(p.vel), dp(p.pos_rattle), ip(p.species), dp(p.mass),
+                                         ip(lk), dp(d), len(d), C.c_double(dt), dp(e), C.c_double(precision),
+                                         ip(im)))
+
+
+def rattle_body_vel(p: Particles, links, distances, dt, edges, precision):
+    lk, d = _links(links, distances)
+    e = np.ascontiguousarray(edges, np.float64)
+    im = np.zeros(6 * p.N, np.int32)
+    return int(lib().orc_rattle_body_vel(p.N, dp(p.pos), dp(p.vel), ip(p.species), dp(p.mass), ip(lk), dp(d),
+                                         len(d), dp(e), C.c_double(precision), ip(im)))
+
+
+def elastic_network(p: Particles, links, distances, k, edges):
+    lk, d = _links(links, distances)
+    e = np.ascontiguousarray(edges, np.float64)
+    return float(lib().orc_elastic_network(dp(p.pos), dp(p.force), ip(lk), dp(d), len(d), C.c_double(k), dp(e)))
+
+
+class RigidBody:
+    """rigid_body_t; state st[26] = mass, pos, vel, force, q (s,x,y,z), L,
+    torque, I_body, omega_body."""
+
+    FIELDS = (("mass", 0, 1), ("pos", 1, 3), ("vel", 4, 3), ("force", 7, 3), ("q", 10, 4), ("L", 14, 3),
+              ("torque", 17, 3), ("I_body", 20, 3), ("omega_body", 23, 3))
+
+    def __init__(self, p: Particles, i_start, i_stop, edges):
+        self.i_start, self.i_stop = int(i_start), int(i_stop)
+        self.st = np.zeros(26)
+        self.pos_body = np.zeros((self.i_stop - self.i_start + 1, 3))
+        e = np.ascontiguousarray(edges, np.float64)
+        lib().orc_rigid_body_init(dp(p.pos), dp(p.vel), ip(p.image), ip(p.species), dp(p.mass), self.i_start,
+                                  self.i_stop, dp(e), dp(self.st), dp(self.pos_body))
+
+    def state(self):
+        return {n: (self.st[a] if k == 1 else self.st[a:a + k].copy()) for n, a, k in self.FIELDS}
+
+    def compute_force_torque(self, p: Particles):
+        lib().orc_rigid_body_force_torque(dp(p.force), self.i_start, self.i_stop, dp(self.st), dp(self.pos_body))
+
+    def vv1(self, p: Particles, dt, treshold, edges):
+        e = np.ascontiguousarray(edges, np.float64)
+        return int(lib().orc_rigid_body_vv1(dp(p.pos), self.i_start, self.i_stop, dp(self.st), dp(self.pos_body),
+                                            C.c_double(dt), C.c_double(treshold), dp(e)))
+
+    def vv2(self, p: Particles, dt):
+        lib().orc_rigid_body_vv2(dp(p.vel), self.i_start, self.i_stop, dp(self.st), dp(self.pos_body),
+                                 C.c_double(dt))

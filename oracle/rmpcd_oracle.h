@@ -267,4 +267,24 @@ void orc_bulk_run(const orc_grid *g_in, int N, int n_intervals, double tau,
 #ifdef __cplusplus
 }
 #endif
+/* ---------------- rigid-body colloids (src/md.f90:321-700) ---------------- */
+/* links: n_link pairs of 1-based particle numbers; im: 6 N ints of scratch.
+ * Returns the reference's rattle_i at exit (1001: no convergence). */
+int orc_rattle_body_pos(int N, double *pos, double *vel, double *pos_rattle, const int *species,
+                        const double *mass, const int *links, const double *dist, int n_link, double dt,
+                        const double *edges, double precision, int *im);
+int orc_rattle_body_vel(int N, double *pos, double *vel, const int *species, const double *mass,
+                        const int *links, const double *dist, int n_link, const double *edges,
+                        double precision, int *im);
+double orc_elastic_network(const double *pos, double *force, const int *links, const double *dist, int n_link,
+                           double kel, const double *edges);
+/* rigid body state st[26] = mass, pos3, vel3, force3, q4 (s,x,y,z), L3, torque3, I_body3, omega_body3 */
+void orc_rigid_body_init(const double *pos, const double *vel, const int *image, const int *species,
+                         const double *mass_table, int i_start, int i_stop, const double *edges, double *st,
+                         double *pos_body);
+void orc_rigid_body_force_torque(const double *force, int i_start, int i_stop, double *st, const double *pos_body);
+int orc_rigid_body_vv1(double *pos, int i_start, int i_stop, double *st, const double *pos_body, double dt,
+                       double treshold, const double *edges);
+void orc_rigid_body_vv2(double *vel, int i_start, int i_stop, double *st, const double *pos_body, double dt);
+
 #endif

@@ -74,6 +74,22 @@ class NCOLLOIDS_STATE(C.Structure):
 
 
 CELLS_P = c_void_p
+class RIGID_STATE(C.Structure):
+    """rmpcd_rigid_body_state: rigid_body_t's scalar state (src/md.f90:40-58)."""
+
+    _fields_ = [
+        ("mass", C.c_double),
+        ("pos", C.c_double * 3),
+        ("vel", C.c_double * 3),
+        ("force", C.c_double * 3),
+        ("q", C.c_double * 4),
+        ("L", C.c_double * 3),
+        ("torque", C.c_double * 3),
+        ("I_body", C.c_double * 3),
+        ("omega_body", C.c_double * 3),
+    ]
+
+
 PART_P = c_void_p
 NL_P = c_void_p
 LJ_P = C.POINTER(LJ)
@@ -148,6 +164,16 @@ PROTOTYPES = {
     "rmpcd_cell_md_pos_zwall": [CELLS_P, PART_P, C.c_double, C.c_int],
     "rmpcd_apply_pbc": [PART_P, c_double_p],
     "rmpcd_rattle_dimer_pos": [PART_P, C.c_double, C.c_double, c_double_p],
+    "rmpcd_rattle_body_pos": [PART_P, c_int_p, c_double_p, C.c_int, C.c_double, c_double_p, C.c_double, c_int_p],
+    "rmpcd_rattle_body_vel": [PART_P, c_int_p, c_double_p, C.c_int, C.c_double, c_double_p, C.c_double, c_int_p],
+    "rmpcd_elastic_network": [PART_P, c_int_p, c_double_p, C.c_int, C.c_double, c_double_p, c_double_p],
+    "rmpcd_rigid_body_init": [C.POINTER(c_void_p), PART_P, C.c_int, C.c_int, c_double_p],
+    "rmpcd_rigid_body_destroy": [c_void_p],
+    "rmpcd_rigid_body_compute_force_torque": [c_void_p, PART_P],
+    "rmpcd_rigid_body_vv1": [c_void_p, PART_P, C.c_double, C.c_double, c_double_p],
+    "rmpcd_rigid_body_vv2": [c_void_p, PART_P, C.c_double],
+    "rmpcd_rigid_body_get": [c_void_p, C.POINTER(RIGID_STATE), c_double_p],
+    "rmpcd_rigid_body_set": [c_void_p, C.POINTER(RIGID_STATE)],
     "rmpcd_rattle_dimer_vel": [PART_P, C.c_double, C.c_double, c_double_p],
     "rmpcd_colloid_vv_pos": [PART_P, C.c_double, c_double_p],
     "rmpcd_colloid_vv_vel": [PART_P, C.c_double, c_double_p],

@@ -17,7 +17,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._capi import LJ, RNG, RmpcdError, call, lib
+from ._capi import LJ, RIGID_STATE, RNG, RmpcdError, call, lib
 
 FP64 = 64
 FP32 = 32
@@ -515,6 +515,98 @@ def rattle_dimer_pos(p: ParticleSystem, d: float, dt: float, edges) -> None:
 
 def rattle_dimer_vel(p: ParticleSystem, d: float, dt: float, edges) -> None:
     call("rmpcd_rattle_dimer_vel", p.handle, float(d), float(dt), _dp(_d3(edges)))
+
+
+def _links(links, distances):
+    lk = np.ascontiguousarray(links, np.int32).reshape(-1, 2)
+    d = np.ascontiguousarray(distances, np.float64).reshape(-1)
+    if len(lk) != len(d):
+        raise ValueError("one distance per link")
+    return lk, d
+
+
+def rattle_body_pos(p: ParticleSystem, links, distances, dt: float, edges, precision: float) -> int:
+    """src/md.f90:321-408.  links: (n_link, 2) 1-based particle numbers (the
+    reference's links(2, n_link)).  Returns the reference's rattle_i at exit
+    (1001 when 1000 sweeps did not converge)."""
+    lk, d = _links(links, distances)
+    it = C.c_int(0)
+    call("rmpcd_rattle_body_pos", p.handle, _ip(lk), _dp(d), len(d), float(dt), _dp(_d3(edges)), float(precision),
+         C.byref(it))
+    return it.value
+
+
+def rattle_body_vel(p: ParticleSystem, links, distances, dt: float, edges, precision: float) -> int:
+    """src/md.f90:410-480."""
+    lk, d = _links(links, distances)
+    it = C.c_int(0)
+    call("rmpcd_rattle_body_vel", p.handle, _ip(lk), _dp(d), len(d), float(dt), _dp(_d3(edges)), float(precision),
+         C.byref(it))
+    return it.value
+
+
+def elastic_network(p: ParticleSystem, links, distances, k: float, edges) -> float:
+    """src/md.f90:516-544: adds the link forces to force, returns the energy."""
+    lk, d = _links(links, distances)
+    e = C.c_double(0)
+    call("rmpcd_elastic_network", p.handle, _ip(lk), _dp(d), len(d), float(k), _dp(_d3(edges)), C.byref(e))
+    return e.value
+
+
+class RigidBody:
+    """rigid_body_t (src/md.f90:40-58): init, compute_force_torque, vv1, vv2
+    on the beads i_start..i_stop (1-based) of an FP64 particle system; the
+    state lives on the device (``state()`` reads it)."""
+
+    def __init__(self, p: ParticleSystem, i_start: int, i_stop: int, edges):
+        h = C.c_void_p()
+        call("rmpcd_rigid_body_init", C.byref(h), p.handle, int(i_start), int(i_stop), _dp(_d3(edges)))
+        self._h = h
+        self.i_start, self.i_stop = int(i_start), int(i_stop)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                call("rmpcd_rigid_body_destroy", h)
+            except Exception:
+                pass
+            self._h = None
+
+    def state(self) -> dict:
+        st = RIGID_STATE()
+        call("rmpcd_rigid_body_get", self._h, C.byref(st), None)
+        return {n: (getattr(st, n) if n == "mass" else np.array(getattr(st, n)[:])) for n, _ in st._fields_}
+
+    def pos_body(self) -> np.ndarray:
+        st = RIGID_STATE()
+        out = np.zeros((self.i_stop - self.i_start + 1, 3))
+        call("rmpcd_rigid_body_get", self._h, C.byref(st), _dp(out))
+        return out
+
+    def set_state(self, **fields) -> None:
+        st = RIGID_STATE()
+        call("rmpcd_rigid_body_get", self._h, C.byref(st), None)
+        for n, v in fields.items():
+            if n == "mass":
+                st.mass = float(v)
+            else:
+                arr = getattr(st, n)
+                for k, x in enumerate(np.asarray(v, np.float64).reshape(-1)):
+                    arr[k] = x
+        call("rmpcd_rigid_body_set", self._h, C.byref(st))
+
+    def compute_force_torque(self, p: ParticleSystem) -> None:
+        call("rmpcd_rigid_body_compute_force_torque", self._h, p.handle)
+
+    def vv1(self, p: ParticleSystem, dt: float, treshold: float, edges) -> None:
+        call("rmpcd_rigid_body_vv1", self._h, p.handle, float(dt), float(treshold), _dp(_d3(edges)))
+
+    def vv2(self, p: ParticleSystem, dt: float) -> None:
+        call("rmpcd_rigid_body_vv2", self._h, p.handle, float(dt))
+
+
+__all__ += ["rattle_body_pos", "rattle_body_vel", "elastic_network", "RigidBody"]
 
 
 def colloid_vv_pos(p: ParticleSystem, dt: float, mass) -> None:

@@ -95,7 +95,9 @@ int check_dev_error(unsigned *bits_out)
         if (bits & DEV_ERR_WALL_LOOP)
             return fail(RMPCD_ERR_DEVICE, "wall collision loop exceeded 64 crossings in one step");
         if (bits & DEV_ERR_RATTLE)
-            return fail(RMPCD_ERR_DEVICE, "rattle_dimer_pos: negative discriminant");
+            return fail(RMPCD_ERR_DEVICE, "rattle: negative discriminant or bead species outside the mass table");
+        if (bits & DEV_ERR_QUAT_LOOP)
+            return fail(RMPCD_ERR_DEVICE, "rigid_body_vv1: quaternion iteration did not converge");
         return fail(RMPCD_ERR_DEVICE, "device error bits 0x%x", bits);
     }
     return RMPCD_OK;
