@@ -99,8 +99,22 @@ class SingleDimerPBC:
         O.change_species(s, c, self.edges, self.cut_sq[0, 0], self.cut_sq[0, 1], self.prob, self.seed, self._next())
 
     def interval(self):
+        self.md_loop()
+        self.mpcd()
+
+    def md_loop(self):
         for _ in range(self.N_MD):
             self.md_step()
+
+    def thermo(self):
+        """programs/single_dimer_pbc.f90:388-396: internal energy e1 + e2 +
+        kinetic and the centre-of-mass velocity after md_loop."""
+        cv = self.c.vel
+        kin = (self.mass[0] * (cv[0] ** 2).sum() + self.mass[1] * (cv[1] ** 2).sum()) / 2 + (self.s.vel ** 2).sum() / 2
+        vcom = (self.s.vel.sum(0) + self.mass[0] * cv[0] + self.mass[1] * cv[1]) / (self.N + self.mass[0] + self.mass[1])
+        return dict(internal=self.e1 + self.e2 + kin, v_com=vcom)
+
+    def mpcd(self):
         self.cells.random_shift(self.seed, self._next())
         self._resort()
         O.simple_mpcd_step(self.s, self.cells, self.seed, self._next(), thermostat=self.do_thermostat, T=self.T,

@@ -117,8 +117,10 @@ class SingleDimerPBC:
         c.switch_force()
         s.zero_force()
         c.zero_force()
-        self.e1 = A.compute_force(c, s, self.neigh, self.edges, self.solvent_colloid_lj, energy=want_energy)
-        self.e2 = A.compute_force_n2(c, self.edges, self.colloid_lj, energy=want_energy)
+        e1 = A.compute_force(c, s, self.neigh, self.edges, self.solvent_colloid_lj, energy=want_energy)
+        e2 = A.compute_force_n2(c, self.edges, self.colloid_lj, energy=want_energy)
+        if want_energy:
+            self.e1, self.e2 = e1, e2
         A.md_vel(s, dt)
         A.colloid_vv_vel(c, dt, self.mass)
         A.rattle_dimer_vel(c, self.d, dt, self.edges)
@@ -137,8 +139,25 @@ class SingleDimerPBC:
 
     def interval(self):
         """md_loop followed by the MPCD part, programs/single_dimer_pbc.f90:303-443."""
-        for _ in range(self.N_MD):
-            self.md_step()
+        self.md_loop()
+        self.mpcd()
+
+    def md_loop(self, want_energy: bool = False):
+        """The N_MD steps of md_loop (programs/single_dimer_pbc.f90:306-384);
+        with want_energy the last step's e1, e2 are kept (the thermo sample)."""
+        for j in range(self.N_MD):
+            self.md_step(want_energy=want_energy and j == self.N_MD - 1)
+
+    def thermo(self):
+        """The thermo sample taken after md_loop (programs/single_dimer_pbc.f90:388-396):
+        temperature, potential e1 + e2, kinetic, internal energy and v_com."""
+        o = self.observables()
+        pot = self.e1 + self.e2
+        return dict(temperature=o["temperature"], potential=pot, kinetic=o["kinetic"],
+                    internal=pot + o["kinetic"], v_com=o["v_com"])
+
+    def mpcd(self):
+        """The MPCD part of an interval (programs/single_dimer_pbc.f90:399-426)."""
         self.cells.random_shift(self.rng)
         self._resort()
         A.simple_mpcd_step(self.solvent, self.cells, self.rng, thermostat=self.do_thermostat, T=self.T,

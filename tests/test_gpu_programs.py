@@ -74,6 +74,33 @@ def test_single_dimer_pbc_bit_exact(rm, oracle, n_int):
     assert g.rng.step == o.step
 
 
+def test_reference_dimer_test(rm):
+    """test/dimer_test.py:13-22 on test/dimer_test.parameters, full length
+    (200 loops after 20 of equilibration): the internal energy e1 + e2 +
+    kinetic sampled after each md_loop has std < 0.1 and the centre-of-mass
+    velocity is constant to 1e-15."""
+    from rmpcdmd_b200.programs import SingleDimerPBC
+
+    g = SingleDimerPBC(L=(24, 24, 24), rho=10, T=1.0, tau=1.0, N_MD=125, sigma_C=3.0, sigma_N=3.0, d=6.5,
+                       epsilon_C=(1.0, 1.0), epsilon_N=(1.0, 0.2), epsilon_CC=1.0, epsilon_NC=1.0, epsilon_NN=1.0,
+                       probability=1.0, bulk_rmpcd=False, do_thermostat=False, do_hydro=True, seed=5)
+    n_loop, equilibration = 200, 20
+    E, V = [], []
+    for i in range(0, n_loop + equilibration + 1):
+        g.md_loop(want_energy=i >= equilibration)
+        if i >= equilibration:
+            th = g.thermo()
+            E.append(th["internal"])
+            V.append(th["v_com"])
+        g.mpcd()
+    E, V = np.array(E), np.array(V)
+    assert len(E) == n_loop + 1
+    assert (E - E.mean()).std() < 0.1
+    assert np.abs(V - V.mean(0)).max() < 1e-15
+    # reactions happened and B was refuelled (species 2 present, then converted)
+    assert g.n_extra_sorting > 0
+
+
 def test_n_colloids_pbc_bit_exact(rm, oracle):
     """programs/n_colloids_pbc.f90: thermalisation (MPC-AT + rescaling) and
     production intervals with lazy cell-wise streaming, against the oracle."""

@@ -174,3 +174,31 @@ def test_bulk_reaction_endothermic_energy_and_pick(oracle):
         assert abs(kin(v0[a:a + n]) - kin(p.vel[a:a + n]) - du) < 1e-9
         assert np.allclose(v0[a:a + n].sum(0), p.vel[a:a + n].sum(0), atol=1e-12)
     assert n_fired > 100
+
+
+# test/dimer_test.parameters (programs/single_dimer_pbc.f90 input)
+DIMER_TEST = dict(L=(24, 24, 24), rho=10, T=1.0, tau=1.0, N_MD=125, sigma_C=3.0, sigma_N=3.0, d=6.5,
+                  epsilon_C=(1.0, 1.0), epsilon_N=(1.0, 0.2), epsilon_CC=1.0, epsilon_NC=1.0, epsilon_NN=1.0,
+                  probability=1.0, bulk_rmpcd=False, do_thermostat=False, do_hydro=True)
+
+
+def test_dimer_test_energy_and_momentum(oracle):
+    # test/dimer_test.py:13-22 on test/dimer_test.parameters: the internal
+    # energy sampled after each md_loop fluctuates with std < 0.1 and the
+    # centre-of-mass velocity is constant to 1e-15.  20 + 2 loops here (the
+    # reference runs 200 + 20; the GPU test runs those).
+    from oracle.programs import SingleDimerPBC
+
+    o = SingleDimerPBC(seed=5, **DIMER_TEST)
+    E, V = [], []
+    for i in range(0, 20 + 2 + 1):
+        o.md_loop()
+        if i >= 2:
+            th = o.thermo()
+            E.append(th["internal"])
+            V.append(th["v_com"])
+        o.mpcd()
+    E, V = np.array(E), np.array(V)
+    assert (E - E.mean()).std() < 0.1
+    assert np.abs(V - V.mean(0)).max() < 1e-15
+    assert o.n_extra_sorting > 0
