@@ -180,6 +180,10 @@ int rmpcd_particles_random_placement(rmpcd_particles *p, const double L[3],
                                      uint64_t seed);
 /* Maxwell velocities with the mean removed, programs/single_dimer_pbc.f90:240-245 */
 int rmpcd_particles_maxwell(rmpcd_particles *p, double T, uint64_t seed);
+/* Number of particles with a NaN or infinite position or velocity component
+ * (no counterpart in the reference, which has no such check; a run fed with
+ * such values keeps running, every slot index staying inside the grid). */
+int rmpcd_particles_count_nonfinite(const rmpcd_particles *p, long long *n_bad);
 /* switch(force, force_old), src/common.f90:268-276; force = 0;
  * pos_old = pos; pos_rattle = pos (programs/single_dimer_pbc.f90:311-348) */
 int rmpcd_particles_switch_force(rmpcd_particles *p);

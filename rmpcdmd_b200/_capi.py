@@ -138,6 +138,7 @@ PROTOTYPES = {
     "rmpcd_particles_maximum_displacement": [PART_P, c_double_p],
     "rmpcd_cell_maximum_displacement": [CELLS_P, PART_P, C.c_double, c_double_p],
     "rmpcd_particles_random_placement": [PART_P, c_double_p, PART_P, LJ_P, C.c_uint64],
+    "rmpcd_particles_count_nonfinite": [PART_P, C.POINTER(C.c_longlong)],
     "rmpcd_particles_maxwell": [PART_P, C.c_double, C.c_uint64],
     "rmpcd_particles_switch_force": [PART_P],
     "rmpcd_particles_zero_force": [PART_P],

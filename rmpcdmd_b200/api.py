@@ -97,6 +97,10 @@ class Rng:
     def step(self, v: int) -> None:
         self._s.step = v
 
+    @seed.setter
+    def seed(self, v: int) -> None:
+        self._s.seed = v & 0xFFFFFFFFFFFFFFFF
+
     @property
     def ptr(self):
         return C.byref(self._s)
@@ -297,6 +301,12 @@ class ParticleSystem:
     @property
     def handle(self):
         return self._h
+
+    def count_nonfinite(self) -> int:
+        """Particles with a NaN or infinite position or velocity component."""
+        n = C.c_longlong(0)
+        call("rmpcd_particles_count_nonfinite", self._h, C.byref(n))
+        return n.value
 
     def download(self, field: str) -> np.ndarray:
         if field in _REAL3:

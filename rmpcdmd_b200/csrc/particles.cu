@@ -52,6 +52,22 @@ __global__ void k_id_to_idx(const int *id, int N, int *out)
     }
 }
 
+// particles with a non-finite position or velocity component (one atomic
+// per warp that found any)
+template <typename R>
+__global__ void k_count_nonfinite(Vec3<R> pos, Vec3<R> vel, long long N, unsigned long long *out)
+{
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < N; base += (long long)gridDim.x * blockDim.x) {
+        const long long i = base + threadIdx.x;
+        bool bad = false;
+        if (i < N)
+            bad = !(isfinite(pos.x[i]) && isfinite(pos.y[i]) && isfinite(pos.z[i]) && isfinite(vel.x[i]) &&
+                    isfinite(vel.y[i]) && isfinite(vel.z[i]));
+        const unsigned b = __ballot_sync(0xffffffffu, bad);
+        if (b && (threadIdx.x & 31) == 0) atomicAdd(out, (unsigned long long)__popc(b));
+    }
+}
+
 // maximum_displacement, src/particle_system.f90:357-378
 template <typename R>
 __global__ void k_max_disp(Vec3<R> pos, Vec3<R> old, const int *species, int N,
@@ -602,6 +618,29 @@ int rmpcd_particles_zero_force(rmpcd_particles *p)
             RMPCD_CUDA_TRY(cudaMemsetAsync(p->force[p->cur][k], 0, (size_t)p->N * p->rsize, stream()));
     p->force_zero = true;
     return RMPCD_OK;
+}
+
+int rmpcd_particles_count_nonfinite(const rmpcd_particles *p, long long *n_bad)
+{
+    RMPCD_ARG(p && n_bad, "null argument");
+    *n_bad = 0;
+    if (p->N == 0) return RMPCD_OK;
+    cudaStream_t s = stream();
+    unsigned long long *d = p->d_max;  // the reduction word, free between calls
+    RMPCD_CUDA_TRY(cudaMemsetAsync(d, 0, 8, s));
+    if (p->precision == RMPCD_FP32) {
+        PView<float> v = cur<float>(p);
+        k_count_nonfinite<float><<<grid_for(p->N, 256), 256, 0, s>>>(v.pos, v.vel, p->N, d);
+    } else {
+        PView<double> v = cur<double>(p);
+        k_count_nonfinite<double><<<grid_for(p->N, 256), 256, 0, s>>>(v.pos, v.vel, p->N, d);
+    }
+    RMPCD_CHECK_LAUNCH();
+    unsigned long long h = 0;
+    RMPCD_CUDA_TRY(cudaMemcpyAsync(&h, d, 8, cudaMemcpyDeviceToHost, s));
+    int rc = sync();
+    if (!rc) *n_bad = (long long)h;
+    return rc;
 }
 
 int rmpcd_particles_copy_pos_old(rmpcd_particles *p)

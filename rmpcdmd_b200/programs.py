@@ -58,6 +58,12 @@ class SingleDimerPBC:
                  epsilon_C=(1.0, 1.0), epsilon_N=(1.0, 0.5), epsilon_CC=1.0, epsilon_NC=1.0, epsilon_NN=1.0,
                  probability=1.0, bulk_rmpcd=False, bulk_rate=0.001, do_thermostat=False, do_hydro=True,
                  seed=1, skin=2.0, list_capacity=None, precision=A.FP64, initial_velocities=None):
+        self._init_kwargs = dict(
+            L=[int(x) for x in L], rho=rho, T=T, tau=tau, N_MD=N_MD, sigma_C=sigma_C, sigma_N=sigma_N, d=d,
+            epsilon_C=[float(x) for x in epsilon_C], epsilon_N=[float(x) for x in epsilon_N], epsilon_CC=epsilon_CC,
+            epsilon_NC=epsilon_NC, epsilon_NN=epsilon_NN, probability=probability, bulk_rmpcd=bulk_rmpcd,
+            bulk_rate=bulk_rate, do_thermostat=do_thermostat, do_hydro=do_hydro, seed=int(seed), skin=skin,
+            list_capacity=list_capacity, precision=precision)
         self.L = np.asarray(L, dtype=np.int32)
         self.rho, self.T, self.tau, self.N_MD = rho, T, tau, N_MD
         self.dt = tau / N_MD
@@ -292,6 +298,11 @@ class NColloidsPBC:
     def __init__(self, L=(32, 32, 32), rho=10, T=1.0 / 3.0, T_final=None, tau=1.0, N_MD=100, N_colloids=10,
                  sigma=3.0, epsilon=1.0, epsilon_colloids=1.0, do_hydro=True, do_thermostat=False, seed=1,
                  skin=0.8, list_capacity=None, precision=A.FP64, volume_correction=True):
+        self._init_kwargs = dict(
+            L=[int(x) for x in L], rho=rho, T=T, T_final=T_final, tau=tau, N_MD=N_MD, N_colloids=N_colloids,
+            sigma=sigma, epsilon=epsilon, epsilon_colloids=epsilon_colloids, do_hydro=do_hydro,
+            do_thermostat=do_thermostat, seed=int(seed), skin=skin, list_capacity=list_capacity,
+            precision=precision, volume_correction=volume_correction)
         self.L = np.asarray(L, dtype=np.int32)
         self.rho, self.T_init, self.tau, self.N_MD = rho, T, tau, N_MD
         self.T_final = T if T_final is None else T_final
