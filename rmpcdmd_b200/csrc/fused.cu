@@ -238,10 +238,13 @@ __device__ inline int stream_values(const FusedArgs<R> &A, R &x, R &y, R &z, R v
     return slot_of(A.g_next, (double)x, (double)y, (double)z);
 }
 
+// shared memory of a tile: velocity parts and source indices per particle,
+// the tile-local cell of each particle (one byte) and each cell's local start
+// and count
 template <typename R, typename S>
 constexpr size_t fused_smem()
 {
-    return (size_t)S::kCap * (Rec<R>::kVelBytes + sizeof(int));
+    return (size_t)S::kCap * (Rec<R>::kVelBytes + sizeof(int) + 1) + 2 * (size_t)S::kSlots * sizeof(int);
 }
 
 // the non-velocity part of a record, as loaded from global memory
@@ -309,9 +312,13 @@ __global__ void __launch_bounds__(kFusedThreads, S::kMinBlocks) k_bulk_interval(
     static_assert(SL <= kFusedThreads, "one thread per slot of the tile");
     constexpr int B = Rec<R>::kBytes;
     constexpr int VB = Rec<R>::kVelBytes;
+    static_assert(SL <= 256, "tile-local cell index kept in one byte");
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned char *s_vel = smem;
     int *s_perm = (int *)(smem + (size_t)CAP * VB);
+    int *s_cstart = s_perm + CAP;                           // per cell of the tile
+    int *s_ccount = s_cstart + SL;
+    unsigned char *s_cell = (unsigned char *)(s_ccount + SL);  // per particle
 
     const int t = threadIdx.x;
     const int lane = t & 31;
@@ -333,8 +340,29 @@ __global__ void __launch_bounds__(kFusedThreads, S::kMinBlocks) k_bulk_interval(
         } else {
             for (int j = t; j < np; j += kFusedThreads) s_perm[j] = a0 + j;
         }
-        __syncthreads();
-        if (A.perm && my_n > 1) sort_segment(s_perm + (my_a - a0), my_n);
+        if (A.perm) {
+            // each cell's indices in ascending order (the reference's stable
+            // scatter order): every index is placed at its rank among the
+            // cell's indices, one thread per index, so a crowded cell costs
+            // no more than its share; the ranks go through the (still unused)
+            // velocity buffer and back
+            if (t < SL) {
+                s_cstart[t] = my_a - a0;
+                s_ccount[t] = my_n;
+                for (int k = 0; k < my_n; k++) s_cell[my_a - a0 + k] = (unsigned char)t;
+            }
+            __syncthreads();
+            int *s_tmp = (int *)s_vel;
+            for (int j = t; j < np; j += kFusedThreads) {
+                const int c = s_cell[j], a = s_cstart[c], n = s_ccount[c];
+                const int v = s_perm[j];
+                int r = 0;
+                for (int k = a; k < a + n; k++) r += s_perm[k] < v;
+                s_tmp[a + r] = v;
+            }
+            __syncthreads();
+            for (int j = t; j < np; j += kFusedThreads) s_perm[j] = s_tmp[j];
+        }
         __syncthreads();
         // gather the velocity parts (16 B per particle in FP32, 4 x 8 B in FP64)
         if constexpr (VB == 16) {
