@@ -357,6 +357,7 @@ __global__ void __launch_bounds__(kFusedThreads, S::kMinBlocks) k_bulk_interval(
                 const int c = s_cell[j], a = s_cstart[c], n = s_ccount[c];
                 const int v = s_perm[j];
                 int r = 0;
+#pragma unroll 4
                 for (int k = a; k < a + n; k++) r += s_perm[k] < v;
                 s_tmp[a + r] = v;
             }
