@@ -410,11 +410,17 @@ def run_ours(args):
     results = {}
     tuned = {}
     for precision in (32, 64):
-        # the autotuner times every tile shape of the fused kernel on a
-        # synthetic fluid of this box and keeps the fastest (same results)
-        best, ms_shapes = rm.bulk_autotune([L, L, L], precision, TAU, 5)
-        tuned[f"fp{precision}"] = {"shape": best, "shapes": rm.bulk_shapes(precision),
-                                   "ms_per_5_intervals": [round(m, 3) for m in ms_shapes]}
+        if args.shapes:
+            # a fixed tile shape (for profilers: no autotuning launches)
+            rm.set_bulk_shape(precision, args.shapes[0 if precision == 32 else 1])
+            tuned[f"fp{precision}"] = {"shape": rm.bulk_shape(precision), "shapes": rm.bulk_shapes(precision),
+                                       "fixed": True}
+        else:
+            # the autotuner times every tile shape of the fused kernel on a
+            # synthetic fluid of this box and keeps the fastest (same results)
+            best, ms_shapes = rm.bulk_autotune([L, L, L], precision, TAU, 5)
+            tuned[f"fp{precision}"] = {"shape": best, "shapes": rm.bulk_shapes(precision),
+                                       "ms_per_5_intervals": [round(m, 3) for m in ms_shapes]}
         p, cells, rng = make_system(rm, L, precision)
         barrier(dist)
         with ClockSampler(local) as cs:
@@ -563,6 +569,8 @@ def main(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-dimer", action="store_true", help="skip the single-dimer engine configurations")
+    ap.add_argument("--shapes", type=lambda t: [int(x) for x in t.split(",")], default=None, metavar="S32,S64",
+                    help="use these fused-interval tile shapes instead of autotuning (for profilers)")
     ap.add_argument("--profile-ncolloids", type=int, default=0, metavar="C",
                     help="only run two intervals of n_colloids_pbc with C colloids at 128^3, for profilers")
     ap.add_argument("--profile-dimer", type=int, default=0, metavar="R",
