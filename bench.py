@@ -525,6 +525,81 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def cpu_table(args):
+    """The CPU restatement (oracle, C + OpenMP) timed on bounded samples of
+    the five configurations, with all host threads and with one, for the
+    baseline table: particle-steps/s (MD steps for the colloid programs,
+    MPCD intervals for the bulk fluid).  Prints one JSON line."""
+    from oracle import oracle as O
+    from oracle.programs import NColloidsPBC as ONC
+    from oracle.programs import SingleDimerPBC as OD
+
+    nt = os.cpu_count() or 1
+
+    def dimer_rate(L, n_md, seed=1):
+        o = OD(L=L, rho=RHO, N_MD=DIMER_N_MD, seed=seed, list_capacity=DIMER_LIST_CAPACITY)
+        t0 = time.perf_counter()
+        for _ in range(n_md):
+            o.md_step()
+        t_md = (time.perf_counter() - t0) / n_md
+        t0 = time.perf_counter()
+        o.mpcd()
+        t_mpcd = time.perf_counter() - t0
+        return o.N, t_md + t_mpcd / DIMER_N_MD
+
+    out = {"impl": "reference", "cpu_table": {}, "threads_all": nt}
+    for threads in (nt, 1):
+        O.set_threads(threads)
+        row = {}
+        N, t = dimer_rate((32, 32, 32), 20)
+        row["single_dimer_32"] = {"value": N / t, "sample": "20 MD steps + 1 MPCD part, per MD step"}
+        Ls = 64
+        N = RHO * Ls ** 3
+        c = O.Cells([Ls] * 3)
+        p = O.Particles(N, 1)
+        r = np.random.default_rng(SEED)
+        p.pos[:] = r.random((N, 3)) * Ls
+        p.vel[:] = r.normal(size=(N, 3)) * np.sqrt(T_INIT)
+        p.species[:] = 1
+        c.origin = O.random_shift_values(SEED, 0)
+        p.sort(c)
+        O.bulk_run(p, c, 1, TAU, SEED, 1)
+        t0 = time.perf_counter()
+        O.bulk_run(p, c, 3, TAU, SEED, 3)
+        row["bulk_128"] = {"value": N * 3 / (time.perf_counter() - t0),
+                           "sample": "3 intervals on 64^3 cells (per-particle intensive)"}
+        del p, c
+        N, t = dimer_rate((96, 96, 96), 3 if threads > 1 else 1)
+        row["single_dimer_96"] = {"value": N / t, "sample": "1-3 MD steps + 1 MPCD part, per MD step"}
+        boxes = dimer_boxes_batched()[:8]
+        tot_n = tot_t = 0.0
+        for k, L in enumerate(boxes):
+            n, t = dimer_rate(L, 5, seed=k + 1)
+            tot_n += n
+            tot_t += t
+        row["batched_512"] = {"value": tot_n / tot_t,
+                              "sample": "replicas 0-7 of the 512 (5 MD steps + 1 MPCD part each), run one "
+                                        "after the other; the 512 scale with their particle count"}
+        o = ONC(L=(128, 128, 128), rho=RHO, N_MD=DIMER_N_MD, N_colloids=200, seed=SEED, volume_correction=False)
+        n_md = 3 if threads > 1 else 1
+        t0 = time.perf_counter()
+        for _ in range(n_md):
+            o.md_step()
+        t_md = (time.perf_counter() - t0) / n_md
+        t0 = time.perf_counter()
+        o._catch_up_and_sort()
+        t_sort = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        O.simple_mpcd_step(o.s, o.cells, o.seed, 99, thermostat=True, T=o.T_init, hydro=True)
+        t_srd = time.perf_counter() - t0
+        row["n_colloids_128"] = {"value": o.N / (t_md + (5 * t_sort + t_srd) / DIMER_N_MD),
+                                 "sample": "MD steps + one catch-up/sort and one collision, per MD step with "
+                                           "5 sorts per 100-step interval (the rate the GPU runs see)"}
+        del o
+        out["cpu_table"][f"threads_{threads}"] = row
+    print(json.dumps(out))
+
+
 def profile_dimer(args):
     """A fixed engine workload for profilers: R replicas of the batched
     dimer (cubic sides drawn from {16..48}), FP32 solvent, one interval with
@@ -573,12 +648,16 @@ def main(argv=None):
                     help="use these fused-interval tile shapes instead of autotuning (for profilers)")
     ap.add_argument("--profile-ncolloids", type=int, default=0, metavar="C",
                     help="only run two intervals of n_colloids_pbc with C colloids at 128^3, for profilers")
+    ap.add_argument("--cpu-table", action="store_true",
+                    help="only time the CPU restatement on samples of every configuration (baseline table)")
     ap.add_argument("--profile-dimer", type=int, default=0, metavar="R",
                     help="only run one interval of R batched dimer replicas (graph off), for profilers")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
-    if args.profile_dimer:
+    if args.cpu_table:
+        cpu_table(args)
+    elif args.profile_dimer:
         profile_dimer(args)
     elif args.profile_ncolloids:
         profile_ncolloids(args)
