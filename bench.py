@@ -609,6 +609,8 @@ def profile_dimer(args):
     from rmpcdmd_b200.programs import DimerBatch, SingleDimerPBC
 
     boxes = dimer_boxes_batched()[: args.profile_dimer]
+    if args.profile_box:
+        boxes = [(args.profile_box,) * 3] * args.profile_dimer
     ds = [SingleDimerPBC(L=L, rho=RHO, N_MD=DIMER_N_MD, seed=k + 1, list_capacity=DIMER_LIST_CAPACITY,
                          precision=32) for k, L in enumerate(boxes)]
     b = DimerBatch(ds, use_graph=False)
@@ -648,6 +650,8 @@ def main(argv=None):
                     help="use these fused-interval tile shapes instead of autotuning (for profilers)")
     ap.add_argument("--profile-ncolloids", type=int, default=0, metavar="C",
                     help="only run two intervals of n_colloids_pbc with C colloids at 128^3, for profilers")
+    ap.add_argument("--profile-box", type=int, default=0, metavar="L",
+                    help="with --profile-dimer: every replica in an L^3 box instead of the drawn sides")
     ap.add_argument("--cpu-table", action="store_true",
                     help="only time the CPU restatement on samples of every configuration (baseline table)")
     ap.add_argument("--profile-dimer", type=int, default=0, metavar="R",
