@@ -232,8 +232,9 @@ def dimer_entry(N, ms, n_intervals, precision, peak, peak_kind, extra=None):
 
 def run_dimer(rm, peak, peak_kind, local):
     """single_dimer_pbc through the batched engine: one dimer at 32^3 (plain
-    FP64, and the call-by-call driver for comparison), one at 96^3 (FP32
-    solvent and FP64), and 512 replicas with uneven boxes (FP32 solvent)."""
+    FP64, FP32 solvent, and the call-by-call driver for comparison), one at
+    96^3 (FP32 solvent and FP64), and 512 replicas with uneven boxes (FP32
+    solvent)."""
     from rmpcdmd_b200.programs import SingleDimerPBC
 
     def make(boxes, seeds, precision):
@@ -245,6 +246,8 @@ def run_dimer(rm, peak, peak_kind, local):
                    "dimer sigma=2, d=4.5, p(A->B)=1, refuel beyond 0.45 L; list capacity 4000"}
     ms, N, ex = dimer_time(rm, make([(32, 32, 32)], [SEED], 64), 5)
     out["single_dimer_32_fp64_plain"] = dict(dimer_entry(N, ms, 5, 64, peak, peak_kind, ex), N=N, replicas=1)
+    ms, N, ex = dimer_time(rm, make([(32, 32, 32)], [SEED], 32), 5)
+    out["single_dimer_32_fp32"] = dict(dimer_entry(N, ms, 5, 32, peak, peak_kind, ex), N=N, replicas=1)
     d = make([(32, 32, 32)], [SEED], 64)[0]
     d.interval()
     rm.synchronize()
