@@ -25,7 +25,8 @@
 //       rest of its record, streams and wraps it, keys it in G_{i+1}, counts
 //       it and writes the record in G_i order with coalesced stores.
 //   P2  slot scan of the G_{i+1} counts (starts and scatter cursors).
-//   P3  k_perm: perm[place] = j for every particle j of the new arrays.
+//   P3  k_perm_tiles: perm[place] = j for every particle j of the new arrays
+//       (k_perm for boxes of more than 2^22 slots).
 // The records written by P1 hold exactly the reference's arrays after
 // simple_mpcd_step and mpcd_stream_periodic; the sort into G_{i+1} is
 // completed by the gather of the next P1 (or by the final gather).
@@ -33,6 +34,7 @@
 // HBM traffic of P1 per particle: perm 4 + record read + record write +
 // key 4 (72 B in FP32, 120 B in FP64), plus 12 B per slot, plus a 12-byte
 // image update for each particle that wraps.
+#include <algorithm>
 #include <cmath>
 
 #include "async_copy.cuh"
@@ -95,7 +97,9 @@ struct FusedArgs {
     int S;
     int N;
     int *count_next;          // G_{i+1} histogram (accumulated)
-    int *key_out;             // G_{i+1} slot of out[j]
+    int *key_out;             // G_{i+1} slot of out[j] (packed with its warp group when pack != 0)
+    int *tile_info;           // per tile: first particle and count (written)
+    int pack;
     int *ix, *iy, *iz;        // image, indexed by idx (updated in place on a wrap)
     Grid g_next;
     double e0, e1, e2;        // edges
@@ -304,6 +308,21 @@ __device__ inline int finish_particle(const FusedArgs<double> &A, const unsigned
     return key;
 }
 
+// The next slot of a particle packed with its place in the warp group of
+// equal slots that the counting atomic formed: bits 0-21 slot, 22-26 the
+// distance back to the group's first lane, 27-31 the rank in the group (for
+// the first lane: the group size - 1).  k_perm_tiles replays the same warp
+// chunks and so places every particle without regrouping the keys.
+constexpr int kPackSlotBits = 22;
+
+__device__ inline int pack_key(int key, unsigned peers)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned lead_off = lane - (unsigned)(__ffs(peers) - 1);
+    const unsigned r = lead_off == 0u ? (unsigned)__popc(peers) - 1u : (unsigned)__popc(peers & lanemask_lt());
+    return (int)((unsigned)key | (lead_off << kPackSlotBits) | (r << (kPackSlotBits + 5)));
+}
+
 template <typename R, typename S>
 __global__ void __launch_bounds__(kFusedThreads, S::kMinBlocks) k_bulk_interval(FusedArgs<R> A)
 {
@@ -332,6 +351,10 @@ __global__ void __launch_bounds__(kFusedThreads, S::kMinBlocks) k_bulk_interval(
     }
     const int a0 = A.start[s0];
     const int np = A.start[last] + A.count[last] - a0;
+    if (t == 0) {
+        A.tile_info[2 * blockIdx.x] = a0;
+        A.tile_info[2 * blockIdx.x + 1] = np;
+    }
 
     if (np <= CAP) {
         // ---- staged path ----
@@ -393,11 +416,9 @@ __global__ void __launch_bounds__(kFusedThreads, S::kMinBlocks) k_bulk_interval(
             int jn = j + kFusedThreads;
             if (jn < np) load_rest(nxt, A.in + (size_t)s_perm[jn] * B);
             int key = -1;
-            if (ok) {
-                key = finish_particle(A, s_vel + (size_t)j * VB, cur, A.out + (size_t)(a0 + j) * B);
-                A.key_out[a0 + j] = key;
-            }
+            if (ok) key = finish_particle(A, s_vel + (size_t)j * VB, cur, A.out + (size_t)(a0 + j) * B);
             unsigned peers = __match_any_sync(0xffffffffu, key);
+            if (ok) A.key_out[a0 + j] = A.pack ? pack_key(key, peers) : key;
             if (ok && lane == __ffs(peers) - 1) atomicAdd(A.count_next + key, __popc(peers));
             cur = nxt;
             j = jn;
@@ -428,10 +449,57 @@ __global__ void __launch_bounds__(kFusedThreads, S::kMinBlocks) k_bulk_interval(
                 p[0] = x;
                 p[1] = y;
                 p[2] = z;
-                A.key_out[j] = key;
             }
             unsigned peers = __match_any_sync(0xffffffffu, key);
+            if (ok) A.key_out[j] = A.pack ? pack_key(key, peers) : key;
             if (ok && lane == __ffs(peers) - 1) atomicAdd(A.count_next + key, __popc(peers));
+        }
+    }
+}
+
+// perm[place] = j for every particle of the new arrays, from keys packed by
+// k_bulk_interval: the blocks walk the interval's tiles with the same
+// thread-to-particle mapping, so each warp meets exactly the groups the
+// interval formed; the first lane of a group takes the group's places with
+// one cursor atomic and hands the base to the others by a shuffle (no
+// regrouping of the keys).  Rounds of a thread issue their atomics before
+// using any result.
+constexpr int kPermTileRounds = 4;
+
+__global__ void __launch_bounds__(kFusedThreads) k_perm_tiles(const int *__restrict__ packed,
+                                                              const int *__restrict__ tile_info, int ntiles,
+                                                              int *__restrict__ cursor, int *__restrict__ perm)
+{
+    const int t = threadIdx.x, lane = t & 31;
+    const int slot_mask = (1 << kPackSlotBits) - 1;
+    for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+        const int a0 = tile_info[2 * b], np = tile_info[2 * b + 1];
+        for (int jb0 = 0; jb0 < np; jb0 += kFusedThreads * kPermTileRounds) {
+            unsigned w[kPermTileRounds];
+            int base[kPermTileRounds];
+            bool ok[kPermTileRounds];
+#pragma unroll
+            for (int r = 0; r < kPermTileRounds; r++) {
+                const int j = jb0 + r * kFusedThreads + t;
+                ok[r] = j < np;
+                w[r] = ok[r] ? (unsigned)packed[a0 + j] : 0u;
+            }
+#pragma unroll
+            for (int r = 0; r < kPermTileRounds; r++) {
+                base[r] = 0;
+                if (ok[r] && ((w[r] >> kPackSlotBits) & 31u) == 0u)
+                    base[r] = atomicAdd(cursor + (int)(w[r] & (unsigned)slot_mask),
+                                        (int)((w[r] >> (kPackSlotBits + 5)) & 31u) + 1);
+            }
+#pragma unroll
+            for (int r = 0; r < kPermTileRounds; r++) {
+                const int off = ok[r] ? (int)((w[r] >> kPackSlotBits) & 31u) : 0;
+                const int bb = __shfl_sync(0xffffffffu, base[r], lane - off);
+                if (ok[r]) {
+                    const int rank = off == 0 ? 0 : (int)((w[r] >> (kPackSlotBits + 5)) & 31u);
+                    perm[bb + rank] = a0 + jb0 + r * kFusedThreads + t;
+                }
+            }
         }
     }
 }
@@ -600,6 +668,10 @@ static int bulk_run_fused(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r, doub
     const PView<R> side = cur<R>(p);
     int rb = 0;  // record buffer holding the current arrays
     const int nblocks = (c->S + shape.slots - 1) / shape.slots;
+    const int ntiles = nblocks;
+    // slots fit the packed key for every box up to 2^22 slots (128^3 is 2^21);
+    // larger boxes keep plain keys and regroup them in k_perm
+    const int pack = c->S <= (1 << kPackSlotBits) ? 1 : 0;
     int *perm = nullptr;  // identity for the first interval (data sorted on entry)
     for (int it = 0; it < n_intervals; it++) {
         uint64_t step_c = r->step;
@@ -618,6 +690,8 @@ static int bulk_run_fused(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r, doub
         A.N = p->N;
         A.count_next = c->count_next;
         A.key_out = p->key;
+        A.tile_info = c->start_next;
+        A.pack = pack;
         A.ix = side.ix;
         A.iy = side.iy;
         A.iz = side.iz;
@@ -653,8 +727,14 @@ static int bulk_run_fused(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r, doub
         }
         {
             PhaseTimer t("perm");
-            rc = build_perm_unsorted(c, p);
-            if (rc) return rc;
+            if (pack) {
+                k_perm_tiles<<<ntiles, kFusedThreads, 0, st>>>(p->key, c->start_next,
+                                                                                       ntiles, c->cursor, p->perm);
+                RMPCD_CHECK_LAUNCH();
+            } else {
+                rc = build_perm_unsorted(c, p);
+                if (rc) return rc;
+            }
         }
         perm = p->perm;
     }

@@ -27,7 +27,7 @@ struct rmpcd_cells {
     int *start = nullptr;      // S, 0-based
     int *cursor = nullptr;     // S, scatter cursors
     int *count_next = nullptr; // S, counts of the next grid in fused schedules
-    int *start_next = nullptr; // S, starts of the next grid in fused schedules
+    int *start_next = nullptr; // S ints of fused-schedule scratch (per tile: first particle, count)
     unsigned char *is_md = nullptr;
     unsigned char *is_reac = nullptr;
     int *lut = nullptr;        // n_lut: slot of cell (p0 + L0*(p1 + L1*p2))
