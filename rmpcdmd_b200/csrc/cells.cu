@@ -85,7 +85,7 @@ int rmpcd_cells_init(rmpcd_cells **out, const int L[3], double a, int has_walls)
         cudaMalloc(&c->start_next, S * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&c->is_md, S) != cudaSuccess || cudaMalloc(&c->is_reac, S) != cudaSuccess ||
         cudaMalloc(&c->lut, (size_t)c->n_lut * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&c->scan_tmp, (size_t)(c->scan_blocks + 1) * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&c->scan_tmp, (size_t)c->scan_blocks * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&c->d_red, (size_t)c->red_cap * sizeof(double)) != cudaSuccess) {
         free_cells(c);
         return fail(RMPCD_ERR_CUDA, "cell_system_t%%init: device allocation failed (S=%d)", (int)S);

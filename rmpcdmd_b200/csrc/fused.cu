@@ -721,9 +721,8 @@ static int bulk_run_fused(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r, doub
             int *tmp = c->count;
             c->count = c->count_next;
             c->count_next = tmp;
-            rc = exclusive_scan(c->count, c->start, c->cursor, c->S, c->scan_tmp, false, st);
+            rc = exclusive_scan(c->count, c->start, c->cursor, c->S, c->scan_tmp, c->count_next, st);
             if (rc) return rc;
-            RMPCD_CUDA_TRY(cudaMemsetAsync(c->count_next, 0, (size_t)c->S * sizeof(int), st));
         }
         {
             PhaseTimer t("perm");

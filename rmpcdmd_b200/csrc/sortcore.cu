@@ -225,7 +225,7 @@ static int count_and_scan_t(rmpcd_cells *c, rmpcd_particles *p)
         k_key_count<R><<<grid_for(p->N, 256), 256, 0, st>>>(grid_of(c), v.pos.x, v.pos.y, v.pos.z,
                                                            p->N, p->key, c->count);
     RMPCD_CHECK_LAUNCH();
-    return exclusive_scan(c->count, c->start, c->cursor, c->S, c->scan_tmp, false, st);
+    return exclusive_scan(c->count, c->start, c->cursor, c->S, c->scan_tmp, nullptr, st);
 }
 
 int count_and_scan(rmpcd_cells *c, rmpcd_particles *p, bool)
@@ -312,7 +312,7 @@ static int sort_particles_flagged_t(rmpcd_cells *c, rmpcd_particles *p, const do
             k_pbc_key_count<R><<<grid_for(p->N, 256), 256, 0, st>>>(grid_of(c), cur<R>(p), edges[0], edges[1],
                                                                    edges[2], p->N, p->key, c->count);
         RMPCD_CHECK_LAUNCH();
-        int rc = exclusive_scan(c->count, c->start, c->cursor, c->S, c->scan_tmp, false, st);
+        int rc = exclusive_scan(c->count, c->start, c->cursor, c->S, c->scan_tmp, nullptr, st);
         if (rc) return rc;
     }
     PhaseTimer t("sort");

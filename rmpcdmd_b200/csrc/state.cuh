@@ -31,7 +31,7 @@ struct rmpcd_cells {
     unsigned char *is_md = nullptr;
     unsigned char *is_reac = nullptr;
     int *lut = nullptr;        // n_lut: slot of cell (p0 + L0*(p1 + L1*p2))
-    int *scan_tmp = nullptr;   // block sums of the slot scan
+    int *scan_tmp = nullptr;   // tile totals of the slot scan
     int scan_blocks = 0;
     double *axes = nullptr;    // injected SRD axes (3*S) or null
     double *d_red = nullptr;   // reduction scratch (temperature etc.)

@@ -10,7 +10,8 @@ from helpers import assert_cells_same, assert_same, make_pair
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("L,rho", [([16, 16, 16], 10), ([12, 10, 9], 10), ([6, 5, 4], 300), ([1, 20, 5], 10)])
+@pytest.mark.parametrize("L,rho", [([16, 16, 16], 10), ([12, 10, 9], 10), ([6, 5, 4], 300), ([1, 20, 5], 10),
+                                   ([64, 64, 40], 1)])
 def test_bulk_run_fp64_bit_exact(rm, oracle, L, rho):
     N = int(np.prod(L)) * rho
     (oc, op), (gc, gp) = make_pair(rm, oracle, L, N, seed=N % 101, origin=[-0.1, -0.9, -0.45])
