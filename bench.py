@@ -458,9 +458,10 @@ def run_ours(args):
                          "clocks": r64["clocks"], "fp32_over_fp64": value / fp64_value}
     out["phases_ms"] = {k: round(v[0] * 1e3 / max(1, args.steps), 4)
                         for k, v in r32["phases"].items()}
-    # kernels launched per step: fused interval, 3 scan kernels, key scatter;
-    # plus the final segment sort (2) and gather (1) of the run
-    out["gpu_launches"] = 5 * args.steps + 3
+    # kernels launched per step: fused interval, 2 scan kernels, placement;
+    # plus, once per timed call, the record packing (1), the final segment
+    # sort (2) and gather (1)
+    out["gpu_launches"] = 4 * args.steps + 4
     if not args.no_e2e:
         e2e_steps = max(1, min(args.e2e_steps, args.steps))
         v, hb, db = e2e_run(rm, r32["p"], r32["cells"], r32["rng"], e2e_steps)
