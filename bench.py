@@ -165,6 +165,33 @@ def timed_run(rm, p, cells, rng, steps, warmup):
     return float(ms.value), tm
 
 
+def call_by_call_ms(rm, p, cells, rng, steps):
+    """Device time (ms) of `steps` intervals issued the way the reference's
+    bulk loop issues them (test/setup_bulk_decay.f90:112-121), one C-ABI call
+    per module procedure: simple_mpcd_step, mpcd_stream_periodic,
+    random_shift, sort."""
+    from rmpcdmd_b200._capi import call
+    import ctypes as C
+
+    def interval():
+        rm.simple_mpcd_step(p, cells, rng)
+        rm.mpcd_stream_periodic(p, cells, TAU)
+        cells.random_shift(rng)
+        p.sort(cells)
+
+    interval()
+    rm.synchronize()
+    a, b = C.c_int(), C.c_int()
+    call("rmpcd_mark", C.byref(a))
+    for _ in range(steps):
+        interval()
+    call("rmpcd_mark", C.byref(b))
+    rm.synchronize()
+    ms = C.c_float()
+    call("rmpcd_elapsed_ms", a, b, C.byref(ms))
+    return float(ms.value)
+
+
 def roofline(N, S, precision, phase, peak, peak_kind):
     secs, calls = phase.get("interval_fused", (0.0, 0))
     if not calls:
@@ -432,6 +459,8 @@ def run_ours(args):
         rl = roofline(N, cells.N, precision, phases, peak, peak_kind)
         results[precision] = dict(ms=ms, phases=phases, roofline=rl, clocks=cs.summary(), p=p, cells=cells, rng=rng)
         if precision == 64:
+            cbc_steps = max(1, min(3, args.steps))
+            results[64]["cbc"] = (max_over_ranks(dist, call_by_call_ms(rm, p, cells, rng, cbc_steps)), cbc_steps)
             del p, cells
     r32, r64 = results[32], results[64]
     value = world * N * args.steps / (r32["ms"] * 1e-3)
@@ -454,8 +483,15 @@ def run_ours(args):
     out["autotune"] = tuned
     out["clocks"] = r32["clocks"]
     fp64_value = world * N * args.steps / (r64["ms"] * 1e-3)
+    cbc_ms, cbc_steps = r64["cbc"]
+    cbc_value = world * N * cbc_steps / (cbc_ms * 1e-3)
     out["fp64_plain"] = {"value": fp64_value, "ms_per_step": r64["ms"] / args.steps, "roofline": r64["roofline"],
-                         "clocks": r64["clocks"], "fp32_over_fp64": value / fp64_value}
+                         "clocks": r64["clocks"], "fp32_over_fp64": value / fp64_value,
+                         "call_by_call": {"value": cbc_value, "ms_per_step": cbc_ms / cbc_steps, "steps": cbc_steps,
+                                          "path": "rmpcd_simple_mpcd_step, rmpcd_mpcd_stream_periodic, "
+                                                  "rmpcd_cells_random_shift, rmpcd_particles_sort per interval "
+                                                  "(device time)"},
+                         "fp32_over_fp64_call_by_call": value / cbc_value}
     out["phases_ms"] = {k: round(v[0] * 1e3 / max(1, args.steps), 4)
                         for k, v in r32["phases"].items()}
     # kernels launched per step: fused interval, 2 scan kernels, placement;
