@@ -42,4 +42,50 @@ __device__ inline void cp_async_wait_all()
     asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
+// Bulk copies (cp.async.bulk, the TMA unit's untiled form, sm_90 and later;
+// no multicast) completing on a shared-memory mbarrier.  Source, destination
+// and size must be multiples of 16 bytes.
+__device__ inline void mbar_init(unsigned long long *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+
+// one arrival that also announces the bytes the phase's copies will deliver
+__device__ inline void mbar_arrive_expect_tx(unsigned long long *bar, unsigned bytes)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(
+                     smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ inline void bulk_copy_to_smem(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ inline bool mbar_try_wait(unsigned long long *bar, unsigned parity)
+{
+    unsigned done;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(done)
+                 : "r"(smem_addr(bar)), "r"(parity)
+                 : "memory");
+    return done != 0;
+}
+
+// waits for the phase of the given parity at most `polls` times; false if
+// it did not complete
+__device__ inline bool mbar_wait_bounded(unsigned long long *bar, unsigned parity, int polls)
+{
+    for (int i = 0; i < polls; i++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
 }  // namespace rmpcd

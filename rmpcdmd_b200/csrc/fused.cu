@@ -107,6 +107,7 @@ struct FusedArgs {
     double sin_a, cos_a;
     uint64_t seed, step;
     const double *axes;
+    unsigned *err;            // device error word
 };
 
 // rotation matrix of one cell in the working precision: the injected axis or
@@ -242,13 +243,20 @@ __device__ inline int stream_values(const FusedArgs<R> &A, R &x, R &y, R &z, R v
     return slot_of(A.g_next, (double)x, (double)y, (double)z);
 }
 
+// room for the 16-byte rounding of the tile's index window
+constexpr int kPermPad = 8;
+// polls of the index copy's mbarrier before the block gives up on it (far
+// above the microseconds one copy takes)
+constexpr int kBulkPolls = 1 << 16;
+
 // shared memory of a tile: velocity parts and source indices per particle,
 // the tile-local cell of each particle (one byte) and each cell's local start
 // and count
 template <typename R, typename S>
 constexpr size_t fused_smem()
 {
-    return (size_t)S::kCap * (Rec<R>::kVelBytes + sizeof(int) + 1) + 2 * (size_t)S::kSlots * sizeof(int);
+    return (size_t)S::kCap * (Rec<R>::kVelBytes + sizeof(int) + 1) + (size_t)kPermPad * sizeof(int) +
+           2 * (size_t)S::kSlots * sizeof(int);
 }
 
 // the non-velocity part of a record, as loaded from global memory
@@ -334,13 +342,15 @@ __global__ void __launch_bounds__(kFusedThreads, S::kMinBlocks) k_bulk_interval(
     static_assert(SL <= 256, "tile-local cell index kept in one byte");
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned char *s_vel = smem;
-    int *s_perm = (int *)(smem + (size_t)CAP * VB);
-    int *s_cstart = s_perm + CAP;                           // per cell of the tile
+    int *s_idx = (int *)(smem + (size_t)CAP * VB);          // the tile's index window
+    int *s_cstart = s_idx + CAP + kPermPad;                 // per cell of the tile
     int *s_ccount = s_cstart + SL;
     unsigned char *s_cell = (unsigned char *)(s_ccount + SL);  // per particle
 
+    __shared__ __align__(8) unsigned long long s_bar;
     const int t = threadIdx.x;
     const int lane = t & 31;
+    if (t == 0) mbar_init(&s_bar, 1);
     const int s0 = blockIdx.x * SL;
     const int slot = s0 + t;
     const int last = min(s0 + SL, A.S) - 1;
@@ -358,8 +368,24 @@ __global__ void __launch_bounds__(kFusedThreads, S::kMinBlocks) k_bulk_interval(
 
     if (np <= CAP) {
         // ---- staged path ----
+        // the tile's source indices perm[a0, a0 + np): one bulk copy of the
+        // enclosing 16-byte window (perm is allocated to a multiple of 4)
+        int *s_perm = s_idx;
         if (A.perm) {
-            for (int j = t; j < np; j += kFusedThreads) s_perm[j] = __ldcs(A.perm + a0 + j);
+            const int w0 = a0 & ~3;
+            const unsigned bytes = (unsigned)(((a0 - w0 + np + 3) & ~3) * sizeof(int));
+            s_perm = s_idx + (a0 - w0);
+            __syncthreads();  // the mbarrier's initialisation
+            if (t == 0 && bytes) {
+                mbar_arrive_expect_tx(&s_bar, bytes);
+                bulk_copy_to_smem(s_idx, A.perm + w0, bytes, &s_bar);
+            }
+            if (bytes && !mbar_wait_bounded(&s_bar, 0, kBulkPolls)) {
+                // not delivered in time: report it and load the same values
+                // directly (a late copy can only write them again)
+                atomicOr(A.err, DEV_ERR_BULK_WAIT);
+                for (int j = t; j < np; j += kFusedThreads) s_perm[j] = __ldcs(A.perm + a0 + j);
+            }
         } else {
             for (int j = t; j < np; j += kFusedThreads) s_perm[j] = a0 + j;
         }
@@ -708,6 +734,7 @@ static int bulk_run_fused(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r, doub
         A.seed = r->seed;
         A.step = step_c;
         A.axes = c->axes;
+        A.err = dev_error_word();
         {
             PhaseTimer t("interval_fused");
             shape.kernel<<<nblocks, kFusedThreads, shape.smem, st>>>(A);

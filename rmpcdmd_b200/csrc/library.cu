@@ -98,6 +98,8 @@ int check_dev_error(unsigned *bits_out)
             return fail(RMPCD_ERR_DEVICE, "rattle: negative discriminant or bead species outside the mass table");
         if (bits & DEV_ERR_QUAT_LOOP)
             return fail(RMPCD_ERR_DEVICE, "rigid_body_vv1: quaternion iteration did not converge");
+        if (bits & DEV_ERR_BULK_WAIT)
+            return fail(RMPCD_ERR_DEVICE, "bulk interval: an index bulk copy did not complete within its wait limit");
         return fail(RMPCD_ERR_DEVICE, "device error bits 0x%x", bits);
     }
     return RMPCD_OK;

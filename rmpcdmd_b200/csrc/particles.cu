@@ -362,7 +362,8 @@ int rmpcd_particles_init(rmpcd_particles **out, int Nmax, int n_species, const d
         ok = ok && cudaMalloc(&p->flags[b], ib) == cudaSuccess;
     }
     ok = ok && cudaMalloc(&p->key, ib) == cudaSuccess;
-    ok = ok && cudaMalloc(&p->perm, ib) == cudaSuccess;
+    // perm is read in 16-byte windows rounded outward (bulk copies)
+    ok = ok && cudaMalloc(&p->perm, ((n + 3) & ~(size_t)3) * sizeof(int)) == cudaSuccess;
     p->sums_cap = 8192;
     ok = ok && cudaMalloc(&p->d_max, 64) == cudaSuccess;
     ok = ok && cudaMalloc(&p->d_sums, (size_t)p->sums_cap * sizeof(double)) == cudaSuccess;

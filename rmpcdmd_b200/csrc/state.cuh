@@ -56,7 +56,7 @@ struct rmpcd_particles {
     int *flags[2] = {};
     // scratch
     int *key = nullptr;              // N, slot of each particle
-    int *perm = nullptr;             // N, source index of each sorted slot
+    int *perm = nullptr;             // N (allocated to a multiple of 4), source index of each sorted slot
     int *id_to_idx = nullptr;        // N, built on demand
     double *gauss = nullptr;         // injected normals (3*N) or null
     unsigned long long *d_max = nullptr;  // max-reduction word
