@@ -23,15 +23,32 @@ namespace rmpcd {
 
 constexpr int kNlThreads = kNlBlockThreads;
 
+// one block per colloid; the candidate cells of each stencil chunk are staged
+// in nl_stage_bytes<R>() of dynamic shared memory by bulk copies
 template <typename R>
-__global__ void k_update_list(Grid g, const double *cx, const double *cy, const double *cz, const int *cs,
-                              const R *sx, const R *sy, const R *sz, const int *sspec, const int *count,
-                              const int *start, const int *stencil, int n_stencil, double radiussq,
-                              LJDev lj, int do_lj, int Nmax, int *list, int *n_out, unsigned char *is_md,
-                              unsigned char *is_reac, unsigned *err)
+__global__ void __launch_bounds__(kNlThreads)
+    k_update_list(Grid g, const double *cx, const double *cy, const double *cz, const int *cs, const R *sx,
+                  const R *sy, const R *sz, const int *sspec, const int *count, const int *start,
+                  const int *stencil, int n_stencil, double radiussq, LJDev lj, int do_lj, int Nmax, int *list,
+                  int *n_out, unsigned char *is_md, unsigned char *is_reac, unsigned *err)
 {
+    extern __shared__ __align__(16) unsigned char nl_stage[];
+    __shared__ __align__(8) unsigned long long bar;
     update_list_block<R>(blockIdx.x, g, cx, cy, cz, cs, sx, sy, sz, sspec, count, start, stencil, n_stencil,
-                         radiussq, lj, do_lj, Nmax, list, n_out, is_md, is_reac, err);
+                         radiussq, lj, do_lj, Nmax, list, n_out, is_md, is_reac, err, NlStage{nl_stage, &bar});
+}
+
+template <typename R>
+static int update_list_smem(size_t *bytes)
+{
+    static bool set = false;
+    *bytes = nl_stage_bytes<R>();
+    if (!set) {
+        RMPCD_CUDA_TRY(cudaFuncSetAttribute(k_update_list<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)*bytes));
+        set = true;
+    }
+    return RMPCD_OK;
 }
 
 // PAST_MD <- MD, MD cleared, for every solvent particle (src/neighbor_list.f90:180-188)
@@ -375,16 +392,21 @@ int rmpcd_nlist_update(rmpcd_nlist *nl, rmpcd_particles *s1, rmpcd_particles *s2
     if (s1->N == 0) return RMPCD_OK;
     PView<double> cv = cur<double>(s1);
     LJDev ld = lj_dev(lj);
+    size_t smem = 0;
     if (s2->precision == RMPCD_FP32) {
+        int rc = update_list_smem<float>(&smem);
+        if (rc) return rc;
         PView<float> v = cur<float>(s2);
-        k_update_list<float><<<s1->N, kNlThreads, 0, s>>>(grid_of(c), cv.pos.x, cv.pos.y, cv.pos.z, cv.species,
+        k_update_list<float><<<s1->N, kNlThreads, smem, s>>>(grid_of(c), cv.pos.x, cv.pos.y, cv.pos.z, cv.species,
                                                           v.pos.x, v.pos.y, v.pos.z, v.species, c->count, c->start,
                                                           nl->stencil, nl->n_stencil, radius * radius, ld,
                                                           lj ? 1 : 0, nl->Nmax, nl->list, nl->n, c->is_md,
                                                           c->is_reac, dev_error_word());
     } else {
+        int rc = update_list_smem<double>(&smem);
+        if (rc) return rc;
         PView<double> v = cur<double>(s2);
-        k_update_list<double><<<s1->N, kNlThreads, 0, s>>>(grid_of(c), cv.pos.x, cv.pos.y, cv.pos.z, cv.species,
+        k_update_list<double><<<s1->N, kNlThreads, smem, s>>>(grid_of(c), cv.pos.x, cv.pos.y, cv.pos.z, cv.species,
                                                            v.pos.x, v.pos.y, v.pos.z, v.species, c->count, c->start,
                                                            nl->stencil, nl->n_stencil, radius * radius, ld,
                                                            lj ? 1 : 0, nl->Nmax, nl->list, nl->n, c->is_md,

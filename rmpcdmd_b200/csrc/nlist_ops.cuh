@@ -5,6 +5,7 @@
 
 #include <cstring>
 
+#include "async_copy.cuh"
 #include "keys.cuh"
 #include "rmpcd_common.cuh"
 #include "state.cuh"
@@ -60,21 +61,80 @@ __device__ inline int imod(int a, int p)
     return (r != 0 && ((r < 0) != (p < 0))) ? r + p : r;
 }
 
+// Staging of a chunk's candidate cells in shared memory by bulk copies: per
+// cell the 16-byte window (4 elements) around its particle range of x, y, z
+// and species.  kNlStageCap elements per array; a chunk with more stays on
+// direct loads.
+constexpr int kNlStageCap = 4096;
+constexpr int kNlStagePolls = 1 << 16;
+
+template <typename R>
+constexpr size_t nl_stage_bytes()
+{
+    return (size_t)kNlStageCap * (3 * sizeof(R) + sizeof(int));
+}
+
+struct NlStage {
+    unsigned char *buf;       // nl_stage_bytes<R>() of dynamic shared memory; null = direct loads
+    unsigned long long *bar;  // mbarrier in shared memory
+};
+
+// exclusive scan of one int per thread over a block of kNlBlockThreads;
+// *total gets the sum (shared, read after the call)
+__device__ inline int nl_block_excl_scan(int v, int *warp_sum, int *total)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int inc = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        int w = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += w;
+    }
+    if (lane == 31) warp_sum[wid] = inc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int w = 0; w < kNlBlockThreads / 32; w++) {
+            int x = warp_sum[w];
+            warp_sum[w] = acc;
+            acc += x;
+        }
+        *total = acc;
+    }
+    __syncthreads();
+    int r = warp_sum[wid] + inc - v;
+    __syncthreads();
+    return r;
+}
+
 // update_list, src/neighbor_list.f90:76-157: one block per colloid; stencil
 // cells are processed in chunks of kNlBlockThreads, their particles enumerated in
-// stencil order and compacted in order with a block scan.
+// stencil order and compacted in order with a block scan.  With a stage,
+// each chunk's cells are first brought into shared memory by bulk copies.
 template <typename R>
 __device__ inline void update_list_block(int i, const Grid &g, const double *cx, const double *cy, const double *cz,
                                          const int *cs, const R *sx, const R *sy, const R *sz, const int *sspec,
                                          const int *count, const int *start, const int *stencil, int n_stencil,
                                          double radiussq, const LJDev &lj, int do_lj, int Nmax, int *list,
-                                         int *n_out, unsigned char *is_md, unsigned char *is_reac, unsigned *err)
+                                         int *n_out, unsigned char *is_md, unsigned char *is_reac, unsigned *err,
+                                         NlStage stage = {nullptr, nullptr})
 {
     __shared__ int c_slot[kNlBlockThreads], c_start[kNlBlockThreads], c_off[kNlBlockThreads + 1];
-    __shared__ int c_md[kNlBlockThreads], c_noreac[kNlBlockThreads];
+    __shared__ int c_md[kNlBlockThreads], c_noreac[kNlBlockThreads], c_shift[kNlBlockThreads];
     __shared__ int warp_sum[kNlBlockThreads / 32];
-    __shared__ int s_total, s_base;
+    __shared__ int s_total, s_base, s_wtotal;
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    R *st_x = nullptr, *st_y = nullptr, *st_z = nullptr;
+    int *st_s = nullptr;
+    bool use_stage = stage.buf != nullptr;
+    unsigned phase = 0;
+    bool pending = false;  // a copy phase that was given up on
+    if (use_stage) {
+        st_x = (R *)stage.buf;
+        st_y = st_x + kNlStageCap;
+        st_z = st_y + kNlStageCap;
+        st_s = (int *)(st_z + kNlStageCap);
+        if (t == 0) mbar_init(stage.bar, 1);
+    }
     double x0 = cx[i], x1 = cy[i], x2 = cz[i];
     int si = cs[i];
     int cell[3];
@@ -117,6 +177,37 @@ __device__ inline void update_list_block(int i, const Grid &g, const double *cx,
         if (t == 0) c_off[kNlBlockThreads] = s_total;
         __syncthreads();
         const int total = c_off[kNlBlockThreads];
+        bool staged = false;
+        if (use_stage) {
+            // window of this thread's cell: [w0, w0 + wl), w0 and wl multiples of 4
+            int w0 = 0, wl = 0;
+            if (cnt > 0) {
+                w0 = c_start[t] & ~3;
+                wl = (c_start[t] - w0 + cnt + 3) & ~3;
+            }
+            const int woff = nl_block_excl_scan(wl, warp_sum, &s_wtotal);
+            const int wtot = s_wtotal;
+            if (wtot > 0 && wtot <= kNlStageCap) {
+                if (t == 0) mbar_arrive_expect_tx(stage.bar, (unsigned)(wtot * (3 * sizeof(R) + sizeof(int))));
+                if (wl > 0) {
+                    bulk_copy_to_smem(st_x + woff, sx + w0, (unsigned)(wl * sizeof(R)), stage.bar);
+                    bulk_copy_to_smem(st_y + woff, sy + w0, (unsigned)(wl * sizeof(R)), stage.bar);
+                    bulk_copy_to_smem(st_z + woff, sz + w0, (unsigned)(wl * sizeof(R)), stage.bar);
+                    bulk_copy_to_smem(st_s + woff, sspec + w0, (unsigned)(wl * sizeof(int)), stage.bar);
+                }
+                c_shift[t] = woff - w0;
+                const bool ok = mbar_wait_bounded(stage.bar, phase, kNlStagePolls);
+                phase ^= 1u;
+                if (__syncthreads_or(!ok)) {
+                    // not delivered in time: report it and keep to direct loads
+                    if (t == 0) atomicOr(err, DEV_ERR_BULK_WAIT);
+                    use_stage = false;
+                    pending = true;
+                } else {
+                    staged = true;
+                }
+            }
+        }
         for (int k0 = 0; k0 < total; k0 += kNlBlockThreads) {
             int k = k0 + t;
             int accept = 0;
@@ -131,11 +222,15 @@ __device__ inline void update_list_block(int i, const Grid &g, const double *cx,
                 }
                 const int cl = lo;
                 idx = c_start[cl] + (k - c_off[cl]);
-                int s = sspec[idx];
+                const int q = staged ? idx + c_shift[cl] : 0;
+                int s = staged ? st_s[q] : sspec[idx];
                 if (s > 0) {
-                    double r0 = min_image_d(x0 - (double)sx[idx], L0);
-                    double r1 = min_image_d(x1 - (double)sy[idx], L1);
-                    double r2 = min_image_d(x2 - (double)sz[idx], L2);
+                    const R px = staged ? st_x[q] : sx[idx];
+                    const R py = staged ? st_y[q] : sy[idx];
+                    const R pz = staged ? st_z[q] : sz[idx];
+                    double r0 = min_image_d(x0 - (double)px, L0);
+                    double r1 = min_image_d(x1 - (double)py, L1);
+                    double r2 = min_image_d(x2 - (double)pz, L2);
                     double rsq = r0 * r0 + r1 * r1 + r2 * r2;
                     if (rsq < radiussq) {
                         accept = 1;
@@ -175,6 +270,8 @@ __device__ inline void update_list_block(int i, const Grid &g, const double *cx,
         __syncthreads();
     }
     if (t == 0) n_out[i] = s_base < Nmax ? s_base : Nmax;
+    // copies of a phase given up on land before the block's shared memory goes
+    if (pending) mbar_wait_bounded(stage.bar, phase ^ 1u, kNlStagePolls);
 }
 
 

@@ -345,7 +345,9 @@ int rmpcd_particles_init(rmpcd_particles **out, int Nmax, int n_species, const d
     p->rsize = precision == RMPCD_FP32 ? 4 : 8;
     if (mass)
         for (int s = 0; s < n_species; s++) p->mass[s] = mass[s];
-    size_t n = (size_t)(Nmax > 0 ? Nmax : 1);
+    // every array is allocated to a multiple of 4 elements: bulk copies read
+    // 16-byte windows rounded outward
+    size_t n = ((size_t)(Nmax > 0 ? Nmax : 1) + 3) & ~(size_t)3;
     size_t rb = n * p->rsize, ib = n * sizeof(int);
     bool ok = true;
     cudaStream_t st = stream();
@@ -362,8 +364,7 @@ int rmpcd_particles_init(rmpcd_particles **out, int Nmax, int n_species, const d
         ok = ok && cudaMalloc(&p->flags[b], ib) == cudaSuccess;
     }
     ok = ok && cudaMalloc(&p->key, ib) == cudaSuccess;
-    // perm is read in 16-byte windows rounded outward (bulk copies)
-    ok = ok && cudaMalloc(&p->perm, ((n + 3) & ~(size_t)3) * sizeof(int)) == cudaSuccess;
+    ok = ok && cudaMalloc(&p->perm, ib) == cudaSuccess;
     p->sums_cap = 8192;
     ok = ok && cudaMalloc(&p->d_max, 64) == cudaSuccess;
     ok = ok && cudaMalloc(&p->d_sums, (size_t)p->sums_cap * sizeof(double)) == cudaSuccess;

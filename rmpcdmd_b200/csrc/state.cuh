@@ -38,6 +38,9 @@ struct rmpcd_cells {
     int red_cap = 0;
 };
 
+// The per-particle arrays made at init (pos ... flags, key, perm) are
+// allocated to a multiple of 4 elements: bulk copies read 16-byte windows
+// rounded outward.
 struct rmpcd_particles {
     int N = 0;
     int n_species = 1;
@@ -56,7 +59,7 @@ struct rmpcd_particles {
     int *flags[2] = {};
     // scratch
     int *key = nullptr;              // N, slot of each particle
-    int *perm = nullptr;             // N (allocated to a multiple of 4), source index of each sorted slot
+    int *perm = nullptr;             // N, source index of each sorted slot
     int *id_to_idx = nullptr;        // N, built on demand
     double *gauss = nullptr;         // injected normals (3*N) or null
     unsigned long long *d_max = nullptr;  // max-reduction word

@@ -115,6 +115,42 @@ def test_neighbor_list_many_colloids_small_box(rm, oracle):
         assert_same(gcol, ocol, ("force",))
 
 
+@pytest.mark.parametrize("rho", [10, 40])
+def test_update_list_fp32_solvent(rm, oracle, rho):
+    # the FP32 solvent form of update_list: the oracle gets the same float
+    # positions; at density 40 every full stencil chunk holds more candidates
+    # than the shared-memory stage and reads them directly, at 10 they are
+    # staged by bulk copies
+    L = np.array([24, 20, 22])
+    N = int(L.prod()) * rho
+    (oc, op), (gc, gp) = make_pair(rm, oracle, L, N, seed=7, precision=32, origin=[-0.5, -0.25, -0.75],
+                                   sorted_=False)
+    op.pos[:] = gp.download("pos")
+    op.vel[:] = gp.download("vel")
+    op.sort(oc)
+    gp.sort(gc)
+    C, cutoff = 12, 4.0
+    r = np.random.default_rng(8)
+    ocol = oracle.Particles(C, 1, [100.0])
+    gcol = rm.ParticleSystem(C, 1, [100.0])
+    ocol.species[:] = 1
+    ocol.pos[:] = r.random((C, 3)) * L
+    upload(gcol, ocol, ("pos", "species"))
+    nmax = rho * 6 * int(cutoff ** 3) * 2
+    onl = oracle.NeighborList(C, nmax)
+    gnl = rm.NeighborList(C, nmax)
+    onl.make_stencil(oc, cutoff)
+    gnl.make_stencil(gc, cutoff)
+    onl.update_list(ocol, op, cutoff, oc)
+    gnl.update_list(gcol, gp, cutoff, gc)
+    lst, n = gnl.download()
+    assert np.array_equal(n, onl.n) and n.min() > 0
+    for i in range(C):
+        assert np.array_equal(lst[i, :n[i]], onl.list[i, :n[i]])
+    assert np.array_equal(gc.is_md, oc.is_md.astype(bool))
+    rm.get_status()
+
+
 @pytest.mark.parametrize("C,box", [(200, 20.0), (300, 70.0), (20, 30.0)])
 def test_compute_force_n2(rm, oracle, C, box):
     # box 20: every pair inside the cut; box 70: most pairs beyond it; C = 20:
