@@ -373,6 +373,18 @@ def e2e_run(rm, p, cells, rng, steps):
     return N * steps / dt_s, nbytes_step, nbytes_step
 
 
+def cpu_model():
+    """The host CPU's model name (Linux /proc/cpuinfo), or None."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def cpu_sample(L_sample=64, min_seconds=10.0, max_intervals=20, threads=None):
     """The oracle's OpenMP bulk interval on a 64^3 box at the same density."""
     from oracle import oracle as O
@@ -395,7 +407,8 @@ def cpu_sample(L_sample=64, min_seconds=10.0, max_intervals=20, threads=None):
         O.bulk_run(p, c, 1, TAU, SEED, 3 + 2 * n)
         n += 1
     dt = time.perf_counter() - t0
-    return {"value": N * n / dt, "unit": "particle-steps/s", "cores": nt, "kind": "port",
+    return {"value": N * n / dt, "unit": "particle-steps/s", "cores": nt, "kind": "port", "cpu": cpu_model(),
+            "host_threads": os.cpu_count(),
             "sample": f"{n} bulk intervals of the FP64 oracle (C, OpenMP) on {L_sample}^3 cells x rho {RHO} "
                       f"= {N} particles ({n * N} particle-steps, {dt:.1f} s)"}
 
@@ -563,7 +576,8 @@ def run_reference(args):
            "dtype": "f64", "data": "synthetic (seeded uniform positions, Gaussian velocities kT=1/3)",
            "config": {"workload": f"bulk SRD fluid {Ls}^3-cell sample of the {L_DEFAULT}^3 box, rho={RHO}",
                       "cells": [Ls] * 3, "particles": N},
-           "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": nt, "kind": "port", "sample": sample},
+           "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": nt, "kind": "port", "sample": sample,
+                            "cpu": cpu_model(), "host_threads": os.cpu_count()},
            "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
            "note": "the reference (Fortran 2008 + OpenMP) cannot be built here: no Fortran compiler and empty "
                    "dependency submodules; this arm times the C restatement of its loop"}
