@@ -97,3 +97,17 @@ def test_count_particles(rm, oracle):
     op.count(oc)
     gc.count_particles(gp)
     assert_cells_same(gc, oc)
+
+
+@pytest.mark.parametrize("L,N", [([1, 1, 1], 7), ([3, 1, 2], 50), ([256, 128, 128], 30000)])
+def test_count_particles_slot_scan_extremes(rm, oracle, L, N):
+    # a single slot (one partial scan tile), a few slots, and 2^23 slots
+    # (2048 scan tiles: each block adds more than one round of earlier
+    # tile totals); counted twice so the second scan starts from the first's
+    # state
+    (oc, op), (gc, gp) = make_pair(rm, oracle, L, N, seed=N, sorted_=False, origin=[-0.5, -0.5, -0.5])
+    for _ in range(2):
+        op.count(oc)
+        gc.count_particles(gp)
+        assert_cells_same(gc, oc)
+    assert int(gc.cell_count.sum()) == N
