@@ -626,7 +626,8 @@ struct Shapes<double> {
                                                    entry<double, Shape<112, 1600, 3>>(),
                                                    entry<double, Shape<128, 1792, 3>>(),
                                                    entry<double, Shape<160, 2176, 2>>(),
-                                                   entry<double, Shape<192, 2560, 2>>()};
+                                                   entry<double, Shape<192, 2560, 2>>(),
+                                                   entry<double, Shape<96, 1408, 3>>()};
 };
 template <typename R>
 constexpr int n_shapes()
