@@ -62,9 +62,10 @@ __device__ inline int imod(int a, int p)
 }
 
 // Staging of a chunk's candidate cells in shared memory by bulk copies: per
-// cell the 16-byte window (4 elements) around its particle range of x, y, z
-// and species.  kNlStageCap elements per array; a chunk with more stays on
-// direct loads.
+// cell its particle range of x, y, z and species, rounded outward to
+// multiples of 4 elements so that every copy starts and ends on a 16-byte
+// boundary (the particle arrays are allocated to a multiple of 4 elements).
+// kNlStageCap elements per array; a chunk with more stays on direct loads.
 constexpr int kNlStageCap = 4096;
 constexpr int kNlStagePolls = 1 << 16;
 
