@@ -382,7 +382,9 @@ __global__ void __launch_bounds__(kFusedThreads, S::kMinBlocks) k_bulk_interval(
             }
             if (bytes && !mbar_wait_bounded(&s_bar, 0, kBulkPolls)) {
                 // not delivered in time: report it and load the same values
-                // directly (a late copy can only write them again)
+                // directly (a late copy can only write this tile's indices
+                // again, at worst undoing their in-cell order, which the
+                // error bit already flags; never an index outside the tile)
                 atomicOr(A.err, DEV_ERR_BULK_WAIT);
                 for (int j = t; j < np; j += kFusedThreads) s_perm[j] = __ldcs(A.perm + a0 + j);
             }
