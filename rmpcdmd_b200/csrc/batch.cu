@@ -748,19 +748,38 @@ __global__ void __launch_bounds__(kBT) kb_copyback(TileSet ts, PView<R> d, PView
     }
 }
 
-// update_list (src/neighbor_list.f90:76-157), one block per colloid
+// update_list (src/neighbor_list.f90:76-157), one block per colloid; the
+// candidate cells of each stencil chunk are staged in nl_stage_bytes<R>() of
+// dynamic shared memory by bulk copies (a window may reach into a
+// neighbouring replica's particles, which are read and not used)
 template <typename R>
 __global__ void __launch_bounds__(kNlBlockThreads)
     kb_update_list(const int *flag, const BRep *rep, PView<double> c, PView<R> s, const int *count, const int *start,
                    const int *stencil, int n_stencil, double radiussq, LJDev lj, int Nmax, int *list, int *n,
                    unsigned char *is_md, unsigned char *is_reac, unsigned *err)
 {
+    extern __shared__ __align__(16) unsigned char nl_stage[];
+    __shared__ __align__(8) unsigned long long bar;
     const int i = blockIdx.x, r = i >> 1;
     if (flag && !flag[r]) return;
     const BRep &rp = rep[r];
     update_list_block<R>(i, rp.g, c.pos.x, c.pos.y, c.pos.z, c.species, s.pos.x, s.pos.y, s.pos.z, s.species,
                          count + rp.soff, start + rp.soff, stencil, n_stencil, radiussq, lj, 1, Nmax, list, n,
-                         is_md + rp.soff, is_reac + rp.soff, err);
+                         is_md + rp.soff, is_reac + rp.soff, err, NlStage{nl_stage, &bar});
+}
+
+// the list kernel's dynamic shared memory above the default limit, set once
+// per precision (at batch creation, before any stream capture)
+template <typename R>
+static int allow_list_stage()
+{
+    static bool set = false;
+    if (!set) {
+        RMPCD_CUDA_TRY(cudaFuncSetAttribute(kb_update_list<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)nl_stage_bytes<R>()));
+        set = true;
+    }
+    return RMPCD_OK;
 }
 
 // ------------------------------------------------------------ interval
@@ -852,7 +871,7 @@ static void resort_launches(Batch *b, const int *flag, bool all, cudaStream_t st
     launch_segsort_big(b->start, b->count, b->big, b->n_big, b->sol->perm, b->sol->key, st);
     kb_gather<R><<<gp, kBT, 0, st>>>(pts, cur, alt, b->sol->perm);
     kb_copyback<R><<<gp, kBT, 0, st>>>(pts, cur, alt);
-    kb_update_list<R><<<2 * b->R, kNlBlockThreads, 0, st>>>(
+    kb_update_list<R><<<2 * b->R, kNlBlockThreads, nl_stage_bytes<R>(), st>>>(
         flag, b->rep, cv, cur, b->count, b->start, b->stencil, b->n_stencil, b->prm.list_radius * b->prm.list_radius,
         b->lj_sc, b->Nmax, b->list, b->nn, b->is_md, b->is_reac, dev_error_word());
 }
@@ -1179,6 +1198,10 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
     }
     if (rmpcd_particles_init(&b->sol, (int)off, sol[0]->n_species, sol[0]->mass, b->precision) ||
         rmpcd_particles_init(&b->col, 2 * R, col[0]->n_species, col[0]->mass, RMPCD_FP64)) {
+        free_batch(b);
+        return RMPCD_ERR_CUDA;
+    }
+    if ((b->precision == RMPCD_FP32 ? allow_list_stage<float>() : allow_list_stage<double>()) != RMPCD_OK) {
         free_batch(b);
         return RMPCD_ERR_CUDA;
     }
