@@ -431,7 +431,9 @@ __device__ inline void apply_multi_block(const int *list, const int *n, int C, i
 // contributing entries are compacted in order into clist (one block).  Each
 // chunk of entries is compacted and staged in shared memory by the whole
 // block; the three components are then summed by three threads, each in
-// list order, so every sum is the sequential one.
+// list order, so every sum is the sequential one.  Every thread loads its
+// entry of the next chunk before the sums of the current one, so those loads
+// are in flight while the three threads add.
 __device__ inline void colloid_sum_block(int i, const int *n, int Nmax, const unsigned char *contrib, const double *pf,
                                          double *cfx, double *cfy, double *cfz, int *clist, int *cn)
 {
@@ -443,9 +445,20 @@ __device__ inline void colloid_sum_block(int i, const int *n, int Nmax, const un
     const int ni = n[i];
     double acc = 0;  // thread c < 3 accumulates component c
     int total = 0;
+    // this thread's entry of the current chunk: contribution flag and force
+    int c = 0;
+    double f0 = 0, f1 = 0, f2 = 0;
+    if (t < ni) {
+        const size_t q = (size_t)i * Nmax + t;
+        c = contrib[q];
+        if (c) {
+            f0 = pf[3 * q];
+            f1 = pf[3 * q + 1];
+            f2 = pf[3 * q + 2];
+        }
+    }
     for (int e0 = 0; e0 < ni; e0 += kNlBlockThreads) {
-        int e = e0 + t;
-        int c = (e < ni) ? contrib[(size_t)i * Nmax + e] : 0;
+        const int e = e0 + t;
         unsigned bal = __ballot_sync(0xffffffffu, c);
         if (lane == 0) warp_cnt[wid] = __popc(bal);
         __syncthreads();
@@ -461,14 +474,24 @@ __device__ inline void colloid_sum_block(int i, const int *n, int Nmax, const un
         __syncthreads();
         if (c) {
             const int k = warp_cnt[wid] + __popc(bal & ((1u << lane) - 1u));
-            const size_t q = (size_t)i * Nmax + e;
             idxs[k] = e;
-            vals[0][k] = pf[3 * q];
-            vals[1][k] = pf[3 * q + 1];
-            vals[2][k] = pf[3 * q + 2];
+            vals[0][k] = f0;
+            vals[1][k] = f1;
+            vals[2][k] = f2;
         }
         __syncthreads();
         const int cnt = s_cnt;
+        // the next chunk's entry
+        c = 0;
+        if (e + kNlBlockThreads < ni) {
+            const size_t q = (size_t)i * Nmax + e + kNlBlockThreads;
+            c = contrib[q];
+            if (c) {
+                f0 = pf[3 * q];
+                f1 = pf[3 * q + 1];
+                f2 = pf[3 * q + 2];
+            }
+        }
         if (t < 3) {
 #pragma unroll 8
             for (int k = 0; k < cnt; k++) acc = acc + vals[t][k];
