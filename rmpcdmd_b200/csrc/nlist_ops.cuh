@@ -428,75 +428,73 @@ __device__ inline void apply_multi_block(const int *list, const int *n, int C, i
 }
 
 // f1 = sum of colloid i's pair forces in list order; force(:,i) += f1; the
-// contributing entries are compacted in order into clist (one block).  Each
-// chunk of entries is compacted and staged in shared memory by the whole
-// block; the three components are then summed by three threads, each in
-// list order, so every sum is the sequential one.  Every thread loads its
-// entry of the next chunk before the sums of the current one, so those loads
-// are in flight while the three threads add.
+// contributing entries are compacted in order into clist (one block).  The
+// list is walked in chunks of kCollSumPer entries per thread, each thread owning
+// a contiguous run of its chunk: the chunk's contributing entries are
+// compacted in order and staged in shared memory by the whole block, then
+// the three components are summed by three threads, each in list order, so
+// every sum is the sequential one.  Every thread loads its run of the next
+// chunk before the current chunk is summed, so those loads are in flight
+// while the three threads add.
+constexpr int kCollSumPer = 4;
+constexpr int kCollSumChunk = kCollSumPer * kNlBlockThreads;
+
+__device__ inline void colloid_sum_load(int i, int e_first, int ni, int Nmax, const unsigned char *contrib,
+                                        const double *pf, unsigned &cmask, double (&f)[kCollSumPer][3])
+{
+    cmask = 0u;
+#pragma unroll
+    for (int m = 0; m < kCollSumPer; m++) {
+        const int e = e_first + m;
+        if (e < ni) {
+            const size_t q = (size_t)i * Nmax + e;
+            if (contrib[q]) {
+                cmask |= 1u << m;
+                f[m][0] = pf[3 * q];
+                f[m][1] = pf[3 * q + 1];
+                f[m][2] = pf[3 * q + 2];
+            }
+        }
+    }
+}
+
 __device__ inline void colloid_sum_block(int i, const int *n, int Nmax, const unsigned char *contrib, const double *pf,
                                          double *cfx, double *cfy, double *cfz, int *clist, int *cn)
 {
-    __shared__ int idxs[kNlBlockThreads];
-    __shared__ double vals[3][kNlBlockThreads];
-    __shared__ int warp_cnt[kNlBlockThreads / 32];
+    __shared__ int idxs[kCollSumChunk];
+    __shared__ double vals[3][kCollSumChunk];
+    __shared__ int warp_sum[kNlBlockThreads / 32];
     __shared__ int s_cnt;
-    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    const int t = threadIdx.x;
     const int ni = n[i];
     double acc = 0;  // thread c < 3 accumulates component c
     int total = 0;
-    // this thread's entry of the current chunk: contribution flag and force
-    int c = 0;
-    double f0 = 0, f1 = 0, f2 = 0;
-    if (t < ni) {
-        const size_t q = (size_t)i * Nmax + t;
-        c = contrib[q];
-        if (c) {
-            f0 = pf[3 * q];
-            f1 = pf[3 * q + 1];
-            f2 = pf[3 * q + 2];
-        }
-    }
-    for (int e0 = 0; e0 < ni; e0 += kNlBlockThreads) {
-        const int e = e0 + t;
-        unsigned bal = __ballot_sync(0xffffffffu, c);
-        if (lane == 0) warp_cnt[wid] = __popc(bal);
-        __syncthreads();
-        if (t == 0) {
-            int a = 0;
-            for (int w = 0; w < kNlBlockThreads / 32; w++) {
-                int v = warp_cnt[w];
-                warp_cnt[w] = a;
-                a += v;
+    // this thread's run of the current chunk: contributing entries and forces
+    unsigned cmask;
+    double f[kCollSumPer][3];
+    colloid_sum_load(i, kCollSumPer * t, ni, Nmax, contrib, pf, cmask, f);
+    for (int e0 = 0; e0 < ni; e0 += kCollSumChunk) {
+        const int e_first = e0 + kCollSumPer * t;
+        int k = nl_block_excl_scan(__popc(cmask), warp_sum, &s_cnt);
+#pragma unroll
+        for (int m = 0; m < kCollSumPer; m++) {
+            if ((cmask >> m) & 1u) {
+                idxs[k] = e_first + m;
+                vals[0][k] = f[m][0];
+                vals[1][k] = f[m][1];
+                vals[2][k] = f[m][2];
+                k++;
             }
-            s_cnt = a;
-        }
-        __syncthreads();
-        if (c) {
-            const int k = warp_cnt[wid] + __popc(bal & ((1u << lane) - 1u));
-            idxs[k] = e;
-            vals[0][k] = f0;
-            vals[1][k] = f1;
-            vals[2][k] = f2;
         }
         __syncthreads();
         const int cnt = s_cnt;
-        // the next chunk's entry
-        c = 0;
-        if (e + kNlBlockThreads < ni) {
-            const size_t q = (size_t)i * Nmax + e + kNlBlockThreads;
-            c = contrib[q];
-            if (c) {
-                f0 = pf[3 * q];
-                f1 = pf[3 * q + 1];
-                f2 = pf[3 * q + 2];
-            }
-        }
+        // the next chunk's run
+        colloid_sum_load(i, e_first + kCollSumChunk, ni, Nmax, contrib, pf, cmask, f);
         if (t < 3) {
 #pragma unroll 8
-            for (int k = 0; k < cnt; k++) acc = acc + vals[t][k];
+            for (int q = 0; q < cnt; q++) acc = acc + vals[t][q];
         }
-        for (int k = t; k < cnt; k += kNlBlockThreads) clist[(size_t)i * Nmax + total + k] = idxs[k];
+        for (int q = t; q < cnt; q += kNlBlockThreads) clist[(size_t)i * Nmax + total + q] = idxs[q];
         total += cnt;
         __syncthreads();
     }
