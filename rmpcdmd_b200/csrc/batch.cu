@@ -92,6 +92,7 @@ struct rmpcd_dimer_batch {
     unsigned char *contrib = nullptr;
     int *ncontrib = nullptr, *max_contrib = nullptr, *clist = nullptr, *cn = nullptr;
     unsigned long long *so_max = nullptr;
+    double *co_max = nullptr;  // per replica: the colloids' displacement of this MD step
     int *resort = nullptr, *n_extra = nullptr, *big = nullptr, *n_big = nullptr;
     double *rattle[3] = {nullptr, nullptr, nullptr};
     double *vv_mass = nullptr;
@@ -173,13 +174,13 @@ __device__ inline R flagged(const R *a, long long i, bool set)
     return set ? a[i] : (R)0;
 }
 
-// colloid position half, RATTLE, colloid displacement and the re-sort
-// decision of replica r (programs/single_dimer_pbc.f90:311-330); clears the
-// colloid force entries that become `force` after switch_force
-__device__ inline int colloid_begin(int r, const BRep *rep, const PView<double> &c, const Vec3<double> &cold,
-                                    const Vec3<double> &c_next, double *const rat[3], const double *mass,
-                                    const Masses &ms, double d, double dt, double skin, unsigned long long *so_max,
-                                    int *resort, int *n_extra, unsigned *err)
+// colloid position half, RATTLE and colloid displacement of replica r
+// (programs/single_dimer_pbc.f90:311-322); clears the colloid force entries
+// that become `force` after switch_force; returns the displacement.  Touches
+// no solvent data.
+__device__ inline double colloid_begin(int r, const BRep *rep, const PView<double> &c, const Vec3<double> &cold,
+                                       const Vec3<double> &c_next, double *const rat[3], const double *mass,
+                                       const Masses &ms, double d, double dt, unsigned *err)
 {
     PView<double> cr = shifted(c, 2 * (long long)r, 2);
     for (int k = 0; k < 2; k++) {
@@ -193,13 +194,21 @@ __device__ inline int colloid_begin(int r, const BRep *rep, const PView<double> 
     rattle_pos_dimer(cr, rat[0] + 2 * r, rat[1] + 2 * r, rat[2] + 2 * r, ms, d, dt, L, err);
     Vec3<double> o = {cold.x + 2 * r, cold.y + 2 * r, cold.z + 2 * r};
     double m0 = disp_sq_one(cr.pos, o, cr.species, 0), m1 = disp_sq_one(cr.pos, o, cr.species, 1);
-    double co_max = sqrt(m0 > m1 ? m0 : m1);
+    for (int k = 2 * r; k < 2 * r + 2; k++) c_next.x[k] = c_next.y[k] = c_next.z[k] = 0;
+    return sqrt(m0 > m1 ? m0 : m1);
+}
+
+// the re-sort decision of replica r (programs/single_dimer_pbc.f90:323-330),
+// given its colloid displacement co, once the solvent's maximum displacement
+// of the step is complete
+__device__ inline int resort_decision(int r, double skin, double co, unsigned long long *so_max, int *resort,
+                                      int *n_extra)
+{
     double so = sqrt(__longlong_as_double((long long)__ldcg(so_max + r)));
-    int need = (co_max >= skin * 0.1) || (so >= skin * 0.89);
+    int need = (co >= skin * 0.1) || (so >= skin * 0.89);
     resort[r] = need;
     if (need) n_extra[r] += 1;
     so_max[r] = 0;
-    for (int k = 2 * r; k < 2 * r + 2; k++) c_next.x[k] = c_next.y[k] = c_next.z[k] = 0;
     return need;
 }
 
@@ -212,6 +221,7 @@ struct ColloidStep {
     Masses ms;
     double d, dt, skin;
     int R;
+    double *co_max;        // per replica: the colloids' displacement of this step
 };
 
 // exclusive block scan of one int per thread; *total gets the block's sum
@@ -252,10 +262,20 @@ struct ResortLists {
 // md_pos of every solvent particle, the PAST_MD/MD roll of compute_force,
 // clearing of the entries that become `force` after switch_force and the
 // solvent's maximum displacement (src/md.f90:61-77,
-// src/neighbor_list.f90:180-188, src/particle_system.f90:357-378); the last
-// block to finish runs the colloid half for every replica, the program's
-// re-sort test, lists the tiles of the replicas to re-sort and raises the
-// graph's re-sort condition when there are any
+// src/neighbor_list.f90:180-188, src/particle_system.f90:357-378), one block
+// per particle tile; the last block to finish takes the program's re-sort
+// decision, lists the tiles of the replicas to re-sort and raises the graph's
+// re-sort condition when there are any.  The colloid half of every replica
+// runs in that last block in the FP32 form; in the FP64 form an extra block 0
+// runs it while the solvent streams (its registers would make the FP32
+// streaming path spill, which costs the large FP32 batches more than the
+// overlap gains).
+template <typename R>
+constexpr bool colloid_block_first()
+{
+    return sizeof(R) == 8;
+}
+
 template <typename R>
 __global__ void __launch_bounds__(kBT, 4)
     kb_step_begin(const BTile *tiles, const BRep *rep, PView<R> v, Vec3<R> old, Vec3<R> next, R dt, R dt_sq,
@@ -265,7 +285,12 @@ __global__ void __launch_bounds__(kBT, 4)
     __shared__ int s_last;
     __shared__ int ws[kBT / 32 + 1];
     __shared__ double s_max[kBT / 32];
-    const BTile t = tiles[blockIdx.x];
+    constexpr bool kFirst = colloid_block_first<R>();
+    const bool colloid_block = kFirst && blockIdx.x == 0;
+    const BTile t = colloid_block ? BTile{0, 0, 0, 0} : tiles[blockIdx.x - (kFirst ? 1 : 0)];
+    if (colloid_block)
+        for (int r = threadIdx.x; r < cs.R; r += blockDim.x)
+            cs.co_max[r] = colloid_begin(r, rep, cs.c, cs.cold, cs.c_next, cs.rat, cs.mass, cs.ms, cs.d, cs.dt, err);
     double m = 0;
     // K particles per thread and pass, all loads issued before any use
     constexpr int K = sizeof(R) == 4 ? 4 : 2;
@@ -317,7 +342,8 @@ __global__ void __launch_bounds__(kBT, 4)
     if (threadIdx.x == 0) {
         for (int w = 1; w < kBT / 32; w++) m = m > s_max[w] ? m : s_max[w];
         // one atomic per block, skipped when it cannot raise the maximum
-        if (m > __longlong_as_double((long long)__ldcg(so_max + t.r))) atomic_max_nonneg(so_max + t.r, m);
+        if (!colloid_block && m > __longlong_as_double((long long)__ldcg(so_max + t.r)))
+            atomic_max_nonneg(so_max + t.r, m);
         __threadfence();
         s_last = atomicAdd(done, 1u) == gridDim.x - 1;
     }
@@ -328,9 +354,12 @@ __global__ void __launch_bounds__(kBT, 4)
     for (int r0 = 0; r0 < cs.R; r0 += blockDim.x) {
         const int r = r0 + threadIdx.x;
         int need = 0;
-        if (r < cs.R)
-            need = colloid_begin(r, rep, cs.c, cs.cold, cs.c_next, cs.rat, cs.mass, cs.ms, cs.d, cs.dt, cs.skin, so_max,
-                                 resort, n_extra, err);
+        if (r < cs.R) {
+            const double co = kFirst ? __ldcg(cs.co_max + r)
+                                     : colloid_begin(r, rep, cs.c, cs.cold, cs.c_next, cs.rat, cs.mass, cs.ms, cs.d,
+                                                     cs.dt, err);
+            need = resort_decision(r, cs.skin, co, so_max, resort, n_extra);
+        }
         any |= need;
         const int np = need ? rl.pcount[r] : 0, ns = need ? rl.scount[r] : 0;
         int tp, ts;
@@ -918,7 +947,7 @@ static void md_step_launches(Batch *b, int k)
     PView<R> alt = phys<R>(b->sol, 1);
     PView<double> ca = phys<double>(b->col, 1);
     ColloidStep cs{c, ca.pos, c.force_old, {b->rattle[0], b->rattle[1], b->rattle[2]}, b->vv_mass, b->ms,
-                   b->prm.bond, dt, b->prm.skin, b->R};
+                   b->prm.bond, dt, b->prm.skin, b->R, b->co_max};
     cudaGraphConditionalHandle cond = 0;
     cudaGraph_t g = nullptr;
     if (b->capturing) {
@@ -926,7 +955,7 @@ static void md_step_launches(Batch *b, int k)
         note(b, cudaStreamGetCaptureInfo(st, &st_cap, nullptr, &g, nullptr, nullptr));
         note(b, cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
     }
-    kb_step_begin<R><<<b->n_ptile, kBT, 0, st>>>(b->ptile, b->rep, s, alt.pos, s.force_old, (R)dt, (R)dt_sq,
+    kb_step_begin<R><<<b->n_ptile + (colloid_block_first<R>() ? 1 : 0), kBT, 0, st>>>(b->ptile, b->rep, s, alt.pos, s.force_old, (R)dt, (R)dt_sq,
                                                  b->so_max, b->done, b->resort, b->n_extra, cs,
                                                  ResortLists{b->ptile_first, b->ptile_count, b->stile_first,
                                                              b->stile_count, b->act_p, b->act_s, b->n_act},
@@ -1020,7 +1049,8 @@ static void free_batch(Batch *b)
     rmpcd_particles_destroy(b->col);
     void *ptrs[] = {b->rep, b->ptile, b->stile, b->stile_first, b->stile_count, b->tile_sum, b->tile_off, b->count,
                     b->start, b->cursor, b->is_md, b->is_reac, b->stencil, b->list, b->nn, b->pair_f, b->pair_e,
-                    b->contrib, b->ncontrib, b->max_contrib, b->clist, b->cn, b->so_max, b->resort, b->n_extra,
+                    b->contrib, b->ncontrib, b->max_contrib, b->clist, b->cn, b->so_max, b->co_max, b->resort,
+                    b->n_extra,
                     b->big, b->n_big, b->rattle[0], b->rattle[1], b->rattle[2], b->vv_mass, b->d_step, b->done,
                     b->ptile_first, b->ptile_count, b->act_p, b->act_s, b->n_act, b->all_p, b->all_s, b->n_all};
     for (void *q : ptrs) cudaFree(q);
@@ -1186,7 +1216,8 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
               !dalloc(&b->stencil, 3 * (size_t)b->n_stencil) && !dalloc(&b->list, ne) && !dalloc(&b->nn, 2 * (size_t)R) &&
               !dalloc(&b->pair_f, 3 * ne) && !dalloc(&b->pair_e, ne) && !dalloc(&b->contrib, ne) &&
               !dalloc(&b->ncontrib, off) && !dalloc(&b->max_contrib, R) && !dalloc(&b->clist, ne) &&
-              !dalloc(&b->cn, 2 * (size_t)R) && !dalloc(&b->so_max, R) && !dalloc(&b->resort, R) &&
+              !dalloc(&b->cn, 2 * (size_t)R) && !dalloc(&b->so_max, R) && !dalloc(&b->co_max, R) &&
+              !dalloc(&b->resort, R) &&
               !dalloc(&b->n_extra, R) && !dalloc(&b->big, soff) && !dalloc(&b->n_big, 1) &&
               !dalloc(&b->rattle[0], 2 * (size_t)R) && !dalloc(&b->rattle[1], 2 * (size_t)R) &&
               !dalloc(&b->rattle[2], 2 * (size_t)R) && !dalloc(&b->vv_mass, 2 * (size_t)R) && !dalloc(&b->d_step, 1) &&
