@@ -451,17 +451,24 @@ __global__ void __launch_bounds__(kBT, 4)
         const uint64_t seed = rp.seed;
         const long long off = rp.off;
         constexpr int K = 4;
+        // The FP64 form reads every velocity: a zero-force update turns a -0
+        // component into +0, as the reference's does.  The FP32 form reads
+        // velocities only for particles with a force, leaving the others'
+        // bits untouched (a -0 stays -0; the dynamics never make one).
+        constexpr bool kAllVel = sizeof(R) == 8;
         for (long long base = t.begin + threadIdx.x; base < t.end; base += (long long)K * blockDim.x) {
           int fk[K];
-          R vxk[K], vyk[K], vzk[K];
+          R vxk[K] = {}, vyk[K] = {}, vzk[K] = {};
 #pragma unroll
           for (int k = 0; k < K; k++) {
             const long long i = base + (long long)k * blockDim.x;
             if (i < t.end) {
                 fk[k] = v.flags[i];
-                vxk[k] = v.vel.x[i];
-                vyk[k] = v.vel.y[i];
-                vzk[k] = v.vel.z[i];
+                if (kAllVel) {
+                    vxk[k] = v.vel.x[i];
+                    vyk[k] = v.vel.y[i];
+                    vzk[k] = v.vel.z[i];
+                }
             }
           }
 #pragma unroll
@@ -469,6 +476,11 @@ __global__ void __launch_bounds__(kBT, 4)
             const long long i = base + (long long)k * blockDim.x;
             if (i >= t.end) continue;
             int f = fk[k];
+            if (!kAllVel && !((f >> WALL_BIT) & 1) && (((f >> MD_BIT) & 1) || ((f >> PAST_MD_BIT) & 1))) {
+                vxk[k] = v.vel.x[i];
+                vyk[k] = v.vel.y[i];
+                vzk[k] = v.vel.z[i];
+            }
             const R vx = vxk[k], vy = vyk[k], vz = vzk[k];
             if (!((f >> WALL_BIT) & 1)) {
                 const bool md = (f >> MD_BIT) & 1, past = (f >> PAST_MD_BIT) & 1;
@@ -479,7 +491,7 @@ __global__ void __launch_bounds__(kBT, 4)
                     v.vel.x[i] = vx + dt * (f0 + g0) / 2;
                     v.vel.y[i] = vy + dt * (f1 + g1) / 2;
                     v.vel.z[i] = vz + dt * (f2 + g2) / 2;
-                } else {
+                } else if (kAllVel) {
                     // both forces are zero: the update changes a velocity
                     // only if it is -0, so the store is kept for that case
                     const R z = 0;
