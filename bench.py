@@ -210,9 +210,11 @@ def roofline(N, S, precision, phase, peak, peak_kind):
 DIMER_N_MD = 100
 DIMER_LIST_CAPACITY = 4000
 # HBM bytes per solvent particle and MD step of the two streaming kernels of
-# the dimer engine (step begin: flags, species, pos r/w, vel, pos_old; step
-# end: flags, vel; force entries are touched only for flagged particles)
-DIMER_BYTES_PER_MD_STEP = {32: 72, 64: 132}
+# the dimer engine (step begin: flags, pos r/w, vel, pos_old -- species only
+# for a batch created with a negative species; step end: flags, plus in the
+# FP64 form every velocity, in the FP32 form only those of particles with a
+# force; force entries are touched only for flagged particles)
+DIMER_BYTES_PER_MD_STEP = {32: 56, 64: 128}
 
 
 def dimer_boxes_batched(n=512, seed=2024):

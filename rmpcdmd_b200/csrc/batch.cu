@@ -93,6 +93,10 @@ struct rmpcd_dimer_batch {
     int *ncontrib = nullptr, *max_contrib = nullptr, *clist = nullptr, *cn = nullptr;
     unsigned long long *so_max = nullptr;
     double *co_max = nullptr;  // per replica: the colloids' displacement of this MD step
+    // whether some solvent species was negative at creation; species change
+    // only to 1 or 2 inside the batch, so otherwise every particle passes
+    // maximum_displacement's species >= 0 test and species need not be read
+    bool read_species = true;
     int *resort = nullptr, *n_extra = nullptr, *big = nullptr, *n_big = nullptr;
     double *rattle[3] = {nullptr, nullptr, nullptr};
     double *vv_mass = nullptr;
@@ -280,7 +284,7 @@ template <typename R>
 __global__ void __launch_bounds__(kBT, 4)
     kb_step_begin(const BTile *tiles, const BRep *rep, PView<R> v, Vec3<R> old, Vec3<R> next, R dt, R dt_sq,
                   unsigned long long *so_max, unsigned *done, int *resort, int *n_extra, ColloidStep cs,
-                  ResortLists rl, cudaGraphConditionalHandle cond, int use_cond, unsigned *err)
+                  ResortLists rl, cudaGraphConditionalHandle cond, int use_cond, int read_species, unsigned *err)
 {
     __shared__ int s_last;
     __shared__ int ws[kBT / 32 + 1];
@@ -302,7 +306,7 @@ __global__ void __launch_bounds__(kBT, 4)
             const long long i = base + (long long)k * blockDim.x;
             if (i < t.end) {
                 f[k] = v.flags[i];
-                sp[k] = v.species[i];
+                sp[k] = read_species ? v.species[i] : 0;
                 px[k] = v.pos.x[i];
                 py[k] = v.pos.y[i];
                 pz[k] = v.pos.z[i];
@@ -971,7 +975,8 @@ static void md_step_launches(Batch *b, int k)
                                                  b->so_max, b->done, b->resort, b->n_extra, cs,
                                                  ResortLists{b->ptile_first, b->ptile_count, b->stile_first,
                                                              b->stile_count, b->act_p, b->act_s, b->n_act},
-                                                 cond, b->capturing ? 1 : 0, dev_error_word());
+                                                 cond, b->capturing ? 1 : 0, b->read_species ? 1 : 0,
+                                                 dev_error_word());
     if (b->capturing) capture_conditional_resort<R>(b, st, g, cond);
     else resort_launches<R>(b, b->resort, false, st, -1);
     // switch_force: the cleared entries become `force`
@@ -1081,6 +1086,16 @@ static int d2d(void *dst, const void *src, size_t bytes)
 {
     if (bytes) RMPCD_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream()));
     return RMPCD_OK;
+}
+
+// *out = 1 if some a[i] < 0
+__global__ void k_any_negative(const int *a, long long n, int *out)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        if (a[i] < 0) {
+            *out = 1;
+            return;
+        }
 }
 
 // copy one particle system's current arrays (and pos_old) to/from the batch
@@ -1295,7 +1310,16 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
                                                                           nl[r]->n, 2, b->Nmax, p.off);
         d2d(b->nn + 2 * r, nl[r]->n, 2 * sizeof(int));
     }
-    rc = sync();
+    {
+        int *neg = nullptr, h_neg = 1;
+        if (cudaMalloc(&neg, sizeof(int)) == cudaSuccess && cudaMemsetAsync(neg, 0, sizeof(int), st) == cudaSuccess) {
+            k_any_negative<<<grid_cap(b->sol->N, 256), 256, 0, st>>>(b->sol->species[0], b->sol->N, neg);
+            if (cudaMemcpyAsync(&h_neg, neg, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) h_neg = 1;
+        }
+        rc = sync();
+        cudaFree(neg);
+        b->read_species = h_neg != 0;
+    }
     if (rc) {
         free_batch(b);
         return rc;
