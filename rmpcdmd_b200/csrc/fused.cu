@@ -371,6 +371,7 @@ __global__ void __launch_bounds__(kFusedThreads, S::kMinBlocks) k_bulk_interval(
         // the tile's source indices perm[a0, a0 + np): one bulk copy of the
         // enclosing 16-byte window (perm is allocated to a multiple of 4)
         int *s_perm = s_idx;
+        bool gave_up = false;  // this thread stopped waiting for the index copy
         if (A.perm) {
             const int w0 = a0 & ~3;
             const unsigned bytes = (unsigned)(((a0 - w0 + np + 3) & ~3) * sizeof(int));
@@ -382,10 +383,14 @@ __global__ void __launch_bounds__(kFusedThreads, S::kMinBlocks) k_bulk_interval(
             }
             if (bytes && !mbar_wait_bounded(&s_bar, 0, kBulkPolls)) {
                 // not delivered in time: report it and load the same values
-                // directly (a late copy can only write this tile's indices
-                // again, at worst undoing their in-cell order, which the
-                // error bit already flags; never an index outside the tile)
+                // directly.  While the block runs, a late copy writes only
+                // this tile's index window, with the values loaded here (at
+                // worst undoing their in-cell order, which the error bit
+                // already flags); the thread waits for it again before it
+                // exits (below), so the copy cannot land in the shared memory
+                // of a later block.
                 atomicOr(A.err, DEV_ERR_BULK_WAIT);
+                gave_up = true;
                 for (int j = t; j < np; j += kFusedThreads) s_perm[j] = __ldcs(A.perm + a0 + j);
             }
         } else {
@@ -451,6 +456,10 @@ __global__ void __launch_bounds__(kFusedThreads, S::kMinBlocks) k_bulk_interval(
             cur = nxt;
             j = jn;
         }
+        // a copy given up on must land before the block's shared memory is
+        // released; if it has not within a second limit either, the block
+        // exits with it pending and says so (a separate error bit)
+        if (gave_up && !mbar_wait_bounded(&s_bar, 0, kBulkPolls)) atomicOr(A.err, DEV_ERR_BULK_UNDRAINED);
     } else {
         // ---- over-full tile (dense cells): the same steps in global memory ----
         if (A.perm && my_n > 1) sort_small(A.perm + my_a, my_n);

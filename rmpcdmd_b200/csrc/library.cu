@@ -98,6 +98,9 @@ int check_dev_error(unsigned *bits_out)
             return fail(RMPCD_ERR_DEVICE, "rattle: negative discriminant or bead species outside the mass table");
         if (bits & DEV_ERR_QUAT_LOOP)
             return fail(RMPCD_ERR_DEVICE, "rigid_body_vv1: quaternion iteration did not converge");
+        if (bits & DEV_ERR_BULK_UNDRAINED)
+            return fail(RMPCD_ERR_DEVICE, "a bulk copy was still pending when its block exited; "
+                                          "shared memory of later blocks may have been overwritten");
         if (bits & DEV_ERR_BULK_WAIT)
             return fail(RMPCD_ERR_DEVICE, "bulk interval: an index bulk copy did not complete within its wait limit");
         return fail(RMPCD_ERR_DEVICE, "device error bits 0x%x", bits);

@@ -271,8 +271,10 @@ __device__ inline void update_list_block(int i, const Grid &g, const double *cx,
         __syncthreads();
     }
     if (t == 0) n_out[i] = s_base < Nmax ? s_base : Nmax;
-    // copies of a phase given up on land before the block's shared memory goes
-    if (pending) mbar_wait_bounded(stage.bar, phase ^ 1u, kNlStagePolls);
+    // a copy phase given up on is waited for again, bounded, before the block's
+    // shared memory is released; if it has not landed within that second
+    // limit either, the block exits with it pending and sets its own error bit
+    if (pending && !mbar_wait_bounded(stage.bar, phase ^ 1u, kNlStagePolls)) atomicOr(err, DEV_ERR_BULK_UNDRAINED);
 }
 
 

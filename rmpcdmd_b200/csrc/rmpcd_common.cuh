@@ -57,6 +57,7 @@ enum : unsigned {
     DEV_ERR_RATTLE = 4u,       // RATTLE square root of a negative number
     DEV_ERR_QUAT_LOOP = 8u,    // rigid_body_vv1's quaternion iteration hit its cap
     DEV_ERR_BULK_WAIT = 16u,   // a bulk copy did not complete within its wait limit
+    DEV_ERR_BULK_UNDRAINED = 32u,  // ... nor within a second limit before its block exited
 };
 unsigned *dev_error_word();
 int check_dev_error(unsigned *bits_out);
