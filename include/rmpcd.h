@@ -298,8 +298,12 @@ int rmpcd_colloid_vv_vel(rmpcd_particles *p, double dt, const double *mass);
  * fixed 64 KB scratch array inside the library, so N must be <= 8192
  * (RMPCD_ERR_CAPACITY otherwise).  The first call on each device looks up the
  * scratch address (one-time setup): make it before starting any stream
- * capture.  Nothing in the scratch has to start at zero.  There is one scratch
- * array per device, so calls that overlap (several host threads) race on it. */
+ * capture.  `mass` is read by an asynchronous host-to-device copy on the
+ * library stream: from pageable memory the driver has taken the values when
+ * the call returns; from page-locked memory it reads them later, so keep them
+ * unchanged until the library stream has passed the call (rmpcd_synchronize).
+ * Nothing in the scratch has to start at zero.  There is one scratch array
+ * per device, so calls that overlap (several host threads) race on it. */
 int rmpcd_colloid_vv_pos_noalloc(rmpcd_particles *p, double dt, const double *mass);
 
 /* ------------------------------------------------------------------ */

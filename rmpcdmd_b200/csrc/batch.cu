@@ -457,8 +457,10 @@ __global__ void __launch_bounds__(kBT, 4)
         constexpr int K = 4;
         // The FP64 form reads every velocity: a zero-force update turns a -0
         // component into +0, as the reference's does.  The FP32 form reads
-        // velocities only for particles with a force, leaving the others'
-        // bits untouched (a -0 stays -0; the dynamics never make one).
+        // velocities only for particles with a force and leaves the others'
+        // bits untouched, so it keeps a -0 component (an SRD rotation product
+        // can round to one) where the reference would store +0: equal in
+        // value, not in bits, which is why FP32 results are compared by value.
         constexpr bool kAllVel = sizeof(R) == 8;
         for (long long base = t.begin + threadIdx.x; base < t.end; base += (long long)K * blockDim.x) {
           int fk[K];

@@ -39,6 +39,35 @@ def test_noalloc_matches_allocating_entry_point(rm, N):
     rm.get_status()
 
 
+def _free_device_bytes():
+    for name in ("libcudart.so.12", "libcudart.so"):
+        try:
+            cudart = C.CDLL(name)
+            break
+        except OSError:
+            continue
+    else:
+        pytest.skip("no CUDA runtime library to query free device memory")
+    free, total = C.c_size_t(0), C.c_size_t(0)
+    assert cudart.cudaMemGetInfo(C.byref(free), C.byref(total)) == 0
+    return free.value
+
+
+def test_noalloc_leaves_free_device_memory_unchanged(rm):
+    # the property the entry point exists for: after its one-time set-up it
+    # takes no device memory, even for a system larger than any seen before
+    warm, m0 = system(rm, 16, 9)
+    vv_pos(rm, "rmpcd_colloid_vv_pos_noalloc", warm, 0.01, m0)
+    p, m = system(rm, MAX_PARTICLES, 10)
+    rm._capi.call("rmpcd_synchronize")
+    before = _free_device_bytes()
+    for dt in (0.01, 0.02, 0.005, 0.01):
+        vv_pos(rm, "rmpcd_colloid_vv_pos_noalloc", p, dt, m)
+    rm._capi.call("rmpcd_synchronize")
+    assert _free_device_bytes() == before
+    rm.get_status()
+
+
 def test_noalloc_rejects_more_particles_than_its_scratch(rm):
     p, m = system(rm, MAX_PARTICLES + 1, 8)
     before = p.download("pos")
