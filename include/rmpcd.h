@@ -138,6 +138,17 @@ int rmpcd_cells_set_max_v(rmpcd_cells *cells, double max_v);
 int rmpcd_cells_random_shift(rmpcd_cells *cells, rmpcd_rng *rng);
 /* count_particles, src/cell_system.f90:86-129, on the positions of p */
 int rmpcd_cells_count_particles(rmpcd_cells *cells, rmpcd_particles *p);
+/* sort_particles, src/cell_system.f90:131-151: the positions of position_old
+ * written, in cell order, as the positions of position_new (a different system
+ * of the same size and precision; nothing else of either changes), through the
+ * starts of the last count_particles on those positions.  Inside a cell the
+ * order is ascending in position_old (the reference's single-thread order).
+ * Afterwards every cell_start has advanced by its cell's count, as the
+ * reference's scatter leaves it; call count_particles again before using the
+ * starts.  Counts or starts that do not belong to these positions are
+ * RMPCD_ERR_INVALID, with nothing written. */
+int rmpcd_cells_sort_particles(rmpcd_cells *cells, const rmpcd_particles *position_old,
+                               rmpcd_particles *position_new);
 /* cell_count(S), cell_start(S) (1-based), is_md(S), is_reac(S) */
 int rmpcd_cells_download_count(const rmpcd_cells *cells, int *count);
 int rmpcd_cells_download_start(const rmpcd_cells *cells, int *start);

@@ -215,6 +215,13 @@ class Particles:
     def count(self, c: Cells):
         lib().orc_count_particles(C.byref(c.g), self.N, dp(self.pos), ip(c.cell_count), ip(c.cell_start))
 
+    def sort_particles(self, c: Cells) -> np.ndarray:
+        """cell_system_t%sort_particles of this system's positions; returns
+        the scattered positions (cell_start of c advances by the counts)."""
+        out = np.zeros_like(self.pos)
+        lib().orc_sort_particles(C.byref(c.g), self.N, ip(c.cell_start), dp(self.pos), dp(out))
+        return out
+
     def maximum_displacement(self):
         return float(lib().orc_maximum_displacement(self.N, dp(self.pos), dp(self.pos_old), ip(self.species)))
 

@@ -122,6 +122,7 @@ PROTOTYPES = {
     "rmpcd_cells_set_max_v": [CELLS_P, C.c_double],
     "rmpcd_cells_random_shift": [CELLS_P, RNG_P],
     "rmpcd_cells_count_particles": [CELLS_P, PART_P],
+    "rmpcd_cells_sort_particles": [CELLS_P, PART_P, PART_P],
     "rmpcd_cells_download_count": [CELLS_P, c_int_p],
     "rmpcd_cells_download_start": [CELLS_P, c_int_p],
     "rmpcd_cells_download_is_md": [CELLS_P, c_uchar_p],

@@ -226,6 +226,12 @@ class CellSystem:
     def count_particles(self, p: "ParticleSystem") -> None:
         call("rmpcd_cells_count_particles", self._h, p.handle)
 
+    def sort_particles(self, position_old: "ParticleSystem", position_new: "ParticleSystem") -> None:
+        """sort_particles, src/cell_system.f90:131-151: the positions of
+        position_old, in cell order, become those of position_new; the starts
+        advance by the counts (call count_particles before using them)."""
+        call("rmpcd_cells_sort_particles", self._h, position_old.handle, position_new.handle)
+
     @property
     def cell_count(self) -> np.ndarray:
         a = np.zeros(self.N, np.int32)

@@ -182,6 +182,17 @@ int rmpcd_cells_count_particles(rmpcd_cells *c, rmpcd_particles *p)
     return count_and_scan(c, p, false);
 }
 
+// sort_particles, src/cell_system.f90:131-151
+int rmpcd_cells_sort_particles(rmpcd_cells *c, const rmpcd_particles *position_old, rmpcd_particles *position_new)
+{
+    RMPCD_ARG(c && position_old && position_new, "null argument");
+    RMPCD_ARG(position_old != position_new, "sort_particles: position_old and position_new must be different systems");
+    RMPCD_ARG(position_old->N == position_new->N && position_old->precision == position_new->precision,
+              "sort_particles: both systems need the same size and precision");
+    PhaseTimer t("sort");
+    return sort_positions(c, position_old, position_new);
+}
+
 static int dl(const void *src, void *dst, size_t bytes)
 {
     RMPCD_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream()));

@@ -327,6 +327,98 @@ int sort_particles_flagged(rmpcd_cells *c, rmpcd_particles *p, const double edge
     return sort_particles_flagged_t<double>(c, p, edges);
 }
 
+// cell_system_t%sort_particles (src/cell_system.f90:131-151): the positions
+// of `from` scattered into the positions of `to` through the starts of the
+// last count_particles.  Before any scatter, one pass keys the positions and
+// checks that they give exactly the counts on record and that every cell's
+// range lies inside [0, N); a mismatch is an argument error and nothing is
+// written.  The order inside a cell is ascending source index (the
+// reference's single-thread order); afterwards every start has advanced by
+// its cell's count, as the reference's scatter cursor leaves cell_start.
+template <typename R>
+__global__ void k_key_check(Grid g, const R *__restrict__ x, const R *__restrict__ y, const R *__restrict__ z,
+                            int N, int *__restrict__ key, int *__restrict__ hist)
+{
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < N; base += stride) {
+        long long i = base + threadIdx.x;
+        bool ok = i < N;
+        int s = -1;
+        if (ok) {
+            s = slot_of(g, (double)x[i], (double)y[i], (double)z[i]);
+            key[i] = s;
+        }
+        unsigned peers = __match_any_sync(0xffffffffu, s);
+        if (ok && lane == __ffs(peers) - 1) atomicAdd(hist + s, __popc(peers));
+    }
+}
+
+__global__ void k_counts_agree(const int *__restrict__ hist, const int *__restrict__ count,
+                               const int *__restrict__ start, int S, int N, int *__restrict__ bad)
+{
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
+        const int n = count[s], a = start[s];
+        if (hist[s] != n || n < 0 || a < 0 || (long long)a + n > N) atomicOr(bad, 1);
+    }
+}
+
+template <typename R>
+__global__ void k_gather_pos(Vec3<R> src, Vec3<R> dst, const int *__restrict__ perm, int N)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < N; j += stride) {
+        const int i = perm[j];
+        dst.x[j] = src.x[i];
+        dst.y[j] = src.y[i];
+        dst.z[j] = src.z[i];
+    }
+}
+
+__global__ void k_advance_starts(int *__restrict__ start, const int *__restrict__ count, int S)
+{
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) start[s] += count[s];
+}
+
+template <typename R>
+static int sort_positions_t(rmpcd_cells *c, const rmpcd_particles *from, rmpcd_particles *to)
+{
+    cudaStream_t st = stream();
+    const int N = from->N;
+    int *bad = to->d_ints;
+    // the cursors are free until the scatter: they hold the check's histogram
+    RMPCD_CUDA_TRY(cudaMemsetAsync(c->cursor, 0, (size_t)c->S * sizeof(int), st));
+    RMPCD_CUDA_TRY(cudaMemsetAsync(bad, 0, sizeof(int), st));
+    PView<R> s = cur<R>(from);
+    if (N > 0)
+        k_key_check<R><<<grid_for(N, 256), 256, 0, st>>>(grid_of(c), s.pos.x, s.pos.y, s.pos.z, N, to->key,
+                                                         c->cursor);
+    k_counts_agree<<<grid_for(c->S, 256), 256, 0, st>>>(c->cursor, c->count, c->start, c->S, N, bad);
+    RMPCD_CHECK_LAUNCH();
+    int h_bad = 0;
+    RMPCD_CUDA_TRY(cudaMemcpyAsync(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+    RMPCD_CUDA_TRY(cudaStreamSynchronize(st));
+    if (h_bad)
+        return fail(RMPCD_ERR_INVALID,
+                    "sort_particles: the cell counts and starts are not those of these positions "
+                    "(call count_particles on them first)");
+    if (N > 0) {
+        RMPCD_CUDA_TRY(cudaMemcpyAsync(c->cursor, c->start, (size_t)c->S * sizeof(int), cudaMemcpyDeviceToDevice, st));
+        int rc = build_perm(c, to);
+        if (rc) return rc;
+        k_gather_pos<R><<<grid_for(N, 256), 256, 0, st>>>(s.pos, cur<R>(to).pos, to->perm, N);
+    }
+    k_advance_starts<<<grid_for(c->S, 256), 256, 0, st>>>(c->start, c->count, c->S);
+    RMPCD_CHECK_LAUNCH();
+    return RMPCD_OK;
+}
+
+int sort_positions(rmpcd_cells *c, const rmpcd_particles *from, rmpcd_particles *to)
+{
+    if (from->precision == RMPCD_FP32) return sort_positions_t<float>(c, from, to);
+    return sort_positions_t<double>(c, from, to);
+}
+
 int sort_particles(rmpcd_cells *c, rmpcd_particles *p)
 {
     int rc;

@@ -29,6 +29,8 @@ int build_perm(rmpcd_cells *c, rmpcd_particles *p);
 int gather_all(rmpcd_particles *p);
 // full sort
 int sort_particles(rmpcd_cells *c, rmpcd_particles *p);
+// positions of `from` into `to` in cell order (cell_system_t%sort_particles)
+int sort_positions(rmpcd_cells *c, const rmpcd_particles *from, rmpcd_particles *to);
 // apply_pbc with the given edges, then the full sort, for a system in which a
 // particle with neither MD nor PAST_MD set has zero force and force_old (the
 // state compute_force and its flag roll maintain): those entries are written

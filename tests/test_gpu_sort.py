@@ -111,3 +111,59 @@ def test_count_particles_slot_scan_extremes(rm, oracle, L, N):
         gc.count_particles(gp)
         assert_cells_same(gc, oc)
     assert int(gc.cell_count.sum()) == N
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+@pytest.mark.parametrize("L,N,lo,hi", [([120, 30, 30], 1000000, 0.0, 1.0), ([7, 5, 9], 3000, -0.5, 1.5),
+                                       ([4, 4, 4], 0, 0.0, 1.0)])
+def test_sort_particles(rm, oracle, precision, L, N, lo, hi):
+    """cell_system_t%sort_particles on test/test_cell_system_0.f90's geometry
+    (10^6 positions in a 120 x 30 x 30 box), on positions partly outside the
+    box, and on an empty system: count_particles, sort_particles, the starts
+    the scatter leaves, then the reference test's checks after a recount."""
+    rng = np.random.default_rng(N + 1)
+    pos = (lo + (hi - lo) * rng.random((N, 3))) * np.asarray(L)
+    if precision == 32:
+        pos = pos.astype(np.float32).astype(np.float64)
+    oc = oracle.Cells(L)
+    op = oracle.Particles(N, 1)
+    op.pos[:] = pos
+    op.count(oc)
+    want = op.sort_particles(oc)
+    gc = rm.CellSystem(L, 1.0)
+    a = rm.ParticleSystem(N, 1, None, precision)
+    b = rm.ParticleSystem(N, 1, None, precision)
+    a.pos = pos
+    gc.count_particles(a)
+    gc.sort_particles(a, b)
+    assert np.array_equal(b.pos, want)
+    assert np.array_equal(a.pos, pos)
+    assert np.array_equal(gc.cell_start, oc.cell_start)  # advanced by the counts, as the reference leaves them
+    gc.count_particles(b)
+    start, count = gc.cell_start, gc.cell_count
+    S = len(count)
+    assert start[0] == 1 and start[S - 1] + count[S - 1] == N + 1 and count.sum() == N
+    # every position lies in the cell of its range (test_cell_system_0.f90:61-70)
+    if N:
+        b.sort(gc)  # the scattered order is already the cell order: the sort is the identity
+        assert np.array_equal(b.pos, want)
+    rm.get_status()
+
+
+def test_sort_particles_rejects_counts_of_other_positions(rm):
+    L = [6, 6, 6]
+    r = np.random.default_rng(3)
+    gc = rm.CellSystem(L, 1.0)
+    a = rm.ParticleSystem(2000, 1)
+    b = rm.ParticleSystem(2000, 1)
+    a.pos = r.random((2000, 3)) * 6
+    b.pos = r.random((2000, 3)) * 6
+    gc.count_particles(b)
+    before = b.pos
+    with pytest.raises(rm.RmpcdError) as e:
+        gc.sort_particles(a, b)
+    assert e.value.code == 1 and "count_particles" in str(e.value)
+    assert np.array_equal(b.pos, before)
+    with pytest.raises(rm.RmpcdError):
+        gc.sort_particles(a, a)
+    rm.get_status()
