@@ -185,10 +185,12 @@ int rmpcd_particles_maximum_displacement(rmpcd_particles *p, double *r);
 /* cell_maximum_displacement, src/particle_system.f90:380-410 */
 int rmpcd_cell_maximum_displacement(rmpcd_cells *cells, rmpcd_particles *p,
                                     double delta_t, double *r);
-/* random_placement, src/particle_system.f90:250-302 (other/lj may be NULL) */
+/* random_placement, src/particle_system.f90:250-302 (other/lj may be NULL).
+ * The draws are keyed by state->seed alone (the reference's state(1)); the
+ * step is not advanced. */
 int rmpcd_particles_random_placement(rmpcd_particles *p, const double L[3],
                                      rmpcd_particles *other, const rmpcd_lj *lj,
-                                     uint64_t seed);
+                                     const rmpcd_rng *state);
 /* Maxwell velocities with the mean removed, programs/single_dimer_pbc.f90:240-245 */
 int rmpcd_particles_maxwell(rmpcd_particles *p, double T, uint64_t seed);
 /* Number of particles with a NaN or infinite position or velocity component
@@ -221,8 +223,9 @@ int rmpcd_wall_mpcd_step(rmpcd_particles *p, rmpcd_cells *cells, rmpcd_rng *rng,
                          int has_alpha, double alpha, int keep_cell_v);
 /* compute_temperature, src/mpcd.f90:342-407 */
 int rmpcd_compute_temperature(rmpcd_particles *p, rmpcd_cells *cells, double *te);
-/* rescale_cells, src/mpcd.f90:748-801 */
-int rmpcd_rescale_cells(rmpcd_particles *p, rmpcd_cells *cells, double T);
+/* rescale_cells, src/mpcd.f90:748-801; rng may be NULL (the reference takes
+ * state(:) and draws nothing from it) */
+int rmpcd_rescale_cells(rmpcd_particles *p, rmpcd_cells *cells, rmpcd_rng *rng, double T);
 /* mpcd_stream_periodic, src/mpcd.f90:440-457 */
 int rmpcd_mpcd_stream_periodic(rmpcd_particles *p, rmpcd_cells *cells, double dt);
 /* mpcd_stream_xforce_yzwall, src/mpcd.f90:464-506 (+ yzwall_collision :511-589) */
@@ -236,7 +239,7 @@ int rmpcd_bulk_reaction(rmpcd_particles *p, rmpcd_cells *cells, int from, int to
 /* bulk_reaction_endothermic, src/mpcd.f90:645-700 (the reaction also needs the
  * cell's relative kinetic energy to exceed delta_u, and removes delta_u from it) */
 int rmpcd_bulk_reaction_endothermic(rmpcd_particles *p, rmpcd_cells *cells, int from, int to,
-                                    double rate, double tau, double delta_u, rmpcd_rng *rng);
+                                    double rate, double tau, rmpcd_rng *rng, double delta_u);
 
 /* ------------------------------------------------------------------ */
 /* MD, src/md.f90                                                       */

@@ -138,7 +138,7 @@ PROTOTYPES = {
     "rmpcd_particles_sort": [PART_P, CELLS_P],
     "rmpcd_particles_maximum_displacement": [PART_P, c_double_p],
     "rmpcd_cell_maximum_displacement": [CELLS_P, PART_P, C.c_double, c_double_p],
-    "rmpcd_particles_random_placement": [PART_P, c_double_p, PART_P, LJ_P, C.c_uint64],
+    "rmpcd_particles_random_placement": [PART_P, c_double_p, PART_P, LJ_P, RNG_P],
     "rmpcd_particles_count_nonfinite": [PART_P, C.POINTER(C.c_longlong)],
     "rmpcd_particles_maxwell": [PART_P, C.c_double, C.c_uint64],
     "rmpcd_particles_switch_force": [PART_P],
@@ -151,13 +151,13 @@ PROTOTYPES = {
     "rmpcd_wall_mpcd_step": [PART_P, CELLS_P, RNG_P, c_double_p, c_double_p, c_int_p, C.c_int, C.c_double,
                              C.c_int, C.c_double, C.c_int],
     "rmpcd_compute_temperature": [PART_P, CELLS_P, c_double_p],
-    "rmpcd_rescale_cells": [PART_P, CELLS_P, C.c_double],
+    "rmpcd_rescale_cells": [PART_P, CELLS_P, RNG_P, C.c_double],
     "rmpcd_mpcd_stream_periodic": [PART_P, CELLS_P, C.c_double],
     "rmpcd_mpcd_stream_xforce_yzwall": [PART_P, CELLS_P, C.c_double, C.c_double],
     "rmpcd_mpcd_stream_nogravity_zwall": [PART_P, CELLS_P, C.c_double],
     "rmpcd_bulk_reaction": [PART_P, CELLS_P, C.c_int, C.c_int, C.c_double, C.c_double, RNG_P],
-    "rmpcd_bulk_reaction_endothermic": [PART_P, CELLS_P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
-                                        RNG_P],
+    "rmpcd_bulk_reaction_endothermic": [PART_P, CELLS_P, C.c_int, C.c_int, C.c_double, C.c_double, RNG_P,
+                                        C.c_double],
     "rmpcd_md_pos": [PART_P, C.c_double],
     "rmpcd_md_vel": [PART_P, C.c_double],
     "rmpcd_cell_md_pos": [CELLS_P, PART_P, C.c_double, C.c_int],

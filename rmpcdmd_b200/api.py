@@ -358,9 +358,12 @@ class ParticleSystem:
         return r.value
 
     def random_placement(self, L, other: "ParticleSystem | None" = None, lj_params: LJParams | None = None,
-                         seed: int = 0) -> None:
+                         seed: "int | Rng" = 0) -> None:
+        """random_placement, src/particle_system.f90:250-302; ``seed`` is a
+        seed or the Rng whose seed keys the draws (the reference's state(1))."""
+        state = seed if isinstance(seed, Rng) else Rng(seed)
         call("rmpcd_particles_random_placement", self._h, _dp(_d3(L)), other.handle if other else None,
-             lj_params.ptr if lj_params else None, C.c_uint64(seed))
+             lj_params.ptr if lj_params else None, state.ptr)
 
     def maxwell(self, T: float, seed: int) -> None:
         call("rmpcd_particles_maxwell", self._h, float(T), C.c_uint64(seed))
@@ -471,7 +474,7 @@ def compute_temperature(particles: ParticleSystem, cells: CellSystem) -> float:
 
 
 def rescale_cells(particles: ParticleSystem, cells: CellSystem, state: Rng | None, T: float) -> None:
-    call("rmpcd_rescale_cells", particles.handle, cells.handle, float(T))
+    call("rmpcd_rescale_cells", particles.handle, cells.handle, state.ptr if state is not None else None, float(T))
 
 
 def mpcd_stream_periodic(particles: ParticleSystem, cells: CellSystem, dt: float) -> None:
@@ -494,7 +497,7 @@ def bulk_reaction_endothermic(p: ParticleSystem, c: CellSystem, frm: int, to: in
                               state: Rng, delta_u: float) -> None:
     """src/mpcd.f90:645-700 (argument order of the reference: ..., state, delta_u)."""
     call("rmpcd_bulk_reaction_endothermic", p.handle, c.handle, int(frm), int(to), float(rate), float(tau),
-         float(delta_u), state.ptr)
+         state.ptr, float(delta_u))
 
 
 def md_pos(particles: ParticleSystem, dt: float) -> None:

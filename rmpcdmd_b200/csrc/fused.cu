@@ -812,7 +812,7 @@ static int autotune_t(const int L[3], double tau, int n_intervals, int *best, fl
         const double edges[3] = {c->edges[0], c->edges[1], c->edges[2]};
         const uint64_t seed = 0x5eed;
         rmpcd_rng r{seed, 0};
-        rc = rmpcd_particles_random_placement(p, edges, nullptr, nullptr, seed);
+        rc = rmpcd_particles_random_placement(p, edges, nullptr, nullptr, &r);
         if (!rc) rc = rmpcd_particles_maxwell(p, 1.0 / 3.0, seed);
         if (!rc) {
             k_fill_int<<<grid_for(N, 256), 256, 0, stream()>>>(p->species[p->cur], N, 1);

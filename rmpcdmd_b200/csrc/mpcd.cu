@@ -524,7 +524,7 @@ int rmpcd_compute_temperature(rmpcd_particles *p, rmpcd_cells *c, double *te)
     return sync();
 }
 
-int rmpcd_rescale_cells(rmpcd_particles *p, rmpcd_cells *c, double T)
+int rmpcd_rescale_cells(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *, double T)
 {
     RMPCD_ARG(p && c, "null argument");
     PhaseTimer t("step");
@@ -596,7 +596,7 @@ int rmpcd_bulk_reaction(rmpcd_particles *p, rmpcd_cells *c, int from, int to, do
 }
 
 int rmpcd_bulk_reaction_endothermic(rmpcd_particles *p, rmpcd_cells *c, int from, int to, double rate,
-                                    double tau, double delta_u, rmpcd_rng *r)
+                                    double tau, rmpcd_rng *r, double delta_u)
 {
     RMPCD_ARG(p && c && r, "null argument");
     int gr = grid_full(c->S, 128);

@@ -529,7 +529,7 @@ extern "C" int rmpcd_ncolloids_run(rmpcd_particles *solvent, rmpcd_particles *co
         if (!rc) rc = catch_up_and_sort(L, k == n_intervals - 1);
         if (!rc)
             rc = rmpcd_simple_mpcd_step(solvent, cells, rng, 0, 0.0, thermostat, T ? T[k] : 0.0, params->do_hydro);
-        if (!rc && rescale_every > 0 && i % rescale_every == 0) rc = rmpcd_rescale_cells(solvent, cells, T_rescale);
+        if (!rc && rescale_every > 0 && i % rescale_every == 0) rc = rmpcd_rescale_cells(solvent, cells, nullptr, T_rescale);
         rc0 = rc;
     }
     cudaStreamSynchronize(stream());

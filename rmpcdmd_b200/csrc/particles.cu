@@ -527,9 +527,10 @@ int rmpcd_cell_maximum_displacement(rmpcd_cells *c, rmpcd_particles *p, double d
 }
 
 int rmpcd_particles_random_placement(rmpcd_particles *p, const double L[3], rmpcd_particles *other,
-                                     const rmpcd_lj *lj, uint64_t seed)
+                                     const rmpcd_lj *lj, const rmpcd_rng *state)
 {
-    RMPCD_ARG(p && L, "null argument");
+    RMPCD_ARG(p && L && state, "null argument");
+    const uint64_t seed = state->seed;
     RMPCD_ARG((other == nullptr) == (lj == nullptr),
               "other and lj_params must be present/absent together");
     if (p->N == 0) return RMPCD_OK;
