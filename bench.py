@@ -37,9 +37,10 @@ RHO = 10
 T_INIT = 1.0 / 3.0
 TAU = 1.0
 SEED = 20241203
-# HBM bytes the fused interval kernel must move per particle and per slot
-# (read + write of the full particle record, the permutation index and the
-# next key; see the traffic table in DESIGN.md)
+# HBM bytes the fused interval kernel must move per particle and per slot:
+# read + write of the full particle record (32 B FP32, 56 B FP64), the
+# permutation index (4 B) and the next key (4 B); per slot the count and start
+# read and the next count written
 BYTES_PER_PARTICLE = {32: 72, 64: 120}
 BYTES_PER_SLOT = 12
 # Minimum bytes of one whole interval (stream + sort + collide) over the
@@ -481,7 +482,7 @@ def run_ours(args):
         if precision == 64:
             cbc_steps = max(1, min(3, args.steps))
             results[64]["cbc"] = (max_over_ranks(dist, call_by_call_ms(rm, p, cells, rng, cbc_steps)), cbc_steps)
-            del p, cells
+        del p, cells
     r32, r64 = results[32], results[64]
     value = world * N * args.steps / (r32["ms"] * 1e-3)
     out.update(value=value, ms_per_step=r32["ms"] / args.steps)
@@ -520,12 +521,16 @@ def run_ours(args):
     out["gpu_launches"] = 4 * args.steps + 4
     if not args.no_e2e:
         e2e_steps = max(1, min(args.e2e_steps, args.steps))
-        v, hb, db = e2e_run(rm, r32["p"], r32["cells"], r32["rng"], e2e_steps)
-        v = world * (1.0 / max_over_ranks(dist, 1.0 / v))
-        out["e2e"] = {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": hb, "d2h_bytes_per_step": db,
-                      "steps": e2e_steps,
-                      "path": "rmpcd_particles_upload x6 (pinned host, reference (3,N) layout) -> rmpcd_bulk_run(1) "
-                              "-> rmpcd_particles_download x6"}
+        path = ("rmpcd_particles_upload x6 (pinned host, reference (3,N) layout) -> rmpcd_bulk_run(1) "
+                "-> rmpcd_particles_download x6")
+        for prec, key in ((32, "e2e"), (64, "e2e_fp64")):
+            r = results[prec]
+            v, hb, db = e2e_run(rm, r["p"], r["cells"], r["rng"], e2e_steps)
+            v = world * (1.0 / max_over_ranks(dist, 1.0 / v))
+            out[key] = {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": hb, "d2h_bytes_per_step": db,
+                        "steps": e2e_steps, "dtype": f"f{prec}", "path": path}
+            r.pop("p", None)
+            r.pop("cells", None)
     if not args.no_dimer:
         for r in (r32, r64):
             r.pop("p", None)
