@@ -376,7 +376,11 @@ int rmpcd_velocity_sums(rmpcd_particles *p, double out[4]);
  * test/setup_bulk_decay.f90:112-121 (simple_mpcd_step -> mpcd_stream_periodic
  * -> random_shift -> sort).  The system must be sorted for the current
  * origin on entry and is sorted for the final origin on return.  Interval i
- * uses rng step s+2i for the collision and s+2i+1 for the shift. */
+ * uses rng step s+2i for the collision and s+2i+1 for the shift.  FP64:
+ * results equal the reference's single-thread arithmetic and order.  FP32:
+ * the cell means come from exact fixed-point sums (2^-40 resolution), which
+ * do not depend on the order of a cell's particles; on return each cell's
+ * particles are in ascending order of their position on entry. */
 int rmpcd_bulk_run(rmpcd_particles *p, rmpcd_cells *cells, rmpcd_rng *rng,
                    double tau, int has_alpha, double alpha, int n_intervals);
 /* Tile shapes of the fused interval kernel (slots per block, resident

@@ -150,35 +150,52 @@ __device__ inline void cell_rotate(R &x, R &y, R &z, const R lv[3], const CellRo
     z = lv[2] + r2;
 }
 
+// FP32 cell sums are exact: every velocity component enters as a 64-bit
+// fixed-point integer of 2^-40 resolution (exactly for components of
+// magnitude 2^-17 and above, rounded to 2^-41 below that; a cell sum may
+// reach 2^23 in magnitude), so the cell mean does not depend on the order of
+// the cell's particles.  That is what lets the FP32 interval skip ordering each
+// cell's particles: the result of every particle is the same for any order.
+constexpr float kFixScale = 1099511627776.0f;  // 2^40
+
+__device__ inline long long to_fixed(float v)
+{
+    return __float2ll_rn(v * kFixScale);
+}
+
+__device__ inline float fixed_mean(long long s, int n)
+{
+    return (float)((double)s / (double)n * (1.0 / 1099511627776.0));
+}
+
 // SRD of one cell of n consecutive velocity parts (src/mpcd.f90:127-178);
 // stride is the distance between consecutive particles in bytes
 template <typename R>
 __device__ inline void srd_cell(unsigned char *v0, int stride, int n, const CellRot<R> &o)
 {
     if constexpr (sizeof(R) == 4) {
-        if (stride == 16) {
-            // one 16-byte shared-memory access per particle and pass
-            int n_eff = 0;
-            CellSum<float> sx, sy, sz;
-            for (int k = 0; k < n; k++) {
-                int4 c = ((const int4 *)v0)[k];
-                if (c.w > 0) {
-                    sx.add(__int_as_float(c.x));
-                    sy.add(__int_as_float(c.y));
-                    sz.add(__int_as_float(c.z));
-                    n_eff++;
-                }
+        // [vx vy vz species] in the first 16 bytes of every entry
+        int n_eff = 0;
+        long long sx = 0, sy = 0, sz = 0;
+        for (int k = 0; k < n; k++) {
+            int4 c = *(const int4 *)(v0 + (size_t)k * stride);
+            if (c.w > 0) {
+                sx += to_fixed(__int_as_float(c.x));
+                sy += to_fixed(__int_as_float(c.y));
+                sz += to_fixed(__int_as_float(c.z));
+                n_eff++;
             }
-            if (n_eff <= 1) return;
-            float lv[3] = {sx.value() / n_eff, sy.value() / n_eff, sz.value() / n_eff};
-            for (int k = 0; k < n; k++) {
-                int4 c = ((const int4 *)v0)[k];
-                float x = __int_as_float(c.x), y = __int_as_float(c.y), z = __int_as_float(c.z);
-                cell_rotate(x, y, z, lv, o);
-                ((int4 *)v0)[k] = make_int4(__float_as_int(x), __float_as_int(y), __float_as_int(z), c.w);
-            }
-            return;
         }
+        if (n_eff <= 1) return;
+        const float lv[3] = {fixed_mean(sx, n_eff), fixed_mean(sy, n_eff), fixed_mean(sz, n_eff)};
+        for (int k = 0; k < n; k++) {
+            int4 *q = (int4 *)(v0 + (size_t)k * stride);
+            int4 c = *q;
+            float x = __int_as_float(c.x), y = __int_as_float(c.y), z = __int_as_float(c.z);
+            cell_rotate(x, y, z, lv, o);
+            *q = make_int4(__float_as_int(x), __float_as_int(y), __float_as_int(z), c.w);
+        }
+        return;
     }
     int n_eff = 0;
     CellSum<R> sx, sy, sz;
@@ -396,12 +413,13 @@ __global__ void __launch_bounds__(kFusedThreads, S::kMinBlocks) k_bulk_interval(
         } else {
             for (int j = t; j < np; j += kFusedThreads) s_perm[j] = a0 + j;
         }
-        if (A.perm) {
-            // each cell's indices in ascending order (the reference's stable
-            // scatter order): every index is placed at its rank among the
-            // cell's indices, one thread per index, so a crowded cell costs
-            // no more than its share; the ranks go through the (still unused)
-            // velocity buffer and back
+        if (sizeof(R) == 8 && A.perm) {
+            // FP64: each cell's indices in ascending order (the reference's
+            // stable scatter order): every index is placed at its rank among
+            // the cell's indices, one thread per index, so a crowded cell
+            // costs no more than its share; the ranks go through the (still
+            // unused) velocity buffer and back.  (The FP32 cell sums do not
+            // depend on the order, so FP32 keeps the order of arrival.)
             if (t < SL) {
                 s_cstart[t] = my_a - a0;
                 s_ccount[t] = my_n;
@@ -462,7 +480,7 @@ __global__ void __launch_bounds__(kFusedThreads, S::kMinBlocks) k_bulk_interval(
         if (gave_up && !mbar_wait_bounded(&s_bar, 0, kBulkPolls)) atomicOr(A.err, DEV_ERR_BULK_UNDRAINED);
     } else {
         // ---- over-full tile (dense cells): the same steps in global memory ----
-        if (A.perm && my_n > 1) sort_small(A.perm + my_a, my_n);
+        if (sizeof(R) == 8 && A.perm && my_n > 1) sort_small(A.perm + my_a, my_n);
         __syncthreads();
         if (my_n > 0) {
             for (int k = 0; k < my_n; k++) {
@@ -572,6 +590,30 @@ __global__ void __launch_bounds__(kPackThreads) k_soa_to_rec(PView<R> v, unsigne
         for (int q = threadIdx.x; q < n * (B / 8); q += kPackThreads) dst[q] = src[q];
         __syncthreads();
     }
+}
+
+// FP32 end of a run: each cell's particles are put in ascending order of
+// their position at the start of the run (idx), a canonical order, since the
+// FP32 intervals leave them in order of arrival.  perm[j] is replaced by the
+// idx of its record (inv[idx] keeps the record), the segments are sorted and
+// mapped back to records.
+template <typename R>
+__global__ void k_perm_to_idx(const unsigned char *rec, int *perm, int *inv, int N)
+{
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < N;
+         j += (long long)gridDim.x * blockDim.x) {
+        const int r = perm[j];
+        const int idx = ((const int *)(rec + (size_t)r * Rec<R>::kBytes))[7];
+        inv[idx] = r;
+        perm[j] = idx;
+    }
+}
+
+__global__ void k_idx_to_perm(int *perm, const int *inv, int N)
+{
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < N;
+         j += (long long)gridDim.x * blockDim.x)
+        perm[j] = inv[perm[j]];
 }
 
 // final gather into the API arrays: pos, vel, species from the records
@@ -779,8 +821,19 @@ static int bulk_run_fused(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r, doub
     // complete the last sort: order each cell, gather the records into the
     // API arrays (which become current)
     PhaseTimer t("sort");
-    rc = sort_perm_segments(c, p);
-    if (rc) return rc;
+    if constexpr (sizeof(R) == 4) {
+        // the other record buffer is free: it holds inv
+        int *inv = (int *)p->rec[1 - rb];
+        k_perm_to_idx<R><<<grid_for(p->N, 256), 256, 0, st>>>(p->rec[rb], p->perm, inv, p->N);
+        RMPCD_CHECK_LAUNCH();
+        rc = sort_perm_segments(c, p);
+        if (rc) return rc;
+        k_idx_to_perm<<<grid_for(p->N, 256), 256, 0, st>>>(p->perm, inv, p->N);
+        RMPCD_CHECK_LAUNCH();
+    } else {
+        rc = sort_perm_segments(c, p);
+        if (rc) return rc;
+    }
     k_rec_gather_to_soa<R><<<grid_for(p->N, 256), 256, 0, st>>>(p->rec[rb], p->perm, side, alt<R>(p), p->N);
     RMPCD_CHECK_LAUNCH();
     p->cur = 1 - p->cur;

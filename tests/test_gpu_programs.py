@@ -57,6 +57,31 @@ def test_bulk_run_fp32_conservation(rm, oracle):
     assert abs(t32 - t64) / t64 < 0.05
 
 
+def test_bulk_run_fp32_order_and_determinism(rm, oracle):
+    """The FP32 fused form sums each cell exactly, so its result does not
+    depend on the order of a cell's particles: two runs give the same arrays,
+    and each cell ends in ascending order of the particles' positions on
+    entry."""
+    L, N = [16, 12, 10], 19200
+    outs = []
+    for _ in range(2):
+        (oc, op), (gc, gp) = make_pair(rm, oracle, L, N, seed=12, precision=32)
+        entry_id = gp.download("id")
+        rm.bulk_run(gp, gc, rm.Rng(6, 0), 1.0, 3)
+        outs.append({f: gp.download(f) for f in ("pos", "vel", "image", "id")})
+    for f in outs[0]:
+        assert np.array_equal(outs[0][f], outs[1][f]), f
+    ids = outs[0]["id"]
+    where = np.empty(N + 1, np.int64)
+    where[entry_id] = np.arange(N)
+    cnt = gc.cell_count
+    start = gc.cell_start - 1
+    for s in np.nonzero(cnt > 1)[0]:
+        seg = where[ids[start[s]:start[s] + cnt[s]]]
+        assert np.all(np.diff(seg) > 0), f"cell {s}"
+    assert np.array_equal(np.sort(ids), np.arange(1, N + 1))
+
+
 @pytest.mark.parametrize("n_int", [2])
 def test_single_dimer_pbc_bit_exact(rm, oracle, n_int):
     from oracle.programs import SingleDimerPBC as OD
