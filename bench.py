@@ -223,14 +223,21 @@ def dimer_boxes_batched(n=512, seed=2024):
     return [(int(s),) * 3 for s in r.choice([16, 20, 24, 32, 40, 48], size=n)]
 
 
-def dimer_time(rm, dimers, n_intervals, use_graph=True):
+def dimer_time(rm, dimers, n_intervals, use_graph=True, tuned=None):
     """Device time (ms) of n_intervals of a DimerBatch built from `dimers`,
-    after one warm-up interval (which also captures the interval graph)."""
+    on the engine shape its autotuner picks (its tuning intervals are real
+    intervals of the run), after one warm-up interval (which also captures
+    the interval graph).  `tuned`, if a dict, receives the autotuner's
+    choice."""
     from rmpcdmd_b200.programs import DimerBatch
     from rmpcdmd_b200._capi import call
     import ctypes as C
 
     b = DimerBatch(dimers, use_graph=use_graph)
+    res = b.autotune(1)
+    if tuned is not None:
+        prec = int(dimers[0].solvent.precision)
+        tuned.update(res, shape=DimerBatch.shapes(prec)[res["best"]])
     b.run(1)
     rm.synchronize()
     a, e = C.c_int(), C.c_int()
@@ -274,10 +281,14 @@ def run_dimer(rm, peak, peak_kind, local):
     out = {"unit": "particle-steps/s (solvent particles x MD steps / device time, dt = tau/N_MD = 0.01)",
            "data": "synthetic: seeded uniform solvent (rejected inside the colloid cut), Maxwell kT=1/3, "
                    "dimer sigma=2, d=4.5, p(A->B)=1, refuel beyond 0.45 L; list capacity 4000"}
-    ms, N, ex = dimer_time(rm, make([(32, 32, 32)], [SEED], 64), 5)
-    out["single_dimer_32_fp64_plain"] = dict(dimer_entry(N, ms, 5, 64, peak, peak_kind, ex), N=N, replicas=1)
-    ms, N, ex = dimer_time(rm, make([(32, 32, 32)], [SEED], 32), 5)
-    out["single_dimer_32_fp32"] = dict(dimer_entry(N, ms, 5, 32, peak, peak_kind, ex), N=N, replicas=1)
+    tu = {}
+    ms, N, ex = dimer_time(rm, make([(32, 32, 32)], [SEED], 64), 5, tuned=tu)
+    out["single_dimer_32_fp64_plain"] = dict(dimer_entry(N, ms, 5, 64, peak, peak_kind, ex), N=N, replicas=1,
+                                             autotune=tu)
+    tu = {}
+    ms, N, ex = dimer_time(rm, make([(32, 32, 32)], [SEED], 32), 5, tuned=tu)
+    out["single_dimer_32_fp32"] = dict(dimer_entry(N, ms, 5, 32, peak, peak_kind, ex), N=N, replicas=1,
+                                       autotune=tu)
     d = make([(32, 32, 32)], [SEED], 64)[0]
     d.interval()
     rm.synchronize()
@@ -289,14 +300,17 @@ def run_dimer(rm, peak, peak_kind, local):
                                                 "us_per_md_step": round(cbc * 1e6 / DIMER_N_MD, 2),
                                                 "path": "one C-ABI call per module procedure (wall clock)"}
     for prec in (32, 64):
-        ms, N, ex = dimer_time(rm, make([(96, 96, 96)], [SEED], prec), 2)
-        out[f"single_dimer_96_fp{prec}"] = dict(dimer_entry(N, ms, 2, prec, peak, peak_kind, ex), N=N, replicas=1)
+        tu = {}
+        ms, N, ex = dimer_time(rm, make([(96, 96, 96)], [SEED], prec), 2, tuned=tu)
+        out[f"single_dimer_96_fp{prec}"] = dict(dimer_entry(N, ms, 2, prec, peak, peak_kind, ex), N=N, replicas=1,
+                                                autotune=tu)
     boxes = dimer_boxes_batched()
+    tu = {}
     with ClockSampler(local) as cs:
-        ms, N, ex = dimer_time(rm, make(boxes, list(range(1, len(boxes) + 1)), 32), 2)
+        ms, N, ex = dimer_time(rm, make(boxes, list(range(1, len(boxes) + 1)), 32), 2, tuned=tu)
     e = dimer_entry(N, ms, 2, 32, peak, peak_kind, ex)
     e.update(N=N, replicas=len(boxes), boxes="cubic sides drawn from {16,20,24,32,40,48}, seed 2024",
-             clocks=cs.summary())
+             clocks=cs.summary(), autotune=tu)
     # the same replicas one at a time in plain FP64 (a sample of 8)
     seq_ms, seq_N = 0.0, 0
     for k in range(8):

@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <string>
 #include <vector>
 
 #include "keys.cuh"
@@ -42,8 +43,33 @@
 
 namespace rmpcd {
 
-constexpr int kTile = 1024;  // slots per slot tile; most particles per particle tile
+constexpr int kTile = 1024;  // slots per slot tile
 constexpr int kBT = 256;     // threads per tile block
+
+// Engine shapes (rmpcd_dimer_batch_autotune): the particles a thread of the
+// step-begin / step-end kernel handles per pass, the blocks per SM they are
+// compiled for, and (at run time) the particles per tile.  Every shape gives
+// the same results bit for bit: tiles and passes only decide which thread
+// handles which particle, and every per-particle result, the maximum
+// displacement and the re-sort decision are independent of that.
+template <int KB_, int KE_, int MINB_>
+struct BVar {
+    static constexpr int KB = KB_;      // particles per thread and pass, step begin
+    static constexpr int KE = KE_;      // the same, step end
+    static constexpr int MINB = MINB_;  // resident blocks per SM (launch bound)
+};
+template <typename R, int V>
+struct BVarOf;
+template <> struct BVarOf<float, 0> { using T = BVar<4, 4, 4>; };
+template <> struct BVarOf<float, 1> { using T = BVar<2, 4, 4>; };
+template <> struct BVarOf<float, 2> { using T = BVar<4, 2, 4>; };
+template <> struct BVarOf<double, 0> { using T = BVar<2, 4, 4>; };
+template <> struct BVarOf<double, 1> { using T = BVar<1, 4, 4>; };
+template <> struct BVarOf<double, 2> { using T = BVar<2, 2, 4>; };
+constexpr int kBVars = 3;
+constexpr long long kPTiles[] = {256, 512, 1024, 2048, 4096};  // particles per tile
+constexpr int kNPTiles = 5;
+constexpr int kBShapes = kBVars * kNPTiles;  // shape s = variant s / kNPTiles, tile kPTiles[s % kNPTiles]
 
 struct BTile {
     int r;
@@ -76,6 +102,8 @@ struct rmpcd_dimer_batch {
     rmpcd::BRep *rep = nullptr;
     rmpcd::BTile *ptile = nullptr, *stile = nullptr;
     int n_ptile = 0, n_stile = 0;
+    int cap_ptile = 0;  // particle tiles allocated (enough for the smallest tile size)
+    int shape = 0;      // engine shape in use (kernel variant, particles per tile)
     int *stile_first = nullptr, *stile_count = nullptr;  // per replica
     int *ptile_first = nullptr, *ptile_count = nullptr;  // per replica
     int *act_p = nullptr, *act_s = nullptr, *n_act = nullptr;  // tiles of the replicas flagged for a re-sort
@@ -280,8 +308,8 @@ constexpr bool colloid_block_first()
     return sizeof(R) == 8;
 }
 
-template <typename R>
-__global__ void __launch_bounds__(kBT, 4)
+template <typename R, typename V>
+__global__ void __launch_bounds__(kBT, V::MINB)
     kb_step_begin(const BTile *tiles, const BRep *rep, PView<R> v, Vec3<R> old, Vec3<R> next, R dt, R dt_sq,
                   unsigned long long *so_max, unsigned *done, int *resort, int *n_extra, ColloidStep cs,
                   ResortLists rl, cudaGraphConditionalHandle cond, int use_cond, int read_species, unsigned *err)
@@ -297,7 +325,7 @@ __global__ void __launch_bounds__(kBT, 4)
             cs.co_max[r] = colloid_begin(r, rep, cs.c, cs.cold, cs.c_next, cs.rat, cs.mass, cs.ms, cs.d, cs.dt, err);
     double m = 0;
     // K particles per thread and pass, all loads issued before any use
-    constexpr int K = sizeof(R) == 4 ? 4 : 2;
+    constexpr int K = V::KB;
     for (long long base = t.begin + threadIdx.x; base < t.end; base += (long long)K * blockDim.x) {
         int f[K], sp[K];
         R px[K], py[K], pz[K], vx[K], vy[K], vz[K], ox[K], oy[K], oz[K];
@@ -437,8 +465,8 @@ __global__ void kb_apply_sum(const BRep *rep, int R_, int gx, const int *list, c
 // contribution counters; compute_force_n2, the colloid velocity half and
 // RATTLE's velocity correction per replica (src/neighbor_list.f90:227-264,
 // programs/single_dimer_pbc.f90:356-359, src/md.f90:298-319)
-template <typename R>
-__global__ void __launch_bounds__(kBT, 4)
+template <typename R, typename V>
+__global__ void __launch_bounds__(kBT, V::MINB)
     kb_step_end(const BTile *tiles, int n_tiles, int gx, const BRep *rep, PView<R> v, PView<double> c, R dt,
                 double cut_c, double cut_n, double prob, const uint64_t *d_step, int step_off, const int *list,
                 const int *n, int Nmax, const unsigned char *contrib, int *ncontrib, int *max_contrib,
@@ -454,7 +482,7 @@ __global__ void __launch_bounds__(kBT, 4)
         const uint64_t step = *d_step + (uint64_t)step_off;
         const uint64_t seed = rp.seed;
         const long long off = rp.off;
-        constexpr int K = 4;
+        constexpr int K = V::KE;
         // The FP64 form reads every velocity: a zero-force update turns a -0
         // component into +0, as the reference's does.  The FP32 form reads
         // velocities only for particles with a force and leaves the others'
@@ -954,7 +982,7 @@ static void capture_conditional_resort(Batch *b, cudaStream_t st, cudaGraph_t g,
     note(b, cudaStreamEndCapture(b->body, &out));
 }
 
-template <typename R>
+template <typename R, typename V>
 static void md_step_launches(Batch *b, int k)
 {
     cudaStream_t st = stream();
@@ -973,7 +1001,7 @@ static void md_step_launches(Batch *b, int k)
         note(b, cudaStreamGetCaptureInfo(st, &st_cap, nullptr, &g, nullptr, nullptr));
         note(b, cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
     }
-    kb_step_begin<R><<<b->n_ptile + (colloid_block_first<R>() ? 1 : 0), kBT, 0, st>>>(b->ptile, b->rep, s, alt.pos, s.force_old, (R)dt, (R)dt_sq,
+    kb_step_begin<R, V><<<b->n_ptile + (colloid_block_first<R>() ? 1 : 0), kBT, 0, st>>>(b->ptile, b->rep, s, alt.pos, s.force_old, (R)dt, (R)dt_sq,
                                                  b->so_max, b->done, b->resort, b->n_extra, cs,
                                                  ResortLists{b->ptile_first, b->ptile_count, b->stile_first,
                                                              b->stile_count, b->act_p, b->act_s, b->n_act},
@@ -995,7 +1023,7 @@ static void md_step_launches(Batch *b, int k)
         b->rep, b->R, gx, b->list, b->nn, b->Nmax, b->contrib, b->pair_f, b->ncontrib, b->max_contrib, s.force.x,
         s.force.y, s.force.z, c.force.x, c.force.y, c.force.z, b->clist, b->cn);
     const int n_col_blocks = (b->R + kBT - 1) / kBT;
-    kb_step_end<R><<<b->n_ptile + gx * 2 * b->R + n_col_blocks, kBT, 0, st>>>(
+    kb_step_end<R, V><<<b->n_ptile + gx * 2 * b->R + n_col_blocks, kBT, 0, st>>>(
         b->ptile, b->n_ptile, gx, b->rep, s, c, (R)dt, b->prm.cut_sq_C, b->prm.cut_sq_N, b->prm.prob, b->d_step, k,
         b->list, b->nn, b->Nmax, b->contrib, b->ncontrib, b->max_contrib, cs, b->lj_cc, dev_error_word());
 }
@@ -1005,7 +1033,13 @@ static void interval_launches(Batch *b)
 {
     cudaStream_t st = stream();
     const int N_MD = b->prm.N_MD;
-    for (int k = 0; k < N_MD; k++) md_step_launches<R>(b, k);
+    for (int k = 0; k < N_MD; k++) {
+        switch (b->shape / kNPTiles) {
+        case 1: md_step_launches<R, typename BVarOf<R, 1>::T>(b, k); break;
+        case 2: md_step_launches<R, typename BVarOf<R, 2>::T>(b, k); break;
+        default: md_step_launches<R, typename BVarOf<R, 0>::T>(b, k); break;
+        }
+    }
     resort_launches<R>(b, nullptr, true, st, N_MD);
     SrdParams q{};
     q.sin_a = 1;
@@ -1100,6 +1134,39 @@ __global__ void k_any_negative(const int *a, long long n, int *out)
         }
 }
 
+// the particle tiles of every replica at `ptile` particles per tile: tile
+// list, each replica's first tile and count, and the every-tile id list
+static int build_particle_tiles(Batch *b, long long ptile)
+{
+    std::vector<BTile> pt;
+    std::vector<int> pfirst(b->R), pcount(b->R);
+    for (int r = 0; r < b->R; r++) {
+        const BRep &p = b->rep_h[r];
+        pfirst[r] = (int)pt.size();
+        for (long long t = 0; t < p.n; t += ptile)
+            pt.push_back({r, 0, p.off + t, p.off + (t + ptile < p.n ? t + ptile : p.n)});
+        pcount[r] = (int)pt.size() - pfirst[r];
+    }
+    if ((long long)pt.size() > b->cap_ptile)
+        return fail(RMPCD_ERR_CAPACITY, "dimer batch: %zu particle tiles above the %d allocated", pt.size(),
+                    b->cap_ptile);
+    cudaStream_t st = stream();
+    std::vector<int> ids(pt.size());
+    for (size_t k = 0; k < ids.size(); k++) ids[k] = (int)k;
+    const int n = (int)pt.size();
+    if (n) {
+        RMPCD_CUDA_TRY(cudaMemcpyAsync(b->ptile, pt.data(), pt.size() * sizeof(BTile), cudaMemcpyHostToDevice, st));
+        RMPCD_CUDA_TRY(cudaMemcpyAsync(b->all_p, ids.data(), ids.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    }
+    RMPCD_CUDA_TRY(cudaMemcpyAsync(b->ptile_first, pfirst.data(), b->R * sizeof(int), cudaMemcpyHostToDevice, st));
+    RMPCD_CUDA_TRY(cudaMemcpyAsync(b->ptile_count, pcount.data(), b->R * sizeof(int), cudaMemcpyHostToDevice, st));
+    RMPCD_CUDA_TRY(cudaMemcpyAsync(b->n_all, &n, sizeof(int), cudaMemcpyHostToDevice, st));
+    // the host vectors go out of scope: wait for the copies that read them
+    RMPCD_CUDA_TRY(cudaStreamSynchronize(st));
+    b->n_ptile = n;
+    return RMPCD_OK;
+}
+
 // copy one particle system's current arrays (and pos_old) to/from the batch
 // system at offset off; force/force_old follow the batch's parity
 static int move_particles(Batch *b, rmpcd_particles *big, rmpcd_particles *p, long long off, bool to_batch)
@@ -1179,16 +1246,21 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
     b->ms.n = col[0]->n_species;
     for (int s = 0; s < RMPCD_MAX_SPECIES; s++) b->ms.m[s] = col[0]->mass[s];
     // replica layout and tiles
-    // particle tiles: 1024 particles, smaller only for batches too small to
-    // give ~2 tiles per SM: each tile's block is one round trip to DRAM, so
-    // fewer, fuller tiles beat more blocks (one 32^3 dimer: 1024-particle
-    // tiles take the MD step from 45.8 to 38.0 us against 256-particle ones)
+    // default shape: variant 0 and 1024-particle tiles, smaller only for
+    // batches too small to give ~2 tiles per SM: each tile's block is one
+    // round trip to DRAM, so fewer, fuller tiles beat more blocks (one 32^3
+    // dimer: 1024-particle tiles take the MD step from 45.8 to 38.0 us against
+    // 256-particle ones); rmpcd_dimer_batch_autotune times the others
     long long n_total = 0;
     for (int r = 0; r < R; r++) n_total += sol[r]->N;
-    long long ptile = 1024;
-    while (ptile > kBT && n_total / ptile < 2LL * sm_count()) ptile /= 2;
-    std::vector<BTile> pt, stl;
-    std::vector<int> sfirst(R), scount(R), pfirst(R), pcount(R);
+    int tile_k = 2;  // kPTiles[2] = 1024
+    while (tile_k > 0 && n_total / kPTiles[tile_k] < 2LL * sm_count()) tile_k--;
+    b->shape = tile_k;
+    long long cap_p = 0;
+    for (int r = 0; r < R; r++) cap_p += (sol[r]->N + kPTiles[0] - 1) / kPTiles[0];
+    if (cap_p < 1) cap_p = 1;
+    std::vector<BTile> stl;
+    std::vector<int> sfirst(R), scount(R);
     std::map<std::vector<int>, int *> lut_of;
     b->rep_h.resize(R);
     long long off = 0;
@@ -1220,9 +1292,6 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
             lut_of[key] = l;
         }
         p.g.lut = lut_of[key];
-        pfirst[r] = (int)pt.size();
-        for (long long t = 0; t < p.n; t += ptile) pt.push_back({r, 0, off + t, off + (t + ptile < p.n ? t + ptile : p.n)});
-        pcount[r] = (int)pt.size() - pfirst[r];
         sfirst[r] = (int)stl.size();
         for (long long t = 0; t < p.S; t += kTile) stl.push_back({r, 0, soff + t, soff + (t + kTile < p.S ? t + kTile : p.S)});
         scount[r] = (int)stl.size() - sfirst[r];
@@ -1235,10 +1304,10 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
     }
     b->Ntot = off;
     b->Stot = (int)soff;
-    b->n_ptile = (int)pt.size();
+    b->cap_ptile = (int)cap_p;
     b->n_stile = (int)stl.size();
     size_t ne = (size_t)2 * R * b->Nmax;
-    bool ok = !dalloc(&b->rep, R) && !dalloc(&b->ptile, pt.size()) && !dalloc(&b->stile, stl.size()) &&
+    bool ok = !dalloc(&b->rep, R) && !dalloc(&b->ptile, cap_p) && !dalloc(&b->stile, stl.size()) &&
               !dalloc(&b->stile_first, R) && !dalloc(&b->stile_count, R) && !dalloc(&b->tile_sum, stl.size()) &&
               !dalloc(&b->tile_off, stl.size()) && !dalloc(&b->count, soff) && !dalloc(&b->start, soff) &&
               !dalloc(&b->cursor, soff) && !dalloc(&b->is_md, soff) && !dalloc(&b->is_reac, soff) &&
@@ -1251,8 +1320,8 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
               !dalloc(&b->rattle[0], 2 * (size_t)R) && !dalloc(&b->rattle[1], 2 * (size_t)R) &&
               !dalloc(&b->rattle[2], 2 * (size_t)R) && !dalloc(&b->vv_mass, 2 * (size_t)R) && !dalloc(&b->d_step, 1) &&
               !dalloc(&b->done, 1) && cudaStreamCreateWithFlags(&b->body, cudaStreamNonBlocking) == cudaSuccess &&
-              !dalloc(&b->ptile_first, R) && !dalloc(&b->ptile_count, R) && !dalloc(&b->act_p, pt.size()) &&
-              !dalloc(&b->act_s, stl.size()) && !dalloc(&b->n_act, 2) && !dalloc(&b->all_p, pt.size()) &&
+              !dalloc(&b->ptile_first, R) && !dalloc(&b->ptile_count, R) && !dalloc(&b->act_p, cap_p) &&
+              !dalloc(&b->act_s, stl.size()) && !dalloc(&b->n_act, 2) && !dalloc(&b->all_p, cap_p) &&
               !dalloc(&b->all_s, stl.size()) && !dalloc(&b->n_all, 2);
     if (!ok) {
         free_batch(b);
@@ -1274,19 +1343,21 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
         vm[2 * r + 1] = prm->vv_mass[1];
     }
     RMPCD_CUDA_TRY(cudaMemcpyAsync(b->rep, b->rep_h.data(), R * sizeof(BRep), cudaMemcpyHostToDevice, st));
-    RMPCD_CUDA_TRY(cudaMemcpyAsync(b->ptile, pt.data(), pt.size() * sizeof(BTile), cudaMemcpyHostToDevice, st));
     RMPCD_CUDA_TRY(cudaMemcpyAsync(b->stile, stl.data(), stl.size() * sizeof(BTile), cudaMemcpyHostToDevice, st));
     RMPCD_CUDA_TRY(cudaMemcpyAsync(b->stile_first, sfirst.data(), R * sizeof(int), cudaMemcpyHostToDevice, st));
     RMPCD_CUDA_TRY(cudaMemcpyAsync(b->stile_count, scount.data(), R * sizeof(int), cudaMemcpyHostToDevice, st));
-    RMPCD_CUDA_TRY(cudaMemcpyAsync(b->ptile_first, pfirst.data(), R * sizeof(int), cudaMemcpyHostToDevice, st));
-    RMPCD_CUDA_TRY(cudaMemcpyAsync(b->ptile_count, pcount.data(), R * sizeof(int), cudaMemcpyHostToDevice, st));
-    std::vector<int> ids_p(pt.size()), ids_s(stl.size());
-    for (size_t k = 0; k < ids_p.size(); k++) ids_p[k] = (int)k;
+    std::vector<int> ids_s(stl.size());
     for (size_t k = 0; k < ids_s.size(); k++) ids_s[k] = (int)k;
-    const int n_all[2] = {(int)pt.size(), (int)stl.size()}, n_none[2] = {0, 0};
-    RMPCD_CUDA_TRY(cudaMemcpyAsync(b->all_p, ids_p.data(), ids_p.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    const int n_all[2] = {0, (int)stl.size()}, n_none[2] = {0, 0};
     RMPCD_CUDA_TRY(cudaMemcpyAsync(b->all_s, ids_s.data(), ids_s.size() * sizeof(int), cudaMemcpyHostToDevice, st));
     RMPCD_CUDA_TRY(cudaMemcpyAsync(b->n_all, n_all, sizeof(n_all), cudaMemcpyHostToDevice, st));
+    {
+        int rc = build_particle_tiles(b, kPTiles[b->shape % kNPTiles]);
+        if (rc) {
+            free_batch(b);
+            return rc;
+        }
+    }
     RMPCD_CUDA_TRY(cudaMemcpyAsync(b->n_act, n_none, sizeof(n_none), cudaMemcpyHostToDevice, st));
     RMPCD_CUDA_TRY(cudaMemcpyAsync(b->vv_mass, vm.data(), vm.size() * sizeof(double), cudaMemcpyHostToDevice, st));
     RMPCD_CUDA_TRY(cudaMemcpyAsync(b->d_step, &b->step, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
@@ -1369,11 +1440,155 @@ static int scatter(Batch *b, int r, rmpcd_particles *sol, rmpcd_particles *col, 
     return sync();
 }
 
+// shape in use <- s: kernel variant and particle tiles; the captured interval
+// graphs hold the old launches and are dropped (captured again on the next run)
+static int set_shape(Batch *b, int s)
+{
+    RMPCD_CUDA_TRY(cudaStreamSynchronize(stream()));
+    int rc = build_particle_tiles(b, kPTiles[s % kNPTiles]);
+    if (rc) return rc;
+    for (auto &e : b->exec)
+        if (e) {
+            cudaGraphExecDestroy(e);
+            e = nullptr;
+        }
+    b->shape = s;
+    return RMPCD_OK;
+}
+
+// chosen shapes per GPU, precision, N_MD and mix of boxes
+static std::map<std::string, int> g_batch_tuned;
+
+static std::string tune_key(const Batch *b)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::map<std::vector<int>, int> mix;
+    for (const BRep &p : b->rep_h) mix[{p.g.L[0], p.g.L[1], p.g.L[2]}]++;
+    std::string k = std::to_string(dev) + ":" + std::to_string(b->precision) + ":" + std::to_string(b->prm.N_MD);
+    for (auto &m : mix)
+        k += ":" + std::to_string(m.first[0]) + "x" + std::to_string(m.first[1]) + "x" + std::to_string(m.first[2]) +
+             "*" + std::to_string(m.second);
+    return k;
+}
+
+static int run_any(Batch *b, int n)
+{
+    if (b->precision == RMPCD_FP32) return run_t<float>(b, n);
+    return run_t<double>(b, n);
+}
+
+static int autotune(Batch *b, int n_intervals, int *best, float *ms, int *ran)
+{
+    *ran = 0;
+    const std::string key = tune_key(b);
+    auto hit = g_batch_tuned.find(key);
+    if (hit != g_batch_tuned.end()) {
+        *best = hit->second;
+        if (ms)
+            for (int k = 0; k < kBShapes; k++) ms[k] = -1.0f;
+        return set_shape(b, hit->second);
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    RMPCD_CUDA_TRY(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(RMPCD_ERR_CUDA, "dimer batch autotune: event creation failed");
+    }
+    int rc = RMPCD_OK, b_best = b->shape;
+    float best_ms = 0;
+    for (int k = 0; k < kBShapes && !rc; k++) {
+        rc = set_shape(b, k);
+        // one interval captures the shape's graph and warms it up; then the
+        // timed ones
+        if (!rc) rc = run_any(b, 1);
+        if (!rc && cudaEventRecord(e0, stream()) != cudaSuccess) rc = fail(RMPCD_ERR_CUDA, "event record");
+        if (!rc) rc = run_any(b, n_intervals);
+        if (!rc && cudaEventRecord(e1, stream()) != cudaSuccess) rc = fail(RMPCD_ERR_CUDA, "event record");
+        float t = 0;
+        if (!rc && (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&t, e0, e1) != cudaSuccess))
+            rc = fail(RMPCD_ERR_CUDA, "dimer batch autotune: event timing failed");
+        if (rc) break;
+        *ran += 1 + n_intervals;
+        t /= (float)n_intervals;
+        if (ms) ms[k] = t;
+        if (k == 0 || t < best_ms) {
+            best_ms = t;
+            b_best = k;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    g_batch_tuned[key] = b_best;
+    *best = b_best;
+    return set_shape(b, b_best);
+}
+
 }  // namespace rmpcd
 
 using namespace rmpcd;
 
 extern "C" {
+
+int rmpcd_dimer_batch_shapes(int precision, int *n_shapes)
+{
+    RMPCD_ARG(n_shapes, "null argument");
+    RMPCD_ARG(precision == RMPCD_FP32 || precision == RMPCD_FP64, "precision must be RMPCD_FP32 or RMPCD_FP64");
+    *n_shapes = kBShapes;
+    return RMPCD_OK;
+}
+
+int rmpcd_dimer_batch_shape_info(int precision, int shape, int *particles_per_tile, int *per_thread_begin,
+                                 int *per_thread_end, int *blocks_per_sm)
+{
+    RMPCD_ARG(precision == RMPCD_FP32 || precision == RMPCD_FP64, "precision must be RMPCD_FP32 or RMPCD_FP64");
+    RMPCD_ARG(shape >= 0 && shape < kBShapes, "no such engine shape");
+    int kb, ke, mb;
+    const int v = shape / kNPTiles;
+    if (precision == RMPCD_FP32) {
+        using V0 = BVarOf<float, 0>::T;
+        using V1 = BVarOf<float, 1>::T;
+        using V2 = BVarOf<float, 2>::T;
+        kb = v == 0 ? V0::KB : v == 1 ? V1::KB : V2::KB;
+        ke = v == 0 ? V0::KE : v == 1 ? V1::KE : V2::KE;
+        mb = v == 0 ? V0::MINB : v == 1 ? V1::MINB : V2::MINB;
+    } else {
+        using V0 = BVarOf<double, 0>::T;
+        using V1 = BVarOf<double, 1>::T;
+        using V2 = BVarOf<double, 2>::T;
+        kb = v == 0 ? V0::KB : v == 1 ? V1::KB : V2::KB;
+        ke = v == 0 ? V0::KE : v == 1 ? V1::KE : V2::KE;
+        mb = v == 0 ? V0::MINB : v == 1 ? V1::MINB : V2::MINB;
+    }
+    if (particles_per_tile) *particles_per_tile = (int)kPTiles[shape % kNPTiles];
+    if (per_thread_begin) *per_thread_begin = kb;
+    if (per_thread_end) *per_thread_end = ke;
+    if (blocks_per_sm) *blocks_per_sm = mb;
+    return RMPCD_OK;
+}
+
+int rmpcd_dimer_batch_set_shape(rmpcd_dimer_batch *b, int shape)
+{
+    RMPCD_ARG(b, "null argument");
+    RMPCD_ARG(shape >= 0 && shape < kBShapes, "no such engine shape");
+    return set_shape(b, shape);
+}
+
+int rmpcd_dimer_batch_get_shape(const rmpcd_dimer_batch *b, int *shape)
+{
+    RMPCD_ARG(b && shape, "null argument");
+    *shape = b->shape;
+    return RMPCD_OK;
+}
+
+int rmpcd_dimer_batch_autotune(rmpcd_dimer_batch *b, int n_intervals, int *best, float *ms_per_interval,
+                               int *intervals_run)
+{
+    RMPCD_ARG(b && best && intervals_run, "null argument");
+    RMPCD_ARG(n_intervals >= 1, "n_intervals must be >= 1");
+    return autotune(b, n_intervals, best, ms_per_interval, intervals_run);
+}
 
 int rmpcd_dimer_batch_create(rmpcd_dimer_batch **out, int n_replicas, rmpcd_particles *const *solvent,
                              rmpcd_particles *const *colloids, rmpcd_cells *const *cells,

@@ -245,6 +245,43 @@ class DimerBatch:
         call("rmpcd_dimer_batch_info", self._h, None, None, out.ctypes.data_as(C.POINTER(C.c_int)))
         return out
 
+    @staticmethod
+    def shapes(precision: int = A.FP32) -> list[dict]:
+        """The engine shapes rmpcd_dimer_batch_autotune chooses from."""
+        n = C.c_int()
+        call("rmpcd_dimer_batch_shapes", int(precision), C.byref(n))
+        out = []
+        for k in range(n.value):
+            v = [C.c_int() for _ in range(4)]
+            call("rmpcd_dimer_batch_shape_info", int(precision), k, *[C.byref(x) for x in v])
+            out.append(dict(particles_per_tile=v[0].value, per_thread_begin=v[1].value,
+                            per_thread_end=v[2].value, blocks_per_sm=v[3].value))
+        return out
+
+    @property
+    def shape(self) -> int:
+        s = C.c_int()
+        call("rmpcd_dimer_batch_get_shape", self._h, C.byref(s))
+        return s.value
+
+    @shape.setter
+    def shape(self, k: int) -> None:
+        call("rmpcd_dimer_batch_set_shape", self._h, int(k))
+
+    def autotune(self, n_intervals: int = 1) -> dict:
+        """rmpcd_dimer_batch_autotune: every engine shape runs 1 + n_intervals
+        real intervals of this batch (the results do not depend on the
+        shape) and the fastest is kept; a batch of a kind already tuned takes
+        the remembered choice without running.  Returns the choice, the
+        milliseconds per interval of each shape (-1 when remembered) and the
+        intervals every replica advanced by."""
+        n = C.c_int()
+        call("rmpcd_dimer_batch_shapes", int(self.dimers[0].solvent.precision), C.byref(n))
+        ms = (C.c_float * n.value)()
+        best, ran = C.c_int(), C.c_int()
+        call("rmpcd_dimer_batch_autotune", self._h, int(n_intervals), C.byref(best), ms, C.byref(ran))
+        return dict(best=best.value, ms_per_interval=[round(float(x), 4) for x in ms], intervals_run=ran.value)
+
     def scatter(self, r: int, dimer: SingleDimerPBC | None = None) -> SingleDimerPBC:
         """Copy replica r into the handles of ``dimer`` (its own driver by default)."""
         d = dimer if dimer is not None else self.dimers[r]

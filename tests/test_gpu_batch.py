@@ -86,3 +86,62 @@ def test_batch_rejects_mixed_inputs(rm):
     c[0].rng.step = 5
     with pytest.raises(rm.RmpcdError):
         DimerBatch(a + c)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_every_engine_shape_gives_the_same_results(rm, precision):
+    """The autotuner's choices (particles per tile, per thread, blocks per SM)
+    only decide which thread handles which particle: every shape ends bit
+    for bit where the default shape ends, the shape switched between
+    intervals included."""
+    from rmpcdmd_b200.programs import DimerBatch
+
+    boxes, seeds = [(10, 10, 10), (12, 11, 14), (16, 12, 12)], [4, 18, 102]
+    shapes = DimerBatch.shapes(precision)
+    assert len(shapes) >= 8 and len({s["particles_per_tile"] for s in shapes}) >= 3
+    ref = drivers(rm, boxes, seeds, precision, 10)
+    batch_ref = DimerBatch(ref)
+    batch_ref.run(2)
+    for r in range(len(ref)):
+        batch_ref.scatter(r)
+    for k in range(len(shapes)):
+        mine = drivers(rm, boxes, seeds, precision, 10)
+        batch = DimerBatch(mine)
+        batch.shape = k
+        assert batch.shape == k
+        batch.run(1)
+        batch.shape = (k + 1) % len(shapes)
+        batch.run(1)
+        for r in range(len(mine)):
+            batch.scatter(r)
+            assert_dimers_equal(ref[r], mine[r])
+    rm.get_status()
+
+
+def test_engine_autotune_runs_real_intervals_and_remembers(rm):
+    """rmpcd_dimer_batch_autotune advances the batch by real intervals (the
+    state equals that of the same number of plain intervals), keeps the
+    fastest shape, and a second batch of the same kind takes the remembered
+    choice without running."""
+    from rmpcdmd_b200.programs import DimerBatch
+
+    boxes, seeds = [(12, 12, 12), (10, 10, 10)], [7, 8]
+    tuned = drivers(rm, boxes, seeds, 32, 10)
+    bt = DimerBatch(tuned)
+    res = bt.autotune(1)
+    n = len(DimerBatch.shapes(32))
+    assert res["intervals_run"] == 2 * n
+    assert 0 <= res["best"] < n and bt.shape == res["best"]
+    assert all(m > 0 for m in res["ms_per_interval"])
+    assert res["ms_per_interval"][res["best"]] == min(res["ms_per_interval"])
+    plain = drivers(rm, boxes, seeds, 32, 10)
+    bp = DimerBatch(plain)
+    bp.run(res["intervals_run"])
+    for r in range(len(boxes)):
+        bt.scatter(r)
+        bp.scatter(r)
+        assert_dimers_equal(tuned[r], plain[r])
+    again = DimerBatch(drivers(rm, boxes, seeds, 32, 10))
+    res2 = again.autotune(1)
+    assert res2["intervals_run"] == 0 and res2["best"] == res["best"] and again.shape == res["best"]
+    rm.get_status()
