@@ -118,6 +118,68 @@ def propulsion_check(L=32, replicas=32, n_intervals=60, skip=10, seed0=1000):
                 rel_err=err / abs(p64["v_prop"]) if p64["v_prop"] else None)
 
 
+def _unwrapped(d: SingleDimerPBC):
+    return d.colloids.download("pos") + d.colloids.download("image") * d.edges
+
+
+def _sync_twin(twin: SingleDimerPBC, d: SingleDimerPBC) -> None:
+    """twin (FP32 solvent) <- the state of d (FP64) at an interval boundary:
+    every solvent array rounded to single precision, the colloids as they
+    are, the grid origin and the random-number step; then the re-sort the
+    program makes at that point (sort, neighbor list, pos_old), so the
+    twin's cells and list are those of its own rounded positions."""
+    for f in ("pos", "vel", "force", "force_old", "image", "id", "species", "flags"):
+        twin.solvent.upload(f, d.solvent.download(f))
+    for f in ("pos", "vel", "force", "force_old", "image", "species"):
+        twin.colloids.upload(f, d.colloids.download(f))
+    twin.cells.origin = d.cells.origin
+    twin.rng.step = d.rng.step
+    twin._resort()
+
+
+def paired_propulsion_check(L=16, replicas=8, n_intervals=40, skip=3, seed0=2000):
+    """The FP32 form's bias on the propulsion velocity, paired: at every
+    interval boundary of plain FP64 runs an FP32 twin takes the FP64 state
+    (rounded), both run the same interval with the same random numbers, and
+    the difference of their dimer displacements along the bond is recorded.
+    The two share their noise for the interval, so the mean difference -- the
+    FP32 bias per interval -- is resolved far below the propulsion velocity's
+    own statistical error (programs/single_dimer_pbc.f90:364-369)."""
+    d64 = [SingleDimerPBC(L=(L, L, L), rho=10, N_MD=100, seed=seed0 + k, list_capacity=4000,
+                          precision=A.FP64) for k in range(replicas)]
+    tw = [SingleDimerPBC(L=(L, L, L), rho=10, N_MD=100, seed=seed0 + k, list_capacity=4000,
+                         precision=A.FP32) for k in range(replicas)]
+    for d in d64:
+        for _ in range(skip):
+            d.interval()
+    disp64 = np.zeros((replicas, n_intervals))
+    delta = np.zeros((replicas, n_intervals))
+    for t in range(n_intervals):
+        for r in range(replicas):
+            d, w = d64[r], tw[r]
+            _sync_twin(w, d)
+            x0 = _unwrapped(d)
+            u = x0[0] - x0[1]
+            u = u / np.linalg.norm(u)
+            c0 = (x0[0] + x0[1]) / 2
+            d.interval()
+            w.interval()
+            a = float(((_unwrapped(d)[0] + _unwrapped(d)[1]) / 2 - c0) @ u)
+            b = float(((_unwrapped(w)[0] + _unwrapped(w)[1]) / 2 - c0) @ u)
+            disp64[r, t] = a
+            delta[r, t] = b - a
+    n = delta.size
+    bias = float(delta.mean())
+    # replicas are independent; intervals of one replica are nearly so for
+    # the paired difference (the twin restarts from the FP64 state each time)
+    bias_err = float(delta.std(ddof=1) / np.sqrt(n))
+    v = float(disp64.mean())
+    v_err = float(disp64.mean(axis=1).std(ddof=1) / np.sqrt(replicas)) if replicas > 1 else float("nan")
+    return dict(L=L, replicas=replicas, intervals=n_intervals, skipped=skip, samples=n, bias=bias,
+                bias_err=bias_err, delta_std=float(delta.std(ddof=1)), delta_abs_max=float(np.abs(delta).max()),
+                v_prop_fp64=v, v_prop_fp64_err=v_err)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--quick", action="store_true", help="small sizes (a minute)")
@@ -125,10 +187,12 @@ def main(argv=None):
     t0 = time.perf_counter()
     if a.quick:
         out = dict(bulk=bulk_check(L=24, n_intervals=20),
-                   propulsion=propulsion_check(L=16, replicas=16, n_intervals=30, skip=5))
+                   propulsion=propulsion_check(L=16, replicas=16, n_intervals=30, skip=5),
+                   paired=paired_propulsion_check(L=16, replicas=8, n_intervals=20, skip=3))
     else:
         out = dict(bulk=bulk_check(L=48, n_intervals=50),
-                   propulsion=propulsion_check(L=32, replicas=64, n_intervals=200, skip=20))
+                   propulsion=propulsion_check(L=32, replicas=64, n_intervals=200, skip=20),
+                   paired=paired_propulsion_check(L=32, replicas=16, n_intervals=40, skip=5))
     out["seconds"] = round(time.perf_counter() - t0, 1)
     print(json.dumps(out))
     return out

@@ -1,7 +1,7 @@
 """The FP32-solvent form against the plain FP64 form on the quantities the
 physics fixes (rmpcdmd_b200.validate): momentum conservation per MPCD
-interval, temperature, the velocity autocorrelation, and the dimer's
-propulsion velocity within its statistical error."""
+interval, temperature, the velocity autocorrelation, and the FP32 bias on
+the dimer's propulsion velocity (paired with FP64 runs)."""
 import numpy as np
 import pytest
 
@@ -24,9 +24,21 @@ def test_bulk_fp32_against_fp64():
     assert r["vacf_max_abs_diff"] < 5 * r["vacf_stat_err"] + 1e-3
 
 
-def test_dimer_propulsion_fp32_against_fp64():
-    from rmpcdmd_b200.validate import propulsion_check
+# the dimer's propulsion velocity in plain FP64 (32^3, 64 replicas x 180
+# intervals of tau = 1): 0.00376 +- 0.00073; the bound below uses 0.003
+V_PROP_SCALE = 0.003
 
-    r = propulsion_check(L=16, replicas=16, n_intervals=30, skip=5)
-    assert np.isfinite(r["fp32"]["v_prop"]) and np.isfinite(r["fp64"]["v_prop"])
-    assert abs(r["diff"]) < 4 * r["diff_err"]
+
+def test_dimer_propulsion_fp32_bias_is_below_one_percent():
+    """Paired estimator: at every interval boundary of FP64 runs an FP32 twin
+    takes the (rounded) FP64 state and both run the same interval with the
+    same random numbers; the mean difference of their displacements along the
+    bond is the FP32 form's bias on the propulsion velocity, resolved far
+    below the 1 % target (the unpaired difference of two ensembles would need
+    ~10^6 GPU-seconds for that)."""
+    from rmpcdmd_b200.validate import paired_propulsion_check
+
+    r = paired_propulsion_check(L=16, replicas=4, n_intervals=10, skip=2)
+    assert r["samples"] == 40
+    assert r["delta_std"] < 1e-5  # the pair shares its noise
+    assert abs(r["bias"]) + 3 * r["bias_err"] < 0.01 * V_PROP_SCALE
