@@ -223,6 +223,13 @@ def dimer_boxes_batched(n=512, seed=2024):
     return [(int(s),) * 3 for s in r.choice([16, 20, 24, 32, 40, 48], size=n)]
 
 
+def shard(items, rank, world):
+    """The replicas rank `rank` of `world` runs: every world-th one from
+    `rank` on, so the ranks split a replica ensemble with no overlap and the
+    box mix stays alike on every rank."""
+    return list(items)[rank::world]
+
+
 def dimer_time(rm, dimers, n_intervals, use_graph=True, tuned=None):
     """Device time (ms) of n_intervals of a DimerBatch built from `dimers`,
     on the engine shape its autotuner picks (its tuning intervals are real
@@ -267,12 +274,20 @@ def dimer_entry(N, ms, n_intervals, precision, peak, peak_kind, extra=None):
     return out
 
 
-def run_dimer(rm, peak, peak_kind, local):
+def run_dimer(rm, peak, peak_kind, local, dist=None, rank=0, world=1):
     """single_dimer_pbc through the batched engine: one dimer at 32^3 (plain
     FP64, FP32 solvent, and the call-by-call driver for comparison), one at
     96^3 (FP32 solvent and FP64), and 512 replicas with uneven boxes (FP32
-    solvent)."""
+    solvent).  With N ranks the single dimers run as one independent replica
+    per rank and the 512 replicas are split between the ranks (`shard`);
+    times are the maximum over ranks and rates count every rank's
+    particles."""
     from rmpcdmd_b200.programs import SingleDimerPBC
+
+    def timed(*a, **k):
+        barrier(dist)
+        ms, N, ex = dimer_time(rm, *a, **k)
+        return max_over_ranks(dist, ms), N * world, ex
 
     def make(boxes, seeds, precision):
         return [SingleDimerPBC(L=L, rho=RHO, N_MD=DIMER_N_MD, seed=s, list_capacity=DIMER_LIST_CAPACITY,
@@ -282,11 +297,11 @@ def run_dimer(rm, peak, peak_kind, local):
            "data": "synthetic: seeded uniform solvent (rejected inside the colloid cut), Maxwell kT=1/3, "
                    "dimer sigma=2, d=4.5, p(A->B)=1, refuel beyond 0.45 L; list capacity 4000"}
     tu = {}
-    ms, N, ex = dimer_time(rm, make([(32, 32, 32)], [SEED], 64), 5, tuned=tu)
+    ms, N, ex = timed(make([(32, 32, 32)], [SEED], 64), 5, tuned=tu)
     out["single_dimer_32_fp64_plain"] = dict(dimer_entry(N, ms, 5, 64, peak, peak_kind, ex), N=N, replicas=1,
                                              autotune=tu)
     tu = {}
-    ms, N, ex = dimer_time(rm, make([(32, 32, 32)], [SEED], 32), 5, tuned=tu)
+    ms, N, ex = timed(make([(32, 32, 32)], [SEED], 32), 5, tuned=tu)
     out["single_dimer_32_fp32"] = dict(dimer_entry(N, ms, 5, 32, peak, peak_kind, ex), N=N, replicas=1,
                                        autotune=tu)
     d = make([(32, 32, 32)], [SEED], 64)[0]
@@ -295,30 +310,37 @@ def run_dimer(rm, peak, peak_kind, local):
     t0 = time.perf_counter()
     d.interval()
     rm.synchronize()
-    cbc = time.perf_counter() - t0
+    cbc = max_over_ranks(dist, time.perf_counter() - t0)
     out["single_dimer_32_fp64_call_by_call"] = {"value": N * DIMER_N_MD / cbc,
                                                 "us_per_md_step": round(cbc * 1e6 / DIMER_N_MD, 2),
                                                 "path": "one C-ABI call per module procedure (wall clock)"}
     for prec in (32, 64):
         tu = {}
-        ms, N, ex = dimer_time(rm, make([(96, 96, 96)], [SEED], prec), 2, tuned=tu)
+        ms, N, ex = timed(make([(96, 96, 96)], [SEED], prec), 2, tuned=tu)
         out[f"single_dimer_96_fp{prec}"] = dict(dimer_entry(N, ms, 2, prec, peak, peak_kind, ex), N=N, replicas=1,
                                                 autotune=tu)
-    boxes = dimer_boxes_batched()
+    boxes_all = dimer_boxes_batched()
+    mine = shard(zip(boxes_all, range(1, len(boxes_all) + 1)), rank, world)
+    boxes = [b for b, _ in mine]
     tu = {}
     with ClockSampler(local) as cs:
-        ms, N, ex = dimer_time(rm, make(boxes, list(range(1, len(boxes) + 1)), 32), 2, tuned=tu)
+        barrier(dist)
+        ms, N, ex = dimer_time(rm, make(boxes, [sd for _, sd in mine], 32), 2, tuned=tu)
+        ms = max_over_ranks(dist, ms)
+        N = int(round(sum_over_ranks(dist, N)))
     e = dimer_entry(N, ms, 2, 32, peak, peak_kind, ex)
-    e.update(N=N, replicas=len(boxes), boxes="cubic sides drawn from {16,20,24,32,40,48}, seed 2024",
-             clocks=cs.summary(), autotune=tu)
+    e.update(N=N, replicas=len(boxes_all), replicas_per_rank=len(boxes),
+             boxes="cubic sides drawn from {16,20,24,32,40,48}, seed 2024", clocks=cs.summary(), autotune=tu)
     # the same replicas one at a time in plain FP64 (a sample of 8)
     seq_ms, seq_N = 0.0, 0
     for k in range(8):
         m1, n1, _ = dimer_time(rm, make([boxes[k]], [k + 1], 64), 1)
         seq_ms += m1
         seq_N += n1
+    seq_ms = max_over_ranks(dist, seq_ms)
+    seq_N = int(round(sum_over_ranks(dist, seq_N)))
     e["fp64_plain_one_replica_at_a_time"] = {"value": seq_N * DIMER_N_MD / (seq_ms * 1e-3),
-                                             "sample": "replicas 0-7, one interval each"}
+                                             "sample": "8 replicas of each rank's share, one interval each"}
     e["batched_over_sequential_fp64"] = round(e["value"] / e["fp64_plain_one_replica_at_a_time"]["value"], 3)
     out["batched_512_fp32"] = e
     # n_colloids_pbc: 200 passive colloids (sigma 3) in 128^3, the program's
@@ -333,12 +355,13 @@ def run_dimer(rm, peak, peak_kind, local):
         # clock carries host noise: best of three 2-interval runs
         sec = float("inf")
         for _ in range(3):
+            barrier(dist)
             t0 = time.perf_counter()
             g.thermalise(2)
             rm.synchronize()
-            sec = min(sec, (time.perf_counter() - t0) / 2)
+            sec = min(sec, max_over_ranks(dist, (time.perf_counter() - t0) / 2))
         out[f"n_colloids_128_fp{prec}"] = {
-            "value": g.N * DIMER_N_MD / sec, "us_per_md_step": round(sec * 1e6 / DIMER_N_MD, 2), "N": g.N,
+            "value": world * g.N * DIMER_N_MD / sec, "us_per_md_step": round(sec * 1e6 / DIMER_N_MD, 2), "N": g.N,
             "colloids": 200, "n_extra_sorting": g.n_extra_sorting,
             "path": "rmpcd_ncolloids_run (the program's calls issued in C; wall clock, best of 3 runs of 2 "
                     "thermostatted intervals)"}
@@ -346,9 +369,9 @@ def run_dimer(rm, peak, peak_kind, local):
             t0 = time.perf_counter()
             g.interval(True, g.T_init)
             rm.synchronize()
-            sec = time.perf_counter() - t0
+            sec = max_over_ranks(dist, time.perf_counter() - t0)
             out["n_colloids_128_fp64_call_by_call"] = {
-                "value": g.N * DIMER_N_MD / sec, "us_per_md_step": round(sec * 1e6 / DIMER_N_MD, 2),
+                "value": world * g.N * DIMER_N_MD / sec, "us_per_md_step": round(sec * 1e6 / DIMER_N_MD, 2),
                 "path": "one C-ABI call per module procedure from Python (wall clock)"}
         del g
     return out
@@ -454,6 +477,16 @@ def max_over_ranks(dist, x):
     return float(t.item())
 
 
+def sum_over_ranks(dist, x):
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def barrier(dist):
     if dist is not None:
         dist.barrier()
@@ -549,7 +582,7 @@ def run_ours(args):
         for r in (r32, r64):
             r.pop("p", None)
             r.pop("cells", None)
-        out["dimer"] = run_dimer(rm, peak, peak_kind, local)
+        out["dimer"] = run_dimer(rm, peak, peak_kind, local, dist, rank, world)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_sample()
     if rank == 0:

@@ -64,3 +64,16 @@ def test_reference_arm_under_torchrun_prints_one_line():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_replica_ensemble_is_split_between_ranks_without_overlap():
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    boxes = bench.dimer_boxes_batched()
+    items = list(zip(boxes, range(1, len(boxes) + 1)))
+    for world in (1, 2, 4, 8):
+        parts = [bench.shard(items, r, world) for r in range(world)]
+        seeds = sorted(sd for p in parts for _, sd in p)
+        assert seeds == list(range(1, 513))
+        assert max(len(p) for p in parts) - min(len(p) for p in parts) <= 1
