@@ -484,19 +484,22 @@ int rmpcd_dimer_batch_info(const rmpcd_dimer_batch *batch, int *n_replicas, long
                            int *n_extra_sorting);
 /* Engine shapes (no counterpart in the reference): particles per tile of
  * the solvent kernels, particles per thread and pass of the MD step's
- * begin / end kernels, and the blocks per SM they are compiled for.  Every
- * shape gives the same results bit for bit.  A batch starts on 1024-particle
- * tiles (smaller when that gives fewer than ~2 tiles per SM). */
+ * begin / end kernels, the blocks per SM they are compiled for, and the
+ * list entries per thread of the list kernels (pair forces, their
+ * application, the contribution reset).  Every shape gives the same results
+ * bit for bit.  A batch starts on 1024-particle tiles (smaller when that
+ * gives fewer than ~2 tiles per SM) and one list entry per thread. */
 int rmpcd_dimer_batch_shapes(int precision, int *n_shapes);
 int rmpcd_dimer_batch_shape_info(int precision, int shape, int *particles_per_tile, int *per_thread_begin,
-                                 int *per_thread_end, int *blocks_per_sm);
+                                 int *per_thread_end, int *blocks_per_sm, int *list_entries_per_thread);
 int rmpcd_dimer_batch_set_shape(rmpcd_dimer_batch *batch, int shape);
 int rmpcd_dimer_batch_get_shape(const rmpcd_dimer_batch *batch, int *shape);
-/* The engine's autotuner: every shape in turn runs one interval (capture and
- * warm-up) and n_intervals timed intervals of the batch itself -- real
- * intervals of the run, since every shape gives the same results -- and the
- * fastest is kept (*best; ms_per_interval, if not NULL, receives the time of
- * each of the n_shapes).  The choice is remembered per GPU, precision, N_MD
+/* The engine's autotuner: every tile size and kernel variant with one list
+ * entry per thread, then the fastest of them with each other list setting,
+ * runs one interval (capture and warm-up) and n_intervals timed intervals of
+ * the batch itself -- real intervals of the run, since every shape gives the
+ * same results -- and the fastest is kept (*best; ms_per_interval, if not
+ * NULL, receives the time of each of the n_shapes, -1 for those not run).  The choice is remembered per GPU, precision, N_MD
  * and mix of boxes: a later batch of the same kind takes it without running
  * anything (*intervals_run = 0, ms_per_interval entries -1).
  * *intervals_run = the intervals the call advanced every replica by. */

@@ -69,7 +69,17 @@ template <> struct BVarOf<double, 2> { using T = BVar<2, 2, 4>; };
 constexpr int kBVars = 3;
 constexpr long long kPTiles[] = {256, 512, 1024, 2048, 4096};  // particles per tile
 constexpr int kNPTiles = 5;
-constexpr int kBShapes = kBVars * kNPTiles;  // shape s = variant s / kNPTiles, tile kPTiles[s % kNPTiles]
+// list entries per thread of the list kernels (pair forces, their
+// application, the contribution reset): their blocks per colloid are
+// ceil(capacity / (256 x this)), at most 64
+constexpr int kListPer[] = {1, 4};
+constexpr int kNListPer = 2;
+constexpr int kBShapes = kNListPer * kBVars * kNPTiles;
+// shape s: particle tile kPTiles[s % kNPTiles], kernel variant
+// (s / kNPTiles) % kBVars, list entries per thread kListPer[s / (kNPTiles * kBVars)]
+__host__ __device__ inline int shape_tile(int s) { return s % kNPTiles; }
+__host__ __device__ inline int shape_var(int s) { return (s / kNPTiles) % kBVars; }
+__host__ __device__ inline int shape_list(int s) { return s / (kNPTiles * kBVars); }
 
 struct BTile {
     int r;
@@ -1014,8 +1024,10 @@ static void md_step_launches(Batch *b, int k)
     s = live<R>(b->sol, b->parity);
     c = live<double>(b->col, b->parity);
     cs.c = c;
-    int gx = (b->Nmax + 255) / 256;
+    const int per = 256 * kListPer[shape_list(b->shape)];
+    int gx = (b->Nmax + per - 1) / per;
     if (gx > 64) gx = 64;
+    if (gx < 1) gx = 1;
     kb_pair_forces<R><<<dim3(gx, 2 * b->R), 256, 0, st>>>(b->rep, c, s, b->list, b->nn, b->Nmax, b->lj_sc, b->pair_f,
                                                           b->pair_e, b->contrib, b->ncontrib, b->max_contrib,
                                                           b->prm.cut_sq_C);
@@ -1034,7 +1046,7 @@ static void interval_launches(Batch *b)
     cudaStream_t st = stream();
     const int N_MD = b->prm.N_MD;
     for (int k = 0; k < N_MD; k++) {
-        switch (b->shape / kNPTiles) {
+        switch (shape_var(b->shape)) {
         case 1: md_step_launches<R, typename BVarOf<R, 1>::T>(b, k); break;
         case 2: md_step_launches<R, typename BVarOf<R, 2>::T>(b, k); break;
         default: md_step_launches<R, typename BVarOf<R, 0>::T>(b, k); break;
@@ -1352,7 +1364,7 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
     RMPCD_CUDA_TRY(cudaMemcpyAsync(b->all_s, ids_s.data(), ids_s.size() * sizeof(int), cudaMemcpyHostToDevice, st));
     RMPCD_CUDA_TRY(cudaMemcpyAsync(b->n_all, n_all, sizeof(n_all), cudaMemcpyHostToDevice, st));
     {
-        int rc = build_particle_tiles(b, kPTiles[b->shape % kNPTiles]);
+        int rc = build_particle_tiles(b, kPTiles[shape_tile(b->shape)]);
         if (rc) {
             free_batch(b);
             return rc;
@@ -1445,7 +1457,7 @@ static int scatter(Batch *b, int r, rmpcd_particles *sol, rmpcd_particles *col, 
 static int set_shape(Batch *b, int s)
 {
     RMPCD_CUDA_TRY(cudaStreamSynchronize(stream()));
-    int rc = build_particle_tiles(b, kPTiles[s % kNPTiles]);
+    int rc = build_particle_tiles(b, kPTiles[shape_tile(s)]);
     if (rc) return rc;
     for (auto &e : b->exec)
         if (e) {
@@ -1497,7 +1509,17 @@ static int autotune(Batch *b, int n_intervals, int *best, float *ms, int *ran)
     }
     int rc = RMPCD_OK, b_best = b->shape;
     float best_ms = 0;
-    for (int k = 0; k < kBShapes && !rc; k++) {
+    if (ms)
+        for (int k = 0; k < kBShapes; k++) ms[k] = -1.0f;
+    // every tile size and kernel variant with one list entry per thread,
+    // then the best of them with each other list setting
+    std::vector<int> order;
+    for (int k = 0; k < kNPTiles * kBVars; k++) order.push_back(k);
+    for (size_t oi = 0; !rc; oi++) {
+        if (oi == (size_t)kNPTiles * kBVars && order.size() == oi)
+            for (int m = 1; m < kNListPer; m++) order.push_back(b_best + m * kNPTiles * kBVars);
+        if (oi >= order.size()) break;
+        const int k = order[oi];
         rc = set_shape(b, k);
         // one interval captures the shape's graph and warms it up; then the
         // timed ones
@@ -1512,7 +1534,7 @@ static int autotune(Batch *b, int n_intervals, int *best, float *ms, int *ran)
         *ran += 1 + n_intervals;
         t /= (float)n_intervals;
         if (ms) ms[k] = t;
-        if (k == 0 || t < best_ms) {
+        if (oi == 0 || t < best_ms) {
             best_ms = t;
             b_best = k;
         }
@@ -1540,12 +1562,12 @@ int rmpcd_dimer_batch_shapes(int precision, int *n_shapes)
 }
 
 int rmpcd_dimer_batch_shape_info(int precision, int shape, int *particles_per_tile, int *per_thread_begin,
-                                 int *per_thread_end, int *blocks_per_sm)
+                                 int *per_thread_end, int *blocks_per_sm, int *list_entries_per_thread)
 {
     RMPCD_ARG(precision == RMPCD_FP32 || precision == RMPCD_FP64, "precision must be RMPCD_FP32 or RMPCD_FP64");
     RMPCD_ARG(shape >= 0 && shape < kBShapes, "no such engine shape");
     int kb, ke, mb;
-    const int v = shape / kNPTiles;
+    const int v = shape_var(shape);
     if (precision == RMPCD_FP32) {
         using V0 = BVarOf<float, 0>::T;
         using V1 = BVarOf<float, 1>::T;
@@ -1561,7 +1583,8 @@ int rmpcd_dimer_batch_shape_info(int precision, int shape, int *particles_per_ti
         ke = v == 0 ? V0::KE : v == 1 ? V1::KE : V2::KE;
         mb = v == 0 ? V0::MINB : v == 1 ? V1::MINB : V2::MINB;
     }
-    if (particles_per_tile) *particles_per_tile = (int)kPTiles[shape % kNPTiles];
+    if (particles_per_tile) *particles_per_tile = (int)kPTiles[shape_tile(shape)];
+    if (list_entries_per_thread) *list_entries_per_thread = kListPer[shape_list(shape)];
     if (per_thread_begin) *per_thread_begin = kb;
     if (per_thread_end) *per_thread_end = ke;
     if (blocks_per_sm) *blocks_per_sm = mb;

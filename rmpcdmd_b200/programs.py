@@ -252,10 +252,11 @@ class DimerBatch:
         call("rmpcd_dimer_batch_shapes", int(precision), C.byref(n))
         out = []
         for k in range(n.value):
-            v = [C.c_int() for _ in range(4)]
+            v = [C.c_int() for _ in range(5)]
             call("rmpcd_dimer_batch_shape_info", int(precision), k, *[C.byref(x) for x in v])
             out.append(dict(particles_per_tile=v[0].value, per_thread_begin=v[1].value,
-                            per_thread_end=v[2].value, blocks_per_sm=v[3].value))
+                            per_thread_end=v[2].value, blocks_per_sm=v[3].value,
+                            list_entries_per_thread=v[4].value))
         return out
 
     @property
@@ -269,12 +270,12 @@ class DimerBatch:
         call("rmpcd_dimer_batch_set_shape", self._h, int(k))
 
     def autotune(self, n_intervals: int = 1) -> dict:
-        """rmpcd_dimer_batch_autotune: every engine shape runs 1 + n_intervals
-        real intervals of this batch (the results do not depend on the
-        shape) and the fastest is kept; a batch of a kind already tuned takes
-        the remembered choice without running.  Returns the choice, the
-        milliseconds per interval of each shape (-1 when remembered) and the
-        intervals every replica advanced by."""
+        """rmpcd_dimer_batch_autotune: the engine shapes it tries each run
+        1 + n_intervals real intervals of this batch (the results do not
+        depend on the shape) and the fastest is kept; a batch of a kind
+        already tuned takes the remembered choice without running.  Returns
+        the choice, the milliseconds per interval of each shape (-1 when not
+        run or remembered) and the intervals every replica advanced by."""
         n = C.c_int()
         call("rmpcd_dimer_batch_shapes", int(self.dimers[0].solvent.precision), C.byref(n))
         ms = (C.c_float * n.value)()

@@ -130,10 +130,11 @@ def test_engine_autotune_runs_real_intervals_and_remembers(rm):
     bt = DimerBatch(tuned)
     res = bt.autotune(1)
     n = len(DimerBatch.shapes(32))
-    assert res["intervals_run"] == 2 * n
+    timed = [m for m in res["ms_per_interval"] if m > 0]
+    assert len(timed) > n // 2 and all(m == -1 or m > 0 for m in res["ms_per_interval"])
+    assert res["intervals_run"] == 2 * len(timed)
     assert 0 <= res["best"] < n and bt.shape == res["best"]
-    assert all(m > 0 for m in res["ms_per_interval"])
-    assert res["ms_per_interval"][res["best"]] == min(res["ms_per_interval"])
+    assert res["ms_per_interval"][res["best"]] == min(timed)
     plain = drivers(rm, boxes, seeds, 32, 10)
     bp = DimerBatch(plain)
     bp.run(res["intervals_run"])
