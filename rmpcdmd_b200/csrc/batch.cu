@@ -63,10 +63,12 @@ struct BVarOf;
 template <> struct BVarOf<float, 0> { using T = BVar<4, 4, 4>; };
 template <> struct BVarOf<float, 1> { using T = BVar<2, 4, 4>; };
 template <> struct BVarOf<float, 2> { using T = BVar<4, 2, 4>; };
+template <> struct BVarOf<float, 3> { using T = BVar<4, 16, 4>; };
 template <> struct BVarOf<double, 0> { using T = BVar<2, 4, 4>; };
 template <> struct BVarOf<double, 1> { using T = BVar<1, 4, 4>; };
 template <> struct BVarOf<double, 2> { using T = BVar<2, 2, 4>; };
-constexpr int kBVars = 3;
+template <> struct BVarOf<double, 3> { using T = BVar<2, 8, 4>; };
+constexpr int kBVars = 4;
 constexpr long long kPTiles[] = {256, 512, 1024, 2048, 4096};  // particles per tile
 constexpr int kNPTiles = 5;
 // list entries per thread of the list kernels (pair forces, their
@@ -500,6 +502,61 @@ __global__ void __launch_bounds__(kBT, V::MINB)
         // can round to one) where the reference would store +0: equal in
         // value, not in bits, which is why FP32 results are compared by value.
         constexpr bool kAllVel = sizeof(R) == 8;
+        if constexpr (!kAllVel) {
+            // FP32: only particles with a WALL, MD, PAST_MD or REAC bit do
+            // anything, so the flags are read four at a time (one 16-byte
+            // load; the arrays are allocated to a multiple of 4) and a group
+            // of four without such a bit is skipped whole
+            constexpr int kBits = (1 << WALL_BIT) | (1 << MD_BIT) | (1 << PAST_MD_BIT) | (1 << REAC_BIT);
+            auto one = [&](long long i, int f) {
+                if (!(f & kBits)) return;
+                if (!((f >> WALL_BIT) & 1)) {
+                    const bool md = (f >> MD_BIT) & 1, past = (f >> PAST_MD_BIT) & 1;
+                    if (md || past) {
+                        const R vx = v.vel.x[i], vy = v.vel.y[i], vz = v.vel.z[i];
+                        R f0 = flagged(v.force.x, i, md), f1 = flagged(v.force.y, i, md),
+                          f2 = flagged(v.force.z, i, md);
+                        R g0 = flagged(v.force_old.x, i, past), g1 = flagged(v.force_old.y, i, past),
+                          g2 = flagged(v.force_old.z, i, past);
+                        v.vel.x[i] = vx + dt * (f0 + g0) / 2;
+                        v.vel.y[i] = vy + dt * (f1 + g1) / 2;
+                        v.vel.z[i] = vz + dt * (f2 + g2) / 2;
+                    }
+                } else {
+                    v.flags[i] = f & ~(1 << WALL_BIT);
+                    f = f & ~(1 << WALL_BIT);
+                }
+                if ((f >> REAC_BIT) & 1)
+                    change_species_one(v, i, i - off, a, bb, L0, L1, L2, cut_c, cut_n, prob, seed, step);
+            };
+            const long long a4 = (t.begin + 3) & ~3LL, e4 = t.end & ~3LL;
+            const long long h_end = a4 < t.end ? a4 : t.end;
+            for (long long i = t.begin + threadIdx.x; i < h_end; i += blockDim.x) one(i, v.flags[i]);
+            if (a4 < e4) {
+                const int4 *f4 = (const int4 *)v.flags;
+                constexpr int U = 4;
+                for (long long q0 = a4 / 4 + threadIdx.x; q0 < e4 / 4; q0 += (long long)U * blockDim.x) {
+                    int4 g[U];
+#pragma unroll
+                    for (int u = 0; u < U; u++) {
+                        const long long q = q0 + (long long)u * blockDim.x;
+                        g[u] = q < e4 / 4 ? f4[q] : make_int4(0, 0, 0, 0);
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; u++) {
+                        if (!((g[u].x | g[u].y | g[u].z | g[u].w) & kBits)) continue;
+                        const long long i = 4 * (q0 + (long long)u * blockDim.x);
+                        one(i, g[u].x);
+                        one(i + 1, g[u].y);
+                        one(i + 2, g[u].z);
+                        one(i + 3, g[u].w);
+                    }
+                }
+            }
+            const long long t_begin = e4 > h_end ? e4 : h_end;
+            for (long long i = t_begin + threadIdx.x; i < t.end; i += blockDim.x) one(i, v.flags[i]);
+            return;
+        }
         for (long long base = t.begin + threadIdx.x; base < t.end; base += (long long)K * blockDim.x) {
           int fk[K];
           R vxk[K] = {}, vyk[K] = {}, vzk[K] = {};
@@ -1049,6 +1106,7 @@ static void interval_launches(Batch *b)
         switch (shape_var(b->shape)) {
         case 1: md_step_launches<R, typename BVarOf<R, 1>::T>(b, k); break;
         case 2: md_step_launches<R, typename BVarOf<R, 2>::T>(b, k); break;
+        case 3: md_step_launches<R, typename BVarOf<R, 3>::T>(b, k); break;
         default: md_step_launches<R, typename BVarOf<R, 0>::T>(b, k); break;
         }
     }
@@ -1572,16 +1630,18 @@ int rmpcd_dimer_batch_shape_info(int precision, int shape, int *particles_per_ti
         using V0 = BVarOf<float, 0>::T;
         using V1 = BVarOf<float, 1>::T;
         using V2 = BVarOf<float, 2>::T;
-        kb = v == 0 ? V0::KB : v == 1 ? V1::KB : V2::KB;
-        ke = v == 0 ? V0::KE : v == 1 ? V1::KE : V2::KE;
-        mb = v == 0 ? V0::MINB : v == 1 ? V1::MINB : V2::MINB;
+        using V3 = BVarOf<float, 3>::T;
+        kb = v == 0 ? V0::KB : v == 1 ? V1::KB : v == 2 ? V2::KB : V3::KB;
+        ke = v == 0 ? V0::KE : v == 1 ? V1::KE : v == 2 ? V2::KE : V3::KE;
+        mb = v == 0 ? V0::MINB : v == 1 ? V1::MINB : v == 2 ? V2::MINB : V3::MINB;
     } else {
         using V0 = BVarOf<double, 0>::T;
         using V1 = BVarOf<double, 1>::T;
         using V2 = BVarOf<double, 2>::T;
-        kb = v == 0 ? V0::KB : v == 1 ? V1::KB : V2::KB;
-        ke = v == 0 ? V0::KE : v == 1 ? V1::KE : V2::KE;
-        mb = v == 0 ? V0::MINB : v == 1 ? V1::MINB : V2::MINB;
+        using V3 = BVarOf<double, 3>::T;
+        kb = v == 0 ? V0::KB : v == 1 ? V1::KB : v == 2 ? V2::KB : V3::KB;
+        ke = v == 0 ? V0::KE : v == 1 ? V1::KE : v == 2 ? V2::KE : V3::KE;
+        mb = v == 0 ? V0::MINB : v == 1 ? V1::MINB : v == 2 ? V2::MINB : V3::MINB;
     }
     if (particles_per_tile) *particles_per_tile = (int)kPTiles[shape_tile(shape)];
     if (list_entries_per_thread) *list_entries_per_thread = kListPer[shape_list(shape)];
