@@ -484,14 +484,17 @@ int rmpcd_dimer_batch_info(const rmpcd_dimer_batch *batch, int *n_replicas, long
                            int *n_extra_sorting);
 /* Engine shapes (no counterpart in the reference): particles per tile of
  * the solvent kernels, particles per thread and pass of the MD step's
- * begin / end kernels, the blocks per SM they are compiled for, and the
- * list entries per thread of the list kernels (pair forces, their
- * application, the contribution reset).  Every shape gives the same results
+ * begin / end kernels, the blocks per SM they are compiled for, the list
+ * entries per thread of the list kernels (pair forces, their application,
+ * the contribution reset), and whether the colloid half of the step begin
+ * runs in an extra first block while the solvent streams (1) or in the block
+ * that finishes last (0).  Every shape gives the same results
  * bit for bit.  A batch starts on 1024-particle tiles (smaller when that
  * gives fewer than ~2 tiles per SM) and one list entry per thread. */
 int rmpcd_dimer_batch_shapes(int precision, int *n_shapes);
 int rmpcd_dimer_batch_shape_info(int precision, int shape, int *particles_per_tile, int *per_thread_begin,
-                                 int *per_thread_end, int *blocks_per_sm, int *list_entries_per_thread);
+                                 int *per_thread_end, int *blocks_per_sm, int *list_entries_per_thread,
+                                 int *colloid_block_first);
 int rmpcd_dimer_batch_set_shape(rmpcd_dimer_batch *batch, int shape);
 int rmpcd_dimer_batch_get_shape(const rmpcd_dimer_batch *batch, int *shape);
 /* The engine's autotuner: every tile size and kernel variant with one list

@@ -214,7 +214,7 @@ PROTOTYPES = {
     "rmpcd_dimer_batch_scatter": [c_void_p, C.c_int, PART_P, PART_P, CELLS_P, NL_P, RNG_P],
     "rmpcd_dimer_batch_info": [c_void_p, c_int_p, C.POINTER(C.c_longlong), c_int_p],
     "rmpcd_dimer_batch_shapes": [C.c_int, c_int_p],
-    "rmpcd_dimer_batch_shape_info": [C.c_int, C.c_int, c_int_p, c_int_p, c_int_p, c_int_p, c_int_p],
+    "rmpcd_dimer_batch_shape_info": [C.c_int, C.c_int, c_int_p, c_int_p, c_int_p, c_int_p, c_int_p, c_int_p],
     "rmpcd_dimer_batch_set_shape": [c_void_p, C.c_int],
     "rmpcd_dimer_batch_get_shape": [c_void_p, c_int_p],
     "rmpcd_dimer_batch_autotune": [c_void_p, C.c_int, c_int_p, C.POINTER(C.c_float), c_int_p],

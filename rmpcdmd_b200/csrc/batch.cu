@@ -52,23 +52,28 @@ constexpr int kBT = 256;     // threads per tile block
 // the same results bit for bit: tiles and passes only decide which thread
 // handles which particle, and every per-particle result, the maximum
 // displacement and the re-sort decision are independent of that.
-template <int KB_, int KE_, int MINB_>
+template <int KB_, int KE_, int MINB_, int FIRST_>
 struct BVar {
     static constexpr int KB = KB_;      // particles per thread and pass, step begin
     static constexpr int KE = KE_;      // the same, step end
     static constexpr int MINB = MINB_;  // resident blocks per SM (launch bound)
+    // the colloid half of the step begin in an extra block 0 that runs while
+    // the solvent streams (1), or in the block that finishes last (0)
+    static constexpr bool FIRST = FIRST_ != 0;
 };
 template <typename R, int V>
 struct BVarOf;
-template <> struct BVarOf<float, 0> { using T = BVar<4, 4, 4>; };
-template <> struct BVarOf<float, 1> { using T = BVar<2, 4, 4>; };
-template <> struct BVarOf<float, 2> { using T = BVar<4, 2, 4>; };
-template <> struct BVarOf<float, 3> { using T = BVar<4, 16, 4>; };
-template <> struct BVarOf<double, 0> { using T = BVar<2, 4, 4>; };
-template <> struct BVarOf<double, 1> { using T = BVar<1, 4, 4>; };
-template <> struct BVarOf<double, 2> { using T = BVar<2, 2, 4>; };
-template <> struct BVarOf<double, 3> { using T = BVar<2, 8, 4>; };
-constexpr int kBVars = 4;
+template <> struct BVarOf<float, 0> { using T = BVar<4, 4, 4, 0>; };
+template <> struct BVarOf<float, 1> { using T = BVar<2, 4, 4, 0>; };
+template <> struct BVarOf<float, 2> { using T = BVar<4, 2, 4, 0>; };
+template <> struct BVarOf<float, 3> { using T = BVar<4, 16, 4, 0>; };
+template <> struct BVarOf<float, 4> { using T = BVar<4, 4, 4, 1>; };
+template <> struct BVarOf<double, 0> { using T = BVar<2, 4, 4, 1>; };
+template <> struct BVarOf<double, 1> { using T = BVar<1, 4, 4, 1>; };
+template <> struct BVarOf<double, 2> { using T = BVar<2, 2, 4, 1>; };
+template <> struct BVarOf<double, 3> { using T = BVar<2, 8, 4, 1>; };
+template <> struct BVarOf<double, 4> { using T = BVar<2, 4, 4, 0>; };
+constexpr int kBVars = 5;
 constexpr long long kPTiles[] = {256, 512, 1024, 2048, 4096};  // particles per tile
 constexpr int kNPTiles = 5;
 // list entries per thread of the list kernels (pair forces, their
@@ -310,15 +315,10 @@ struct ResortLists {
 // per particle tile; the last block to finish takes the program's re-sort
 // decision, lists the tiles of the replicas to re-sort and raises the graph's
 // re-sort condition when there are any.  The colloid half of every replica
-// runs in that last block in the FP32 form; in the FP64 form an extra block 0
-// runs it while the solvent streams (its registers would make the FP32
-// streaming path spill, which costs the large FP32 batches more than the
-// overlap gains).
-template <typename R>
-constexpr bool colloid_block_first()
-{
-    return sizeof(R) == 8;
-}
+// runs either in that last block or in an extra block 0 while the solvent
+// streams (V::FIRST, a choice of the engine shape: the extra block's registers
+// make the FP32 streaming path spill, which costs the large FP32 batches more
+// than the overlap gains, and the autotuner weighs the two).
 
 template <typename R, typename V>
 __global__ void __launch_bounds__(kBT, V::MINB)
@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(kBT, V::MINB)
     __shared__ int s_last;
     __shared__ int ws[kBT / 32 + 1];
     __shared__ double s_max[kBT / 32];
-    constexpr bool kFirst = colloid_block_first<R>();
+    constexpr bool kFirst = V::FIRST;
     const bool colloid_block = kFirst && blockIdx.x == 0;
     const BTile t = colloid_block ? BTile{0, 0, 0, 0} : tiles[blockIdx.x - (kFirst ? 1 : 0)];
     if (colloid_block)
@@ -1068,7 +1068,7 @@ static void md_step_launches(Batch *b, int k)
         note(b, cudaStreamGetCaptureInfo(st, &st_cap, nullptr, &g, nullptr, nullptr));
         note(b, cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
     }
-    kb_step_begin<R, V><<<b->n_ptile + (colloid_block_first<R>() ? 1 : 0), kBT, 0, st>>>(b->ptile, b->rep, s, alt.pos, s.force_old, (R)dt, (R)dt_sq,
+    kb_step_begin<R, V><<<b->n_ptile + (V::FIRST ? 1 : 0), kBT, 0, st>>>(b->ptile, b->rep, s, alt.pos, s.force_old, (R)dt, (R)dt_sq,
                                                  b->so_max, b->done, b->resort, b->n_extra, cs,
                                                  ResortLists{b->ptile_first, b->ptile_count, b->stile_first,
                                                              b->stile_count, b->act_p, b->act_s, b->n_act},
@@ -1107,6 +1107,7 @@ static void interval_launches(Batch *b)
         case 1: md_step_launches<R, typename BVarOf<R, 1>::T>(b, k); break;
         case 2: md_step_launches<R, typename BVarOf<R, 2>::T>(b, k); break;
         case 3: md_step_launches<R, typename BVarOf<R, 3>::T>(b, k); break;
+        case 4: md_step_launches<R, typename BVarOf<R, 4>::T>(b, k); break;
         default: md_step_launches<R, typename BVarOf<R, 0>::T>(b, k); break;
         }
     }
@@ -1620,31 +1621,38 @@ int rmpcd_dimer_batch_shapes(int precision, int *n_shapes)
 }
 
 int rmpcd_dimer_batch_shape_info(int precision, int shape, int *particles_per_tile, int *per_thread_begin,
-                                 int *per_thread_end, int *blocks_per_sm, int *list_entries_per_thread)
+                                 int *per_thread_end, int *blocks_per_sm, int *list_entries_per_thread,
+                                 int *colloid_block_first)
 {
     RMPCD_ARG(precision == RMPCD_FP32 || precision == RMPCD_FP64, "precision must be RMPCD_FP32 or RMPCD_FP64");
     RMPCD_ARG(shape >= 0 && shape < kBShapes, "no such engine shape");
     int kb, ke, mb;
+    bool cf;
     const int v = shape_var(shape);
     if (precision == RMPCD_FP32) {
         using V0 = BVarOf<float, 0>::T;
         using V1 = BVarOf<float, 1>::T;
         using V2 = BVarOf<float, 2>::T;
         using V3 = BVarOf<float, 3>::T;
-        kb = v == 0 ? V0::KB : v == 1 ? V1::KB : v == 2 ? V2::KB : V3::KB;
-        ke = v == 0 ? V0::KE : v == 1 ? V1::KE : v == 2 ? V2::KE : V3::KE;
-        mb = v == 0 ? V0::MINB : v == 1 ? V1::MINB : v == 2 ? V2::MINB : V3::MINB;
+        using V4 = BVarOf<float, 4>::T;
+        kb = v == 0 ? V0::KB : v == 1 ? V1::KB : v == 2 ? V2::KB : v == 3 ? V3::KB : V4::KB;
+        ke = v == 0 ? V0::KE : v == 1 ? V1::KE : v == 2 ? V2::KE : v == 3 ? V3::KE : V4::KE;
+        mb = v == 0 ? V0::MINB : v == 1 ? V1::MINB : v == 2 ? V2::MINB : v == 3 ? V3::MINB : V4::MINB;
+        cf = v == 0 ? V0::FIRST : v == 1 ? V1::FIRST : v == 2 ? V2::FIRST : v == 3 ? V3::FIRST : V4::FIRST;
     } else {
         using V0 = BVarOf<double, 0>::T;
         using V1 = BVarOf<double, 1>::T;
         using V2 = BVarOf<double, 2>::T;
         using V3 = BVarOf<double, 3>::T;
-        kb = v == 0 ? V0::KB : v == 1 ? V1::KB : v == 2 ? V2::KB : V3::KB;
-        ke = v == 0 ? V0::KE : v == 1 ? V1::KE : v == 2 ? V2::KE : V3::KE;
-        mb = v == 0 ? V0::MINB : v == 1 ? V1::MINB : v == 2 ? V2::MINB : V3::MINB;
+        using V4 = BVarOf<double, 4>::T;
+        kb = v == 0 ? V0::KB : v == 1 ? V1::KB : v == 2 ? V2::KB : v == 3 ? V3::KB : V4::KB;
+        ke = v == 0 ? V0::KE : v == 1 ? V1::KE : v == 2 ? V2::KE : v == 3 ? V3::KE : V4::KE;
+        mb = v == 0 ? V0::MINB : v == 1 ? V1::MINB : v == 2 ? V2::MINB : v == 3 ? V3::MINB : V4::MINB;
+        cf = v == 0 ? V0::FIRST : v == 1 ? V1::FIRST : v == 2 ? V2::FIRST : v == 3 ? V3::FIRST : V4::FIRST;
     }
     if (particles_per_tile) *particles_per_tile = (int)kPTiles[shape_tile(shape)];
     if (list_entries_per_thread) *list_entries_per_thread = kListPer[shape_list(shape)];
+    if (colloid_block_first) *colloid_block_first = cf ? 1 : 0;
     if (per_thread_begin) *per_thread_begin = kb;
     if (per_thread_end) *per_thread_end = ke;
     if (blocks_per_sm) *blocks_per_sm = mb;

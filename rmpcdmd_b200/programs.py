@@ -252,11 +252,11 @@ class DimerBatch:
         call("rmpcd_dimer_batch_shapes", int(precision), C.byref(n))
         out = []
         for k in range(n.value):
-            v = [C.c_int() for _ in range(5)]
+            v = [C.c_int() for _ in range(6)]
             call("rmpcd_dimer_batch_shape_info", int(precision), k, *[C.byref(x) for x in v])
             out.append(dict(particles_per_tile=v[0].value, per_thread_begin=v[1].value,
                             per_thread_end=v[2].value, blocks_per_sm=v[3].value,
-                            list_entries_per_thread=v[4].value))
+                            list_entries_per_thread=v[4].value, colloid_block_first=bool(v[5].value)))
         return out
 
     @property
