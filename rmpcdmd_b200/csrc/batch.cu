@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1527,8 +1528,19 @@ static int set_shape(Batch *b, int s)
     return RMPCD_OK;
 }
 
-// chosen shapes per GPU, precision, N_MD and mix of boxes
+// chosen shapes per GPU, precision, N_MD and mix of boxes (batches on
+// different host threads may tune at once: the map is guarded)
 static std::map<std::string, int> g_batch_tuned;
+static std::mutex g_batch_tuned_mu;
+
+static bool tuned_lookup(const std::string &key, int *shape)
+{
+    std::lock_guard<std::mutex> lk(g_batch_tuned_mu);
+    auto hit = g_batch_tuned.find(key);
+    if (hit == g_batch_tuned.end()) return false;
+    *shape = hit->second;
+    return true;
+}
 
 static std::string tune_key(const Batch *b)
 {
@@ -1553,12 +1565,12 @@ static int autotune(Batch *b, int n_intervals, int *best, float *ms, int *ran)
 {
     *ran = 0;
     const std::string key = tune_key(b);
-    auto hit = g_batch_tuned.find(key);
-    if (hit != g_batch_tuned.end()) {
-        *best = hit->second;
+    int remembered = 0;
+    if (tuned_lookup(key, &remembered)) {
+        *best = remembered;
         if (ms)
             for (int k = 0; k < kBShapes; k++) ms[k] = -1.0f;
-        return set_shape(b, hit->second);
+        return set_shape(b, remembered);
     }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     RMPCD_CUDA_TRY(cudaEventCreate(&e0));
@@ -1601,7 +1613,10 @@ static int autotune(Batch *b, int n_intervals, int *best, float *ms, int *ran)
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) return rc;
-    g_batch_tuned[key] = b_best;
+    {
+        std::lock_guard<std::mutex> lk(g_batch_tuned_mu);
+        g_batch_tuned[key] = b_best;
+    }
     *best = b_best;
     return set_shape(b, b_best);
 }
