@@ -563,9 +563,10 @@ def run_ours(args):
     out["phases_ms"] = {k: round(v[0] * 1e3 / max(1, args.steps), 4)
                         for k, v in r32["phases"].items()}
     # kernels launched per step: fused interval, 2 scan kernels, placement;
-    # plus, once per timed call, the record packing (1), the final segment
-    # sort (2) and gather (1)
-    out["gpu_launches"] = 4 * args.steps + 4
+    # plus, once per timed call, the record packing (1) and the FP32 end of
+    # the run: entry positions of the records (1), segment sort (2), records
+    # back from entry positions (1), gather into the API arrays (1)
+    out["gpu_launches"] = 4 * args.steps + 6
     if not args.no_e2e:
         e2e_steps = max(1, min(args.e2e_steps, args.steps))
         path = ("rmpcd_particles_upload x6 (pinned host, reference (3,N) layout) -> rmpcd_bulk_run(1) "
