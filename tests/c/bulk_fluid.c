@@ -104,6 +104,44 @@ int main(int argc, char **argv)
         fprintf(stderr, "rng step %llu, expected 7\n", (unsigned long long)rng.step);
         bad = 1;
     }
+    /* sort_particles (src/cell_system.f90:131-151): the current positions of p,
+     * counted, scattered in cell order into a second system q; the compact
+     * Hilbert index of each scattered position must not decrease */
+    rmpcd_particles *q = NULL;
+    CHECK(rmpcd_particles_init(&q, N, 1, NULL, precision));
+    CHECK(rmpcd_cells_count_particles(cells, p));
+    CHECK(rmpcd_cells_sort_particles(cells, p, q));
+    double *qpos = malloc(sizeof(double) * 3 * N), o[3];
+    CHECK(rmpcd_particles_download(q, "pos", qpos));
+    CHECK(rmpcd_cells_get_origin(cells, o));
+    int prev = -1;
+    for (int i = 0; i < N && !bad; i++) {
+        int pc[3], h = 0;
+        for (int k = 0; k < 3; k++) {
+            pc[k] = (int)floor(qpos[3 * i + k] - o[k]);
+            if (pc[k] == Lo[k]) pc[k] = 0;
+        }
+        CHECK(rmpcd_compact_p_to_h(pc, M, &h));
+        if (h < prev) {
+            fprintf(stderr, "sort_particles: position %d in slot %d after slot %d\n", i, h, prev);
+            bad = 1;
+        }
+        prev = h;
+    }
+    /* random_placement keyed by the state's seed; the step stays */
+    CHECK(rmpcd_particles_random_placement(q, edges, NULL, NULL, &rng));
+    CHECK(rmpcd_particles_download(q, "pos", qpos));
+    for (int i = 0; i < 3 * N && !bad; i++)
+        if (!(qpos[i] >= 0 && qpos[i] < edges[i % 3])) {
+            fprintf(stderr, "random_placement: coordinate %d = %g outside the box\n", i, qpos[i]);
+            bad = 1;
+        }
+    if (rng.step != 7) {
+        fprintf(stderr, "random_placement moved the rng step to %llu\n", (unsigned long long)rng.step);
+        bad = 1;
+    }
+    free(qpos);
+    CHECK(rmpcd_particles_destroy(q));
     CHECK(rmpcd_particles_destroy(p));
     CHECK(rmpcd_cells_destroy(cells));
     free(pos);
