@@ -266,14 +266,14 @@ constexpr int kPermPad = 8;
 // above the microseconds one copy takes)
 constexpr int kBulkPolls = 1 << 16;
 
-// shared memory of a tile: velocity parts and source indices per particle,
-// the tile-local cell of each particle (one byte) and each cell's local start
-// and count
+// shared memory of a tile: velocity parts and source indices per particle;
+// the FP64 form's in-cell ordering also keeps the tile-local cell of each
+// particle (one byte) and each cell's local start and count
 template <typename R, typename S>
 constexpr size_t fused_smem()
 {
-    return (size_t)S::kCap * (Rec<R>::kVelBytes + sizeof(int) + 1) + (size_t)kPermPad * sizeof(int) +
-           2 * (size_t)S::kSlots * sizeof(int);
+    return (size_t)S::kCap * (Rec<R>::kVelBytes + sizeof(int)) + (size_t)kPermPad * sizeof(int) +
+           (sizeof(R) == 8 ? (size_t)S::kCap + 2 * (size_t)S::kSlots * sizeof(int) : 0);
 }
 
 // the non-velocity part of a record, as loaded from global memory
@@ -360,9 +360,11 @@ __global__ void __launch_bounds__(kFusedThreads, S::kMinBlocks) k_bulk_interval(
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned char *s_vel = smem;
     int *s_idx = (int *)(smem + (size_t)CAP * VB);          // the tile's index window
-    int *s_cstart = s_idx + CAP + kPermPad;                 // per cell of the tile
+    // FP64 only (the in-cell ordering): cell starts and counts of the tile,
+    // tile-local cell of each particle
+    int *s_cstart = s_idx + CAP + kPermPad;
     int *s_ccount = s_cstart + SL;
-    unsigned char *s_cell = (unsigned char *)(s_ccount + SL);  // per particle
+    unsigned char *s_cell = (unsigned char *)(s_ccount + SL);
 
     __shared__ __align__(8) unsigned long long s_bar;
     const int t = threadIdx.x;
@@ -413,7 +415,7 @@ __global__ void __launch_bounds__(kFusedThreads, S::kMinBlocks) k_bulk_interval(
         } else {
             for (int j = t; j < np; j += kFusedThreads) s_perm[j] = a0 + j;
         }
-        if (sizeof(R) == 8 && A.perm) {
+        if constexpr (sizeof(R) == 8) if (A.perm) {
             // FP64: each cell's indices in ascending order (the reference's
             // stable scatter order): every index is placed at its rank among
             // the cell's indices, one thread per index, so a crowded cell
