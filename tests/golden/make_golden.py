@@ -30,6 +30,12 @@ Cases (all plain FP64, density 10, kT = 1/3, alpha = pi/2, tau = 1):
             4.5, N_MD = 100, dt = 0.01, probability 1), 32^3 cells, 327,680
             solvent particles: 10 intervals (1,000 MD steps) and 100 intervals
             (100 collision steps, 10,000 MD steps).
+  dimer_96  the same program in a 96^3 box (8,847,360 solvent particles, the
+            large-box dimer configuration): 1 and 2 intervals.
+  ncolloids_128  programs/n_colloids_pbc.f90: 200 passive colloids (sigma 3)
+            in 128^3 cells (20,971,520 solvent particles, no volume
+            correction), one thermostatted interval (MPC-AT, lazy cell-wise
+            streaming) and one production interval.
 """
 from __future__ import annotations
 
@@ -54,6 +60,10 @@ CASES = {
     "bulk_32": dict(kind="bulk", L=[32, 32, 32], rho=10, seed=3, checkpoints=[5, 100]),
     "dimer_32": dict(kind="dimer", L=[32, 32, 32], rho=10, N_MD=100, seed=1, list_capacity=6000,
                      checkpoints=[10, 100]),
+    "dimer_96": dict(kind="dimer", L=[96, 96, 96], rho=10, N_MD=100, seed=5, list_capacity=6000,
+                     checkpoints=[1, 2]),
+    "ncolloids_128": dict(kind="ncolloids", L=[128, 128, 128], rho=10, N_MD=100, N_colloids=200, seed=7,
+                          checkpoints=[1, 2]),
 }
 
 
@@ -159,9 +169,46 @@ def make_dimer(name: str, case: dict) -> dict:
     return out
 
 
+# ------------------------------------------------------------ n colloids
+def ncolloids_kwargs(case: dict) -> dict:
+    return dict(L=tuple(case["L"]), rho=case["rho"], N_MD=case["N_MD"], N_colloids=case["N_colloids"],
+                seed=case["seed"], volume_correction=False)
+
+
+def ncolloids_state(d, rows) -> dict:
+    arrays = {f: getattr(d.s, f) for f in SOLVENT + ("force",)}
+    rec = state_record(arrays, d.cells.cell_count, d.cells.cell_start, d.cells.origin, rows)
+    rec["lists"] = lists_record(d.nl.list, d.nl.n)
+    rec["colloids"] = {f: getattr(d.c, f).tolist() for f in ("pos", "vel", "force", "image")}
+    rec["n_extra_sorting"] = int(d.n_extra_sorting)
+    rec["rng_step"] = int(d.step)
+    return rec
+
+
+def make_ncolloids(name: str, case: dict) -> dict:
+    """Checkpoint 1: one thermostatted interval (thermalise(1)); checkpoint 2:
+    one production interval after it (run(1))."""
+    from oracle.programs import NColloidsPBC as ON
+
+    d = ON(**ncolloids_kwargs(case))
+    rows = sample_rows(d.N, case["seed"])
+    out = dict(case, name=name, checkpoint_states={})
+    d.thermalise(1)
+    out["checkpoint_states"]["1"] = ncolloids_state(d, rows)
+    print(f"  {name}: thermalised", flush=True)
+    d.run(1)
+    out["checkpoint_states"]["2"] = ncolloids_state(d, rows)
+    print(f"  {name}: 1 production interval", flush=True)
+    return out
+
+
 def make(name: str) -> dict:
     case = CASES[name]
-    return make_bulk(name, case) if case["kind"] == "bulk" else make_dimer(name, case)
+    if case["kind"] == "bulk":
+        return make_bulk(name, case)
+    if case["kind"] == "ncolloids":
+        return make_ncolloids(name, case)
+    return make_dimer(name, case)
 
 
 def path_of(name: str) -> Path:

@@ -11,7 +11,10 @@ oracle wrote (tests/golden/make_golden.py, one oracle thread).
   intervals (1,000 MD steps) and 100 intervals (100 collision steps), through
   the call-by-call driver and through the replica engine: the colloid
   trajectory after every interval and every solvent array, the cell counts
-  and starts and the neighbor lists at the checkpoints.
+  and starts and the neighbor lists at the checkpoints;
+* single_dimer_pbc at 96^3 for 2 intervals in the replica engine;
+* n_colloids_pbc at 128^3 with 200 colloids (rmpcd_ncolloids_run): one
+  thermostatted interval and one production interval.
 
 Every array is compared by its SHA-256 digest, so a match is equality bit for
 bit; on a mismatch the sampled rows say where the arrays part."""
@@ -162,4 +165,46 @@ def test_single_dimer_32_engine_100_intervals(rm):
         g = batch.scatter(0)
         check_colloids(g, fx["colloids"][k - 1], f"dimer_32 engine interval {k}")
         dimer_check(g, fx["checkpoint_states"][str(k)], f"dimer_32 engine after {k} intervals")
+    rm.get_status()
+
+
+def test_single_dimer_96_engine_2_intervals(rm):
+    """The large-box dimer (96^3, 8,847,360 solvent particles) in the replica
+    engine against the oracle's run of the same program."""
+    from rmpcdmd_b200.programs import DimerBatch, SingleDimerPBC
+
+    fx = G.load("dimer_96")
+    d = SingleDimerPBC(**G.dimer_kwargs(fx))
+    batch = DimerBatch([d])
+    done = 0
+    for k in fx["checkpoints"]:
+        batch.run(k - done)
+        done = k
+        g = batch.scatter(0)
+        check_colloids(g, fx["colloids"][k - 1], f"dimer_96 engine interval {k}")
+        dimer_check(g, fx["checkpoint_states"][str(k)], f"dimer_96 engine after {k} intervals")
+    rm.get_status()
+
+
+def test_n_colloids_128_native_loop(rm):
+    """n_colloids_pbc at its configuration size (128^3, 200 colloids): one
+    thermostatted and one production interval of rmpcd_ncolloids_run against
+    the oracle's run of the program."""
+    from rmpcdmd_b200.programs import NColloidsPBC
+
+    fx = G.load("ncolloids_128")
+    g = NColloidsPBC(**G.ncolloids_kwargs(fx))
+    for k, step in ((1, lambda: g.thermalise(1)), (2, lambda: g.run(1))):
+        step()
+        rec = fx["checkpoint_states"][str(k)]
+        what = f"ncolloids_128 checkpoint {k}"
+        arrays = {f: g.solvent.download(f) for f in FIELDS + ("force",)}
+        check_state(rec, arrays, g.cells.cell_count, g.cells.cell_start, g.cells.origin, what)
+        for f in ("pos", "vel", "force", "image"):
+            assert g.colloids.download(f).tolist() == rec["colloids"][f], f"{what}: colloid {f}"
+        lst, n = g.neigh.download()
+        assert [int(x) for x in n] == rec["lists"]["n"], f"{what}: list lengths"
+        for i in range(len(n)):
+            assert G.digest(lst[i, : n[i]]) == rec["lists"]["sha256"][i], f"{what}: list of colloid {i + 1}"
+        assert g.n_extra_sorting == rec["n_extra_sorting"] and g.rng.step == rec["rng_step"], what
     rm.get_status()
