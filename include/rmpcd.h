@@ -339,7 +339,10 @@ int rmpcd_nlist_update(rmpcd_nlist *nl, rmpcd_particles *system1, rmpcd_particle
                        double radius, rmpcd_cells *cells, const rmpcd_lj *lj);
 /* list(Nmax, Npoints) column-major 1-based, n(Npoints) */
 int rmpcd_nlist_download(const rmpcd_nlist *nl, int *list, int *n);
-/* compute_force, src/neighbor_list.f90:159-225 (energy may be NULL) */
+/* compute_force, src/neighbor_list.f90:159-225 (energy may be NULL).  Each
+ * colloid's force sum is in list order for an FP64 solvent (ps2); for an
+ * FP32 solvent it is an FP64 sum by a fixed tree over the list (the same bits
+ * on every call, not the list-order bits). */
 int rmpcd_compute_force(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist *nl,
                         const double L[3], const rmpcd_lj *lj, double *energy);
 /* compute_force_n2, src/neighbor_list.f90:227-264 (energy may be NULL) */

@@ -139,6 +139,7 @@ struct rmpcd_dimer_batch {
     int *ncontrib = nullptr, *max_contrib = nullptr, *clist = nullptr, *cn = nullptr;
     unsigned long long *so_max = nullptr;
     double *co_max = nullptr;  // per replica: the colloids' displacement of this MD step
+    double *csnap = nullptr;   // colloid positions at the step's force evaluation, 3 per colloid
     // whether some solvent species was negative at creation; species change
     // only to 1 or 2 inside the batch, so otherwise every particle passes
     // maximum_displacement's species >= 0 test and species need not be read
@@ -156,6 +157,7 @@ struct rmpcd_dimer_batch {
     bool capturing = false;
     cudaError_t cap_err = cudaSuccess;
     cudaStream_t body = nullptr;  // captures the bodies of the re-sort IF nodes
+    cudaGraphConditionalHandle cond_next = 0;  // re-sort condition of the next MD step, while capturing
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
 };
 
@@ -309,36 +311,15 @@ struct ResortLists {
     int *n;                                        // out: n[0] particle tiles, n[1] slot tiles
 };
 
-// md_pos of every solvent particle, the PAST_MD/MD roll of compute_force,
-// clearing of the entries that become `force` after switch_force and the
-// solvent's maximum displacement (src/md.f90:61-77,
-// src/neighbor_list.f90:180-188, src/particle_system.f90:357-378), one block
-// per particle tile; the last block to finish takes the program's re-sort
-// decision, lists the tiles of the replicas to re-sort and raises the graph's
-// re-sort condition when there are any.  The colloid half of every replica
-// runs either in that last block or in an extra block 0 while the solvent
-// streams (V::FIRST, a choice of the engine shape: the extra block's registers
-// make the FP32 streaming path spill, which costs the large FP32 batches more
-// than the overlap gains, and the autotuner weighs the two).
-
-template <typename R, typename V>
-__global__ void __launch_bounds__(kBT, V::MINB)
-    kb_step_begin(const BTile *tiles, const BRep *rep, PView<R> v, Vec3<R> old, Vec3<R> next, R dt, R dt_sq,
-                  unsigned long long *so_max, unsigned *done, int *resort, int *n_extra, ColloidStep cs,
-                  ResortLists rl, cudaGraphConditionalHandle cond, int use_cond, int read_species, unsigned *err)
+// md_pos over the particle tile t (the solvent half of the MD step's
+// beginning): returns this thread's largest squared displacement from pos_old
+// among particles of species >= 0.  K particles per thread and pass, all
+// loads issued before any use.
+template <typename R, int K>
+__device__ __forceinline__ double begin_tile(const BTile &t, const PView<R> &v, const Vec3<R> &old,
+                                             const Vec3<R> &next, R dt, R dt_sq, int read_species)
 {
-    __shared__ int s_last;
-    __shared__ int ws[kBT / 32 + 1];
-    __shared__ double s_max[kBT / 32];
-    constexpr bool kFirst = V::FIRST;
-    const bool colloid_block = kFirst && blockIdx.x == 0;
-    const BTile t = colloid_block ? BTile{0, 0, 0, 0} : tiles[blockIdx.x - (kFirst ? 1 : 0)];
-    if (colloid_block)
-        for (int r = threadIdx.x; r < cs.R; r += blockDim.x)
-            cs.co_max[r] = colloid_begin(r, rep, cs.c, cs.cold, cs.c_next, cs.rat, cs.mass, cs.ms, cs.d, cs.dt, err);
     double m = 0;
-    // K particles per thread and pass, all loads issued before any use
-    constexpr int K = V::KB;
     for (long long base = t.begin + threadIdx.x; base < t.end; base += (long long)K * blockDim.x) {
         int f[K], sp[K];
         R px[K], py[K], pz[K], vx[K], vy[K], vz[K], ox[K], oy[K], oz[K];
@@ -381,19 +362,38 @@ __global__ void __launch_bounds__(kBT, V::MINB)
             }
         }
     }
+    return m;
+}
+
+// the block's maximum displacement into its replica's so_max (r_tile < 0:
+// a block without particles), then the last-block hand-off: true in the one
+// block of the grid that finishes last
+__device__ __forceinline__ bool block_done(double m, int r_tile, unsigned long long *so_max, unsigned *done,
+                                           double *s_max, int *s_last)
+{
     m = warp_max(m);
     if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = m;
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int w = 1; w < kBT / 32; w++) m = m > s_max[w] ? m : s_max[w];
         // one atomic per block, skipped when it cannot raise the maximum
-        if (!colloid_block && m > __longlong_as_double((long long)__ldcg(so_max + t.r)))
-            atomic_max_nonneg(so_max + t.r, m);
+        if (r_tile >= 0 && m > __longlong_as_double((long long)__ldcg(so_max + r_tile)))
+            atomic_max_nonneg(so_max + r_tile, m);
         __threadfence();
-        s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+        *s_last = atomicAdd(done, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (!s_last) return;
+    return *s_last;
+}
+
+// the last block's part of an MD step's beginning: the colloid half of every
+// replica unless an earlier block did it (kFirst), the re-sort decisions, the
+// tile lists of the replicas to re-sort and the graph's re-sort condition
+template <bool kFirst>
+__device__ __forceinline__ void begin_tail(const BRep *rep, unsigned long long *so_max, unsigned *done, int *resort,
+                                           int *n_extra, const ColloidStep &cs, const ResortLists &rl,
+                                           cudaGraphConditionalHandle cond, int use_cond, unsigned *err, int *ws)
+{
     __threadfence();
     int any = 0, base_p = 0, base_s = 0;
     for (int r0 = 0; r0 < cs.R; r0 += blockDim.x) {
@@ -424,18 +424,56 @@ __global__ void __launch_bounds__(kBT, V::MINB)
     }
 }
 
+// md_pos of every solvent particle, the PAST_MD/MD roll of compute_force,
+// clearing of the entries that become `force` after switch_force and the
+// solvent's maximum displacement (src/md.f90:61-77,
+// src/neighbor_list.f90:180-188, src/particle_system.f90:357-378), one block
+// per particle tile; the last block to finish takes the program's re-sort
+// decision, lists the tiles of the replicas to re-sort and raises the graph's
+// re-sort condition when there are any.  The colloid half of every replica
+// runs either in that last block or in an extra block 0 while the solvent
+// streams (V::FIRST, a choice of the engine shape: the extra block's registers
+// make the FP32 streaming path spill, which costs the large FP32 batches more
+// than the overlap gains, and the autotuner weighs the two).
+template <typename R, typename V>
+__global__ void __launch_bounds__(kBT, V::MINB)
+    kb_step_begin(const BTile *tiles, const BRep *rep, PView<R> v, Vec3<R> old, Vec3<R> next, R dt, R dt_sq,
+                  unsigned long long *so_max, unsigned *done, int *resort, int *n_extra, ColloidStep cs,
+                  ResortLists rl, cudaGraphConditionalHandle cond, int use_cond, int read_species, unsigned *err)
+{
+    __shared__ int s_last;
+    __shared__ int ws[kBT / 32 + 1];
+    __shared__ double s_max[kBT / 32];
+    constexpr bool kFirst = V::FIRST;
+    double m = 0;
+    int r_tile = -1;
+    if (kFirst && blockIdx.x == 0) {
+        for (int r = threadIdx.x; r < cs.R; r += blockDim.x)
+            cs.co_max[r] = colloid_begin(r, rep, cs.c, cs.cold, cs.c_next, cs.rat, cs.mass, cs.ms, cs.d, cs.dt, err);
+    } else {
+        const BTile t = tiles[blockIdx.x - (kFirst ? 1 : 0)];
+        r_tile = t.r;
+        m = begin_tile<R, V::KB>(t, v, old, next, dt, dt_sq, read_species);
+    }
+    if (!block_done(m, r_tile, so_max, done, s_max, &s_last)) return;
+    begin_tail<kFirst>(rep, so_max, done, resort, n_extra, cs, rl, cond, use_cond, err, ws);
+}
+
 // list pair forces (src/neighbor_list.f90:198-219) fused with
 // flag_particles_nl of the catalytic bead (programs/single_dimer_pbc.f90:493-509):
-// both only read positions and species and OR bits into flags
+// both only read positions and species and OR bits into flags.  Block (0, i)
+// also copies colloid i's position to csnap[3 i ..], the positions that the
+// step's change_species uses.
 template <typename R>
 __global__ void kb_pair_forces(const BRep *rep, PView<double> c, PView<R> s, const int *list, const int *n, int Nmax,
                                LJDev lj, double *pf, double *pe, unsigned char *contrib, int *ncontrib,
-                               int *max_contrib, double flag_cut_sq)
+                               int *max_contrib, double flag_cut_sq, double *csnap)
 {
     const int i = blockIdx.y;
     const int r = i >> 1;
     const int ni = n[i];
     const double x[3] = {c.pos.x[i], c.pos.y[i], c.pos.z[i]};
+    if (blockIdx.x == 0 && threadIdx.x < 3) csnap[3 * i + threadIdx.x] = x[threadIdx.x];
     const int s1 = c.species[i];
     const double L0 = rep[r].g.edges[0], L1 = rep[r].g.edges[1], L2 = rep[r].g.edges[2];
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ni; e += gridDim.x * blockDim.x) {
@@ -449,7 +487,8 @@ __global__ void kb_pair_forces(const BRep *rep, PView<double> c, PView<R> s, con
 
 // the three consumers of the pair forces, on disjoint data: solvent
 // particles with one contribution, those with several (per replica, in
-// order), and the ordered colloid sums
+// order), and the colloid sums (list order in the FP64 form, a fixed tree in
+// the FP32 form)
 template <typename R>
 __global__ void kb_apply_sum(const BRep *rep, int R_, int gx, const int *list, const int *n, int Nmax,
                              const unsigned char *contrib, const double *pf, const int *ncontrib,
@@ -468,8 +507,10 @@ __global__ void kb_apply_sum(const BRep *rep, int R_, int gx, const int *list, c
         const size_t q0 = (size_t)2 * r * Nmax;
         apply_multi_block(list + q0, n + 2 * r, 2, Nmax, contrib + q0, pf + 3 * q0, ncontrib, rep[r].serial, fx, fy,
                           fz);
-    } else {
+    } else if constexpr (sizeof(R) == 8) {
         colloid_sum_block(b - n_single - R_, n, Nmax, contrib, pf, cfx, cfy, cfz, clist, cn);
+    } else {
+        colloid_tree_block(b - n_single - R_, n, Nmax, contrib, pf, cfx, cfy, cfz);
     }
 }
 
@@ -478,6 +519,169 @@ __global__ void kb_apply_sum(const BRep *rep, int R_, int gx, const int *list, c
 // contribution counters; compute_force_n2, the colloid velocity half and
 // RATTLE's velocity correction per replica (src/neighbor_list.f90:227-264,
 // programs/single_dimer_pbc.f90:356-359, src/md.f90:298-319)
+// the solvent half over the particle tile t of replica rp, whose colloid
+// positions are a and bb; step is the random-number step of change_species
+template <typename R, int K>
+__device__ __forceinline__ void end_tile(const BTile &t, const BRep &rp, const PView<R> &v, const double a[3],
+                                         const double bb[3], R dt, double cut_c, double cut_n, double prob,
+                                         uint64_t step)
+{
+    const double L0 = rp.g.edges[0], L1 = rp.g.edges[1], L2 = rp.g.edges[2];
+    const uint64_t seed = rp.seed;
+    const long long off = rp.off;
+    // The FP64 form reads every velocity: a zero-force update turns a -0
+    // component into +0, as the reference's does.  The FP32 form reads
+    // velocities only for particles with a force and leaves the others'
+    // bits untouched, so it keeps a -0 component (an SRD rotation product
+    // can round to one) where the reference would store +0: equal in
+    // value, not in bits, which is why FP32 results are compared by value.
+    constexpr bool kAllVel = sizeof(R) == 8;
+    if constexpr (!kAllVel) {
+        // FP32: only particles with a WALL, MD, PAST_MD or REAC bit do
+        // anything, so the flags are read four at a time (one 16-byte
+        // load; the arrays are allocated to a multiple of 4) and a group
+        // of four without such a bit is skipped whole
+        constexpr int kBits = (1 << WALL_BIT) | (1 << MD_BIT) | (1 << PAST_MD_BIT) | (1 << REAC_BIT);
+        auto one = [&](long long i, int f) {
+            if (!(f & kBits)) return;
+            if (!((f >> WALL_BIT) & 1)) {
+                const bool md = (f >> MD_BIT) & 1, past = (f >> PAST_MD_BIT) & 1;
+                if (md || past) {
+                    const R vx = v.vel.x[i], vy = v.vel.y[i], vz = v.vel.z[i];
+                    R f0 = flagged(v.force.x, i, md), f1 = flagged(v.force.y, i, md),
+                      f2 = flagged(v.force.z, i, md);
+                    R g0 = flagged(v.force_old.x, i, past), g1 = flagged(v.force_old.y, i, past),
+                      g2 = flagged(v.force_old.z, i, past);
+                    v.vel.x[i] = vx + dt * (f0 + g0) / 2;
+                    v.vel.y[i] = vy + dt * (f1 + g1) / 2;
+                    v.vel.z[i] = vz + dt * (f2 + g2) / 2;
+                }
+            } else {
+                v.flags[i] = f & ~(1 << WALL_BIT);
+                f = f & ~(1 << WALL_BIT);
+            }
+            if ((f >> REAC_BIT) & 1)
+                change_species_one(v, i, i - off, a, bb, L0, L1, L2, cut_c, cut_n, prob, seed, step);
+        };
+        const long long a4 = (t.begin + 3) & ~3LL, e4 = t.end & ~3LL;
+        const long long h_end = a4 < t.end ? a4 : t.end;
+        for (long long i = t.begin + threadIdx.x; i < h_end; i += blockDim.x) one(i, v.flags[i]);
+        if (a4 < e4) {
+            const int4 *f4 = (const int4 *)v.flags;
+            constexpr int U = 4;
+            for (long long q0 = a4 / 4 + threadIdx.x; q0 < e4 / 4; q0 += (long long)U * blockDim.x) {
+                int4 g[U];
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const long long q = q0 + (long long)u * blockDim.x;
+                    g[u] = q < e4 / 4 ? f4[q] : make_int4(0, 0, 0, 0);
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    if (!((g[u].x | g[u].y | g[u].z | g[u].w) & kBits)) continue;
+                    const long long i = 4 * (q0 + (long long)u * blockDim.x);
+                    one(i, g[u].x);
+                    one(i + 1, g[u].y);
+                    one(i + 2, g[u].z);
+                    one(i + 3, g[u].w);
+                }
+            }
+        }
+        const long long t_begin = e4 > h_end ? e4 : h_end;
+        for (long long i = t_begin + threadIdx.x; i < t.end; i += blockDim.x) one(i, v.flags[i]);
+        return;
+    }
+    for (long long base = t.begin + threadIdx.x; base < t.end; base += (long long)K * blockDim.x) {
+      int fk[K];
+      R vxk[K] = {}, vyk[K] = {}, vzk[K] = {};
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        const long long i = base + (long long)k * blockDim.x;
+        if (i < t.end) {
+            fk[k] = v.flags[i];
+            if (kAllVel) {
+                vxk[k] = v.vel.x[i];
+                vyk[k] = v.vel.y[i];
+                vzk[k] = v.vel.z[i];
+            }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        const long long i = base + (long long)k * blockDim.x;
+        if (i >= t.end) continue;
+        int f = fk[k];
+        if (!kAllVel && !((f >> WALL_BIT) & 1) && (((f >> MD_BIT) & 1) || ((f >> PAST_MD_BIT) & 1))) {
+            vxk[k] = v.vel.x[i];
+            vyk[k] = v.vel.y[i];
+            vzk[k] = v.vel.z[i];
+        }
+        const R vx = vxk[k], vy = vyk[k], vz = vzk[k];
+        if (!((f >> WALL_BIT) & 1)) {
+            const bool md = (f >> MD_BIT) & 1, past = (f >> PAST_MD_BIT) & 1;
+            if (md || past) {
+                R f0 = flagged(v.force.x, i, md), f1 = flagged(v.force.y, i, md), f2 = flagged(v.force.z, i, md);
+                R g0 = flagged(v.force_old.x, i, past), g1 = flagged(v.force_old.y, i, past),
+                  g2 = flagged(v.force_old.z, i, past);
+                v.vel.x[i] = vx + dt * (f0 + g0) / 2;
+                v.vel.y[i] = vy + dt * (f1 + g1) / 2;
+                v.vel.z[i] = vz + dt * (f2 + g2) / 2;
+            } else if (kAllVel) {
+                // both forces are zero: the update changes a velocity
+                // only if it is -0, so the store is kept for that case
+                const R z = 0;
+                const R nx = vx + dt * (z + z) / 2, ny = vy + dt * (z + z) / 2, nz = vz + dt * (z + z) / 2;
+                if (!same_bits(nx, vx) || !same_bits(ny, vy) || !same_bits(nz, vz)) {
+                    v.vel.x[i] = nx;
+                    v.vel.y[i] = ny;
+                    v.vel.z[i] = nz;
+                }
+            }
+        } else {
+            v.flags[i] = f & ~(1 << WALL_BIT);
+            f = f & ~(1 << WALL_BIT);
+        }
+        if ((f >> REAC_BIT) & 1)
+            change_species_one(v, i, i - off, a, bb, L0, L1, L2, cut_c, cut_n, prob, seed, step);
+      }
+    }
+}
+
+// clearing of the contribution counters over entries [bx * blockDim.x, ...)
+// of list i, strided by gx blocks
+__device__ __forceinline__ void end_reset(int i, int bx, int gx, const int *list, const int *n, int Nmax,
+                                          const unsigned char *contrib, int *ncontrib, int *max_contrib)
+{
+    for (int e = bx * blockDim.x + threadIdx.x; e < n[i]; e += gx * blockDim.x) {
+        size_t qq = (size_t)i * Nmax + e;
+        if (contrib[qq]) ncontrib[list[qq]] = 0;
+    }
+    if (bx == 0 && threadIdx.x == 0 && (i & 1) == 0) max_contrib[i >> 1] = 0;
+}
+
+// compute_force_n2, the colloid velocity half and RATTLE's velocity
+// correction of replica r
+__device__ __forceinline__ void end_colloid(int r, const BRep *rep, const PView<double> &c, const ColloidStep &cs,
+                                            const LJDev &lj_cc, unsigned *err)
+{
+    PView<double> cr = shifted(c, 2 * (long long)r, 2);
+    const double *e = rep[r].g.edges;
+    for (int m = 0; m < 2; m++)
+        force_n2_one(m, cr.pos.x, cr.pos.y, cr.pos.z, cr.species, 2, e[0], e[1], e[2], lj_cc, cr.force.x,
+                     cr.force.y, cr.force.z);
+    colloid_vv_vel_one(cr, 0, cs.mass[2 * r], cs.dt);
+    colloid_vv_vel_one(cr, 1, cs.mass[2 * r + 1], cs.dt);
+    E3 L{{e[0], e[1], e[2]}};
+    rattle_vel_dimer(cr, cs.ms, cs.d, L, err);
+}
+
+// md_vel then change_species of every solvent particle (src/md.f90:219-237,
+// programs/single_dimer_pbc.f90:511-542), one block per particle tile;
+// clearing of the per-particle contribution counters; compute_force_n2, the
+// colloid velocity half and RATTLE's velocity correction per replica
+// (src/neighbor_list.f90:227-264, programs/single_dimer_pbc.f90:356-359,
+// src/md.f90:298-319).  The last MD step of an interval ends with this
+// kernel; the others end inside kb_step_end_begin.
 template <typename R, typename V>
 __global__ void __launch_bounds__(kBT, V::MINB)
     kb_step_end(const BTile *tiles, int n_tiles, int gx, const BRep *rep, PView<R> v, PView<double> c, R dt,
@@ -488,154 +692,77 @@ __global__ void __launch_bounds__(kBT, V::MINB)
     const int b = blockIdx.x;
     if (b < n_tiles) {
         const BTile t = tiles[b];
-        const BRep &rp = rep[t.r];
         const double a[3] = {c.pos.x[2 * t.r], c.pos.y[2 * t.r], c.pos.z[2 * t.r]};
         const double bb[3] = {c.pos.x[2 * t.r + 1], c.pos.y[2 * t.r + 1], c.pos.z[2 * t.r + 1]};
-        const double L0 = rp.g.edges[0], L1 = rp.g.edges[1], L2 = rp.g.edges[2];
-        const uint64_t step = *d_step + (uint64_t)step_off;
-        const uint64_t seed = rp.seed;
-        const long long off = rp.off;
-        constexpr int K = V::KE;
-        // The FP64 form reads every velocity: a zero-force update turns a -0
-        // component into +0, as the reference's does.  The FP32 form reads
-        // velocities only for particles with a force and leaves the others'
-        // bits untouched, so it keeps a -0 component (an SRD rotation product
-        // can round to one) where the reference would store +0: equal in
-        // value, not in bits, which is why FP32 results are compared by value.
-        constexpr bool kAllVel = sizeof(R) == 8;
-        if constexpr (!kAllVel) {
-            // FP32: only particles with a WALL, MD, PAST_MD or REAC bit do
-            // anything, so the flags are read four at a time (one 16-byte
-            // load; the arrays are allocated to a multiple of 4) and a group
-            // of four without such a bit is skipped whole
-            constexpr int kBits = (1 << WALL_BIT) | (1 << MD_BIT) | (1 << PAST_MD_BIT) | (1 << REAC_BIT);
-            auto one = [&](long long i, int f) {
-                if (!(f & kBits)) return;
-                if (!((f >> WALL_BIT) & 1)) {
-                    const bool md = (f >> MD_BIT) & 1, past = (f >> PAST_MD_BIT) & 1;
-                    if (md || past) {
-                        const R vx = v.vel.x[i], vy = v.vel.y[i], vz = v.vel.z[i];
-                        R f0 = flagged(v.force.x, i, md), f1 = flagged(v.force.y, i, md),
-                          f2 = flagged(v.force.z, i, md);
-                        R g0 = flagged(v.force_old.x, i, past), g1 = flagged(v.force_old.y, i, past),
-                          g2 = flagged(v.force_old.z, i, past);
-                        v.vel.x[i] = vx + dt * (f0 + g0) / 2;
-                        v.vel.y[i] = vy + dt * (f1 + g1) / 2;
-                        v.vel.z[i] = vz + dt * (f2 + g2) / 2;
-                    }
-                } else {
-                    v.flags[i] = f & ~(1 << WALL_BIT);
-                    f = f & ~(1 << WALL_BIT);
-                }
-                if ((f >> REAC_BIT) & 1)
-                    change_species_one(v, i, i - off, a, bb, L0, L1, L2, cut_c, cut_n, prob, seed, step);
-            };
-            const long long a4 = (t.begin + 3) & ~3LL, e4 = t.end & ~3LL;
-            const long long h_end = a4 < t.end ? a4 : t.end;
-            for (long long i = t.begin + threadIdx.x; i < h_end; i += blockDim.x) one(i, v.flags[i]);
-            if (a4 < e4) {
-                const int4 *f4 = (const int4 *)v.flags;
-                constexpr int U = 4;
-                for (long long q0 = a4 / 4 + threadIdx.x; q0 < e4 / 4; q0 += (long long)U * blockDim.x) {
-                    int4 g[U];
-#pragma unroll
-                    for (int u = 0; u < U; u++) {
-                        const long long q = q0 + (long long)u * blockDim.x;
-                        g[u] = q < e4 / 4 ? f4[q] : make_int4(0, 0, 0, 0);
-                    }
-#pragma unroll
-                    for (int u = 0; u < U; u++) {
-                        if (!((g[u].x | g[u].y | g[u].z | g[u].w) & kBits)) continue;
-                        const long long i = 4 * (q0 + (long long)u * blockDim.x);
-                        one(i, g[u].x);
-                        one(i + 1, g[u].y);
-                        one(i + 2, g[u].z);
-                        one(i + 3, g[u].w);
-                    }
-                }
-            }
-            const long long t_begin = e4 > h_end ? e4 : h_end;
-            for (long long i = t_begin + threadIdx.x; i < t.end; i += blockDim.x) one(i, v.flags[i]);
-            return;
-        }
-        for (long long base = t.begin + threadIdx.x; base < t.end; base += (long long)K * blockDim.x) {
-          int fk[K];
-          R vxk[K] = {}, vyk[K] = {}, vzk[K] = {};
-#pragma unroll
-          for (int k = 0; k < K; k++) {
-            const long long i = base + (long long)k * blockDim.x;
-            if (i < t.end) {
-                fk[k] = v.flags[i];
-                if (kAllVel) {
-                    vxk[k] = v.vel.x[i];
-                    vyk[k] = v.vel.y[i];
-                    vzk[k] = v.vel.z[i];
-                }
-            }
-          }
-#pragma unroll
-          for (int k = 0; k < K; k++) {
-            const long long i = base + (long long)k * blockDim.x;
-            if (i >= t.end) continue;
-            int f = fk[k];
-            if (!kAllVel && !((f >> WALL_BIT) & 1) && (((f >> MD_BIT) & 1) || ((f >> PAST_MD_BIT) & 1))) {
-                vxk[k] = v.vel.x[i];
-                vyk[k] = v.vel.y[i];
-                vzk[k] = v.vel.z[i];
-            }
-            const R vx = vxk[k], vy = vyk[k], vz = vzk[k];
-            if (!((f >> WALL_BIT) & 1)) {
-                const bool md = (f >> MD_BIT) & 1, past = (f >> PAST_MD_BIT) & 1;
-                if (md || past) {
-                    R f0 = flagged(v.force.x, i, md), f1 = flagged(v.force.y, i, md), f2 = flagged(v.force.z, i, md);
-                    R g0 = flagged(v.force_old.x, i, past), g1 = flagged(v.force_old.y, i, past),
-                      g2 = flagged(v.force_old.z, i, past);
-                    v.vel.x[i] = vx + dt * (f0 + g0) / 2;
-                    v.vel.y[i] = vy + dt * (f1 + g1) / 2;
-                    v.vel.z[i] = vz + dt * (f2 + g2) / 2;
-                } else if (kAllVel) {
-                    // both forces are zero: the update changes a velocity
-                    // only if it is -0, so the store is kept for that case
-                    const R z = 0;
-                    const R nx = vx + dt * (z + z) / 2, ny = vy + dt * (z + z) / 2, nz = vz + dt * (z + z) / 2;
-                    if (!same_bits(nx, vx) || !same_bits(ny, vy) || !same_bits(nz, vz)) {
-                        v.vel.x[i] = nx;
-                        v.vel.y[i] = ny;
-                        v.vel.z[i] = nz;
-                    }
-                }
-            } else {
-                v.flags[i] = f & ~(1 << WALL_BIT);
-                f = f & ~(1 << WALL_BIT);
-            }
-            if ((f >> REAC_BIT) & 1)
-                change_species_one(v, i, i - off, a, bb, L0, L1, L2, cut_c, cut_n, prob, seed, step);
-          }
-        }
+        end_tile<R, V::KE>(t, rep[t.r], v, a, bb, dt, cut_c, cut_n, prob, *d_step + (uint64_t)step_off);
         return;
     }
     const int n_reset = gx * 2 * cs.R;
     if (b < n_tiles + n_reset) {
-        const int q = b - n_tiles, i = q / gx, bx = q % gx;
-        for (int e = bx * blockDim.x + threadIdx.x; e < n[i]; e += gx * blockDim.x) {
-            size_t qq = (size_t)i * Nmax + e;
-            if (contrib[qq]) ncontrib[list[qq]] = 0;
-        }
-        if (bx == 0 && threadIdx.x == 0 && (i & 1) == 0) max_contrib[i >> 1] = 0;
+        const int q = b - n_tiles;
+        end_reset(q / gx, q % gx, gx, list, n, Nmax, contrib, ncontrib, max_contrib);
         return;
     }
     for (int r = (b - n_tiles - n_reset) * blockDim.x + threadIdx.x; r < cs.R;
-         r += (gridDim.x - n_tiles - n_reset) * blockDim.x) {
-        PView<double> cr = shifted(c, 2 * (long long)r, 2);
-        const double *e = rep[r].g.edges;
-        for (int m = 0; m < 2; m++)
-            force_n2_one(m, cr.pos.x, cr.pos.y, cr.pos.z, cr.species, 2, e[0], e[1], e[2], lj_cc, cr.force.x,
-                         cr.force.y, cr.force.z);
-        colloid_vv_vel_one(cr, 0, cs.mass[2 * r], cs.dt);
-        colloid_vv_vel_one(cr, 1, cs.mass[2 * r + 1], cs.dt);
-        E3 L{{e[0], e[1], e[2]}};
-        rattle_vel_dimer(cr, cs.ms, cs.d, L, err);
+         r += (gridDim.x - n_tiles - n_reset) * blockDim.x)
+        end_colloid(r, rep, c, cs, lj_cc, err);
+}
+
+// The end of MD step k and the beginning of MD step k + 1 in one launch
+// (no re-sort falls between them, and both halves see the same force /
+// force_old parity): each particle tile's block runs the end half over its
+// tile, then the beginning half; the clearing of the contribution counters
+// and the colloid velocity half run in their own blocks as in kb_step_end.
+// With V::FIRST, block 0 runs each replica's colloid velocity half and then
+// its colloid position half (one thread per replica, in that order); without
+// it the velocity halves run in the colloid blocks and the position halves in
+// the last block, after every other block has finished.  change_species reads
+// the colloid positions of step k from csnap (written by kb_pair_forces), as
+// block 0 may already be moving the colloids.
+template <typename R, typename V>
+__global__ void __launch_bounds__(kBT, V::MINB)
+    kb_step_end_begin(const BTile *tiles, int n_tiles, int gx, const BRep *rep, PView<R> v, Vec3<R> old,
+                      PView<double> c, R dt, R dt_sq, double cut_c, double cut_n, double prob, const uint64_t *d_step,
+                      int step_off, const int *list, const int *n, int Nmax, const unsigned char *contrib,
+                      int *ncontrib, int *max_contrib, const double *csnap, LJDev lj_cc, unsigned long long *so_max,
+                      unsigned *done, int *resort, int *n_extra, ColloidStep cs, ResortLists rl,
+                      cudaGraphConditionalHandle cond, int use_cond, int read_species, unsigned *err)
+{
+    __shared__ int s_last;
+    __shared__ int ws[kBT / 32 + 1];
+    __shared__ double s_max[kBT / 32];
+    constexpr bool kFirst = V::FIRST;
+    const int n_reset = gx * 2 * cs.R;
+    double m = 0;
+    int r_tile = -1;
+    if (kFirst && blockIdx.x == 0) {
+        for (int r = threadIdx.x; r < cs.R; r += blockDim.x) {
+            end_colloid(r, rep, c, cs, lj_cc, err);
+            cs.co_max[r] = colloid_begin(r, rep, cs.c, cs.cold, cs.c_next, cs.rat, cs.mass, cs.ms, cs.d, cs.dt, err);
+        }
+    } else {
+        const int b = blockIdx.x - (kFirst ? 1 : 0);
+        if (b < n_tiles) {
+            const BTile t = tiles[b];
+            const double *p = csnap + 6 * (size_t)t.r;
+            const double a[3] = {p[0], p[1], p[2]}, bb[3] = {p[3], p[4], p[5]};
+            end_tile<R, V::KE>(t, rep[t.r], v, a, bb, dt, cut_c, cut_n, prob, *d_step + (uint64_t)step_off);
+            // the beginning half reads what the end half wrote: velocities,
+            // flags, species, force_old entries
+            __syncthreads();
+            r_tile = t.r;
+            m = begin_tile<R, V::KB>(t, v, old, v.force_old, dt, dt_sq, read_species);
+        } else if (b < n_tiles + n_reset) {
+            const int q = b - n_tiles;
+            end_reset(q / gx, q % gx, gx, list, n, Nmax, contrib, ncontrib, max_contrib);
+        } else if (!kFirst) {
+            const int nb = gridDim.x - n_tiles - n_reset;
+            for (int r = (b - n_tiles - n_reset) * blockDim.x + threadIdx.x; r < cs.R; r += nb * blockDim.x)
+                end_colloid(r, rep, c, cs, lj_cc, err);
+        }
     }
+    if (!block_done(m, r_tile, so_max, done, s_max, &s_last)) return;
+    begin_tail<kFirst>(rep, so_max, done, resort, n_extra, cs, rl, cond, use_cond, err, ws);
 }
 
 // ------------------------------------------------------ re-sort / sort
@@ -1050,6 +1177,23 @@ static void capture_conditional_resort(Batch *b, cudaStream_t st, cudaGraph_t g,
     note(b, cudaStreamEndCapture(b->body, &out));
 }
 
+// a fresh IF-node handle in the graph being captured on st (0 when not
+// capturing)
+static cudaGraphConditionalHandle new_cond(Batch *b, cudaStream_t st)
+{
+    cudaGraphConditionalHandle cond = 0;
+    if (b->capturing) {
+        cudaStreamCaptureStatus st_cap;
+        cudaGraph_t g = nullptr;
+        note(b, cudaStreamGetCaptureInfo(st, &st_cap, nullptr, &g, nullptr, nullptr));
+        note(b, cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
+    }
+    return cond;
+}
+
+// MD step k of the interval: its beginning (for k = 0; later steps begin in
+// the previous step's kb_step_end_begin), the re-sort test, the forces and
+// its end, merged with the beginning of step k + 1 unless k is the last
 template <typename R, typename V>
 static void md_step_launches(Batch *b, int k)
 {
@@ -1062,40 +1206,54 @@ static void md_step_launches(Batch *b, int k)
     PView<double> ca = phys<double>(b->col, 1);
     ColloidStep cs{c, ca.pos, c.force_old, {b->rattle[0], b->rattle[1], b->rattle[2]}, b->vv_mass, b->ms,
                    b->prm.bond, dt, b->prm.skin, b->R, b->co_max};
-    cudaGraphConditionalHandle cond = 0;
-    cudaGraph_t g = nullptr;
+    const ResortLists rl{b->ptile_first, b->ptile_count, b->stile_first, b->stile_count, b->act_p, b->act_s, b->n_act};
+    const int use_cond = b->capturing ? 1 : 0, read_species = b->read_species ? 1 : 0;
+    cudaGraphConditionalHandle cond = b->cond_next;
+    if (k == 0) {
+        cond = new_cond(b, st);
+        kb_step_begin<R, V><<<b->n_ptile + (V::FIRST ? 1 : 0), kBT, 0, st>>>(
+            b->ptile, b->rep, s, alt.pos, s.force_old, (R)dt, (R)dt_sq, b->so_max, b->done, b->resort, b->n_extra,
+            cs, rl, cond, use_cond, read_species, dev_error_word());
+    }
     if (b->capturing) {
         cudaStreamCaptureStatus st_cap;
+        cudaGraph_t g = nullptr;
         note(b, cudaStreamGetCaptureInfo(st, &st_cap, nullptr, &g, nullptr, nullptr));
-        note(b, cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
+        capture_conditional_resort<R>(b, st, g, cond);
+    } else {
+        resort_launches<R>(b, b->resort, false, st, -1);
     }
-    kb_step_begin<R, V><<<b->n_ptile + (V::FIRST ? 1 : 0), kBT, 0, st>>>(b->ptile, b->rep, s, alt.pos, s.force_old, (R)dt, (R)dt_sq,
-                                                 b->so_max, b->done, b->resort, b->n_extra, cs,
-                                                 ResortLists{b->ptile_first, b->ptile_count, b->stile_first,
-                                                             b->stile_count, b->act_p, b->act_s, b->n_act},
-                                                 cond, b->capturing ? 1 : 0, b->read_species ? 1 : 0,
-                                                 dev_error_word());
-    if (b->capturing) capture_conditional_resort<R>(b, st, g, cond);
-    else resort_launches<R>(b, b->resort, false, st, -1);
     // switch_force: the cleared entries become `force`
     b->parity ^= 1;
     s = live<R>(b->sol, b->parity);
     c = live<double>(b->col, b->parity);
     cs.c = c;
+    cs.c_next = c.force_old;
     const int per = 256 * kListPer[shape_list(b->shape)];
     int gx = (b->Nmax + per - 1) / per;
     if (gx > 64) gx = 64;
     if (gx < 1) gx = 1;
     kb_pair_forces<R><<<dim3(gx, 2 * b->R), 256, 0, st>>>(b->rep, c, s, b->list, b->nn, b->Nmax, b->lj_sc, b->pair_f,
                                                           b->pair_e, b->contrib, b->ncontrib, b->max_contrib,
-                                                          b->prm.cut_sq_C);
+                                                          b->prm.cut_sq_C, b->csnap);
     kb_apply_sum<R><<<gx * 2 * b->R + 3 * b->R, 256, 0, st>>>(
         b->rep, b->R, gx, b->list, b->nn, b->Nmax, b->contrib, b->pair_f, b->ncontrib, b->max_contrib, s.force.x,
         s.force.y, s.force.z, c.force.x, c.force.y, c.force.z, b->clist, b->cn);
     const int n_col_blocks = (b->R + kBT - 1) / kBT;
-    kb_step_end<R, V><<<b->n_ptile + gx * 2 * b->R + n_col_blocks, kBT, 0, st>>>(
-        b->ptile, b->n_ptile, gx, b->rep, s, c, (R)dt, b->prm.cut_sq_C, b->prm.cut_sq_N, b->prm.prob, b->d_step, k,
-        b->list, b->nn, b->Nmax, b->contrib, b->ncontrib, b->max_contrib, cs, b->lj_cc, dev_error_word());
+    const int n_reset = gx * 2 * b->R;
+    if (k + 1 < b->prm.N_MD) {
+        b->cond_next = new_cond(b, st);
+        kb_step_end_begin<R, V><<<(V::FIRST ? 1 : n_col_blocks) + b->n_ptile + n_reset, kBT, 0, st>>>(
+            b->ptile, b->n_ptile, gx, b->rep, s, alt.pos, c, (R)dt, (R)dt_sq, b->prm.cut_sq_C, b->prm.cut_sq_N,
+            b->prm.prob, b->d_step, k, b->list, b->nn, b->Nmax, b->contrib, b->ncontrib, b->max_contrib, b->csnap,
+            b->lj_cc, b->so_max, b->done, b->resort, b->n_extra, cs, rl, b->cond_next, use_cond, read_species,
+            dev_error_word());
+    } else {
+        b->cond_next = 0;
+        kb_step_end<R, V><<<b->n_ptile + n_reset + n_col_blocks, kBT, 0, st>>>(
+            b->ptile, b->n_ptile, gx, b->rep, s, c, (R)dt, b->prm.cut_sq_C, b->prm.cut_sq_N, b->prm.prob, b->d_step,
+            k, b->list, b->nn, b->Nmax, b->contrib, b->ncontrib, b->max_contrib, cs, b->lj_cc, dev_error_word());
+    }
 }
 
 template <typename R>
@@ -1174,7 +1332,7 @@ static void free_batch(Batch *b)
     rmpcd_particles_destroy(b->col);
     void *ptrs[] = {b->rep, b->ptile, b->stile, b->stile_first, b->stile_count, b->tile_sum, b->tile_off, b->count,
                     b->start, b->cursor, b->is_md, b->is_reac, b->stencil, b->list, b->nn, b->pair_f, b->pair_e,
-                    b->contrib, b->ncontrib, b->max_contrib, b->clist, b->cn, b->so_max, b->co_max, b->resort,
+                    b->contrib, b->ncontrib, b->max_contrib, b->clist, b->cn, b->so_max, b->co_max, b->csnap, b->resort,
                     b->n_extra,
                     b->big, b->n_big, b->rattle[0], b->rattle[1], b->rattle[2], b->vv_mass, b->d_step, b->done,
                     b->ptile_first, b->ptile_count, b->act_p, b->act_s, b->n_act, b->all_p, b->all_s, b->n_all};
@@ -1387,7 +1545,7 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
               !dalloc(&b->pair_f, 3 * ne) && !dalloc(&b->pair_e, ne) && !dalloc(&b->contrib, ne) &&
               !dalloc(&b->ncontrib, off) && !dalloc(&b->max_contrib, R) && !dalloc(&b->clist, ne) &&
               !dalloc(&b->cn, 2 * (size_t)R) && !dalloc(&b->so_max, R) && !dalloc(&b->co_max, R) &&
-              !dalloc(&b->resort, R) &&
+              !dalloc(&b->csnap, 6 * (size_t)R) && !dalloc(&b->resort, R) &&
               !dalloc(&b->n_extra, R) && !dalloc(&b->big, soff) && !dalloc(&b->n_big, 1) &&
               !dalloc(&b->rattle[0], 2 * (size_t)R) && !dalloc(&b->rattle[1], 2 * (size_t)R) &&
               !dalloc(&b->rattle[2], 2 * (size_t)R) && !dalloc(&b->vv_mass, 2 * (size_t)R) && !dalloc(&b->d_step, 1) &&

@@ -103,10 +103,20 @@ __global__ void k_apply_multi(const int *list, const int *n, int C, int Nmax, co
 }
 
 // f1 = sum of the pair forces in list order; force(:,i) = force(:,i) + f1
+// (kSum = false: only the contributing entries compacted into clist / cn)
+template <bool kSum>
 __global__ void k_colloid_sum(const int *n, int Nmax, const unsigned char *contrib, const double *pf,
                               double *cfx, double *cfy, double *cfz, int *clist, int *cn)
 {
-    colloid_sum_block(blockIdx.x, n, Nmax, contrib, pf, cfx, cfy, cfz, clist, cn);
+    colloid_sum_block<kSum>(blockIdx.x, n, Nmax, contrib, pf, cfx, cfy, cfz, clist, cn);
+}
+
+// the FP32 form: f1 by the fixed tree of colloid_tree_block
+__global__ void __launch_bounds__(kNlBlockThreads) k_colloid_tree(const int *n, int Nmax, const unsigned char *contrib,
+                                                                  const double *pf, double *cfx, double *cfy,
+                                                                  double *cfz)
+{
+    colloid_tree_block(blockIdx.x, n, Nmax, contrib, pf, cfx, cfy, cfz);
 }
 
 // Sequential sum e = (((0 + t_0) + t_1) + ...) of `total` terms, one block:
@@ -500,8 +510,18 @@ int compute_force_impl(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist *
                                                     nl->ncontrib, max_contrib, serial, v.force.x, v.force.y, v.force.z, nl->mkeys,
                                                    m_count);
         }
-        k_colloid_sum<<<C, kNlThreads, 0, s>>>(nl->n, nl->Nmax, nl->contrib, nl->pair_f, cv.force.x, cv.force.y,
-                                               cv.force.z, clist, cn);
+        // the colloid sums: list order in the FP64 form, the fixed tree in the
+        // FP32 form (whose energy still needs the compacted entries)
+        if (ps2->precision == RMPCD_FP32) {
+            k_colloid_tree<<<C, kNlBlockThreads, 0, s>>>(nl->n, nl->Nmax, nl->contrib, nl->pair_f, cv.force.x,
+                                                         cv.force.y, cv.force.z);
+            if (energy)
+                k_colloid_sum<false><<<C, kNlThreads, 0, s>>>(nl->n, nl->Nmax, nl->contrib, nl->pair_f, cv.force.x,
+                                                              cv.force.y, cv.force.z, clist, cn);
+        } else {
+            k_colloid_sum<true><<<C, kNlThreads, 0, s>>>(nl->n, nl->Nmax, nl->contrib, nl->pair_f, cv.force.x,
+                                                         cv.force.y, cv.force.z, clist, cn);
+        }
         k_reset_contrib<<<grid, 256, 0, s>>>(nl->list, nl->n, nl->Nmax, nl->contrib, nl->ncontrib);
         if (energy) k_energy<<<1, 1024, 0, s>>>(cn, clist, C, nl->Nmax, nl->pair_e, nl->e_pre, e_out);
         RMPCD_CHECK_LAUNCH();

@@ -460,6 +460,8 @@ __device__ inline void colloid_sum_load(int i, int e_first, int ni, int Nmax, co
     }
 }
 
+// (kSum = false: the compaction into clist / cn alone, the force untouched)
+template <bool kSum = true>
 __device__ inline void colloid_sum_block(int i, const int *n, int Nmax, const unsigned char *contrib, const double *pf,
                                          double *cfx, double *cfy, double *cfz, int *clist, int *cn)
 {
@@ -492,7 +494,7 @@ __device__ inline void colloid_sum_block(int i, const int *n, int Nmax, const un
         const int cnt = s_cnt;
         // the next chunk's run
         colloid_sum_load(i, e_first + kCollSumChunk, ni, Nmax, contrib, pf, cmask, f);
-        if (t < 3) {
+        if (kSum && t < 3) {
 #pragma unroll 8
             for (int q = 0; q < cnt; q++) acc = acc + vals[t][q];
         }
@@ -500,13 +502,83 @@ __device__ inline void colloid_sum_block(int i, const int *n, int Nmax, const un
         total += cnt;
         __syncthreads();
     }
+    if (t == 0) cn[i] = total;
+    if (!kSum) return;
     if (t == 0) {
         cfx[i] = cfx[i] + acc;
-        cn[i] = total;
     } else if (t == 1) {
         cfy[i] = cfy[i] + acc;
     } else if (t == 2) {
         cfz[i] = cfz[i] + acc;
+    }
+}
+
+// The FP32 form's colloid force sum: f1 = the sum of colloid i's pair forces
+// in FP64 by a fixed tree, force(:,i) += f1 (one block of kNlBlockThreads).
+// Thread t adds the contributing entries t, t + T, t + 2T, ... (T threads) in
+// that order; the threads' sums are combined by xor butterflies inside each
+// warp, then the warps' sums by one more butterfly over warp numbers.  The
+// order depends on the list alone, not on the grid, so every launch shape
+// gives the same bits; it is not list order, which only the FP64 form keeps.
+constexpr int kCollTreePer = 4;
+
+__device__ inline void colloid_tree_block(int i, const int *n, int Nmax, const unsigned char *contrib,
+                                          const double *pf, double *cfx, double *cfy, double *cfz)
+{
+    __shared__ double wsum[3][kNlBlockThreads / 32];
+    const int ni = n[i];
+    const size_t base = (size_t)i * Nmax;
+    double a0 = 0, a1 = 0, a2 = 0;
+    for (int e0 = threadIdx.x; e0 < ni; e0 += kCollTreePer * kNlBlockThreads) {
+        double f[kCollTreePer][3];
+        bool c[kCollTreePer];
+#pragma unroll
+        for (int u = 0; u < kCollTreePer; u++) {
+            const int e = e0 + u * kNlBlockThreads;
+            c[u] = e < ni && contrib[base + e];
+            if (c[u]) {
+                const size_t q = base + e;
+                f[u][0] = pf[3 * q];
+                f[u][1] = pf[3 * q + 1];
+                f[u][2] = pf[3 * q + 2];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kCollTreePer; u++)
+            if (c[u]) {
+                a0 = a0 + f[u][0];
+                a1 = a1 + f[u][1];
+                a2 = a2 + f[u][2];
+            }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a0 = a0 + __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 = a1 + __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 = a2 + __shfl_xor_sync(0xffffffffu, a2, o);
+    }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        wsum[0][w] = a0;
+        wsum[1][w] = a1;
+        wsum[2][w] = a2;
+    }
+    __syncthreads();
+    if (w == 0) {
+        constexpr int NW = kNlBlockThreads / 32;
+        double b0 = lane < NW ? wsum[0][lane] : 0.0, b1 = lane < NW ? wsum[1][lane] : 0.0,
+               b2 = lane < NW ? wsum[2][lane] : 0.0;
+#pragma unroll
+        for (int o = NW / 2; o > 0; o >>= 1) {
+            b0 = b0 + __shfl_xor_sync(0xffffffffu, b0, o);
+            b1 = b1 + __shfl_xor_sync(0xffffffffu, b1, o);
+            b2 = b2 + __shfl_xor_sync(0xffffffffu, b2, o);
+        }
+        if (lane == 0) {
+            cfx[i] = cfx[i] + b0;
+            cfy[i] = cfy[i] + b1;
+            cfz[i] = cfz[i] + b2;
+        }
     }
 }
 
