@@ -487,7 +487,7 @@ int rmpcd_dimer_batch_info(const rmpcd_dimer_batch *batch, int *n_replicas, long
                            int *n_extra_sorting);
 /* Engine shapes (no counterpart in the reference): particles per tile of
  * the solvent kernels, particles per thread and pass of the MD step's
- * begin / end kernels, the blocks per SM they are compiled for, the list
+ * begin / end halves, the blocks per SM they are compiled for, the list
  * entries per thread of the list kernels (pair forces, their application,
  * the contribution reset), and whether the colloid half of the step begin
  * runs in an extra first block while the solvent streams (1) or in the block

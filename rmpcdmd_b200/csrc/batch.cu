@@ -95,6 +95,7 @@ struct BTile {
     long long begin, end;
 };
 
+
 struct BRep {
     long long off;  // first solvent particle of the replica
     int n;          // its solvent particles
@@ -151,6 +152,7 @@ struct rmpcd_dimer_batch {
     uint64_t step = 0;  // host copy of every replica's RNG step
     rmpcd::Masses ms{};
     rmpcd::LJDev lj_sc{}, lj_cc{};
+    rmpcd::LJDev *lj_dev = nullptr;  // device copies of lj_sc, lj_cc
     int parity = 0;  // 0: force = buffer force[0], force_old = force_old[0]; swapped by each MD step
     unsigned *done = nullptr;   // blocks finished in the current step kernel (last-block hand-off)
     bool use_graph = true;
@@ -158,6 +160,9 @@ struct rmpcd_dimer_batch {
     cudaError_t cap_err = cudaSuccess;
     cudaStream_t body = nullptr;  // captures the bodies of the re-sort IF nodes
     cudaGraphConditionalHandle cond_next = 0;  // re-sort condition of the next MD step, while capturing
+    cudaStream_t side = nullptr;   // captures the speculative force branch beside each re-sort IF node
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    int *any = nullptr;  // 1 when the last MD-step beginning decided to re-sort some replica
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
 };
 
@@ -365,11 +370,9 @@ __device__ __forceinline__ double begin_tile(const BTile &t, const PView<R> &v, 
     return m;
 }
 
-// the block's maximum displacement into its replica's so_max (r_tile < 0:
-// a block without particles), then the last-block hand-off: true in the one
-// block of the grid that finishes last
-__device__ __forceinline__ bool block_done(double m, int r_tile, unsigned long long *so_max, unsigned *done,
-                                           double *s_max, int *s_last)
+// the block's maximum displacement (m, one value per thread) into its
+// replica's so_max (r_tile < 0: a block without particles)
+__device__ __forceinline__ void block_max_into(double m, int r_tile, unsigned long long *so_max, double *s_max)
 {
     m = warp_max(m);
     if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = m;
@@ -379,6 +382,15 @@ __device__ __forceinline__ bool block_done(double m, int r_tile, unsigned long l
         // one atomic per block, skipped when it cannot raise the maximum
         if (r_tile >= 0 && m > __longlong_as_double((long long)__ldcg(so_max + r_tile)))
             atomic_max_nonneg(so_max + r_tile, m);
+    }
+    __syncthreads();
+}
+
+// the last-block hand-off: true in the one block of the grid that finishes
+// last (every block calls it once, after its last write)
+__device__ __forceinline__ bool block_finish(unsigned *done, int *s_last)
+{
+    if (threadIdx.x == 0) {
         __threadfence();
         *s_last = atomicAdd(done, 1u) == gridDim.x - 1;
     }
@@ -386,13 +398,22 @@ __device__ __forceinline__ bool block_done(double m, int r_tile, unsigned long l
     return *s_last;
 }
 
+__device__ __forceinline__ bool block_done(double m, int r_tile, unsigned long long *so_max, unsigned *done,
+                                           double *s_max, int *s_last)
+{
+    block_max_into(m, r_tile, so_max, s_max);
+    return block_finish(done, s_last);
+}
+
 // the last block's part of an MD step's beginning: the colloid half of every
 // replica unless an earlier block did it (kFirst), the re-sort decisions, the
 // tile lists of the replicas to re-sort and the graph's re-sort condition
+// (any_out, if given, receives whether some replica re-sorts)
 template <bool kFirst>
 __device__ __forceinline__ void begin_tail(const BRep *rep, unsigned long long *so_max, unsigned *done, int *resort,
                                            int *n_extra, const ColloidStep &cs, const ResortLists &rl,
-                                           cudaGraphConditionalHandle cond, int use_cond, unsigned *err, int *ws)
+                                           cudaGraphConditionalHandle cond, int use_cond, unsigned *err, int *ws,
+                                           int *any_out = nullptr)
 {
     __threadfence();
     int any = 0, base_p = 0, base_s = 0;
@@ -420,7 +441,9 @@ __device__ __forceinline__ void begin_tail(const BRep *rep, unsigned long long *
         rl.n[0] = base_p;
         rl.n[1] = base_s;
         if (use_cond && any) cudaGraphSetConditional(cond, 1);
+        if (any_out) *any_out = any;
         *done = 0;
+        __threadfence();
     }
 }
 
@@ -439,7 +462,8 @@ template <typename R, typename V>
 __global__ void __launch_bounds__(kBT, V::MINB)
     kb_step_begin(const BTile *tiles, const BRep *rep, PView<R> v, Vec3<R> old, Vec3<R> next, R dt, R dt_sq,
                   unsigned long long *so_max, unsigned *done, int *resort, int *n_extra, ColloidStep cs,
-                  ResortLists rl, cudaGraphConditionalHandle cond, int use_cond, int read_species, unsigned *err)
+                  ResortLists rl, cudaGraphConditionalHandle cond, int use_cond, int read_species, unsigned *err,
+                  int *any_out)
 {
     __shared__ int s_last;
     __shared__ int ws[kBT / 32 + 1];
@@ -456,7 +480,7 @@ __global__ void __launch_bounds__(kBT, V::MINB)
         m = begin_tile<R, V::KB>(t, v, old, next, dt, dt_sq, read_species);
     }
     if (!block_done(m, r_tile, so_max, done, s_max, &s_last)) return;
-    begin_tail<kFirst>(rep, so_max, done, resort, n_extra, cs, rl, cond, use_cond, err, ws);
+    begin_tail<kFirst>(rep, so_max, done, resort, n_extra, cs, rl, cond, use_cond, err, ws, any_out);
 }
 
 // list pair forces (src/neighbor_list.f90:198-219) fused with
@@ -464,19 +488,20 @@ __global__ void __launch_bounds__(kBT, V::MINB)
 // both only read positions and species and OR bits into flags.  Block (0, i)
 // also copies colloid i's position to csnap[3 i ..], the positions that the
 // step's change_species uses.
+// block bx of the gx blocks of colloid i's list
 template <typename R>
-__global__ void kb_pair_forces(const BRep *rep, PView<double> c, PView<R> s, const int *list, const int *n, int Nmax,
-                               LJDev lj, double *pf, double *pe, unsigned char *contrib, int *ncontrib,
-                               int *max_contrib, double flag_cut_sq, double *csnap)
+__device__ __forceinline__ void pair_vblock(int bx, int i, int gx, const BRep *rep, const PView<double> &c,
+                                            const PView<R> &s, const int *list, const int *n, int Nmax,
+                                            const LJDev &lj, double *pf, double *pe, unsigned char *contrib,
+                                            int *ncontrib, int *max_contrib, double flag_cut_sq, double *csnap)
 {
-    const int i = blockIdx.y;
     const int r = i >> 1;
     const int ni = n[i];
     const double x[3] = {c.pos.x[i], c.pos.y[i], c.pos.z[i]};
-    if (blockIdx.x == 0 && threadIdx.x < 3) csnap[3 * i + threadIdx.x] = x[threadIdx.x];
+    if (bx == 0 && threadIdx.x < 3) csnap[3 * i + threadIdx.x] = x[threadIdx.x];
     const int s1 = c.species[i];
     const double L0 = rep[r].g.edges[0], L1 = rep[r].g.edges[1], L2 = rep[r].g.edges[2];
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ni; e += gridDim.x * blockDim.x) {
+    for (int e = bx * blockDim.x + threadIdx.x; e < ni; e += gx * blockDim.x) {
         size_t q = (size_t)i * Nmax + e;
         pair_force_entry(q, x, s1, s.pos.x, s.pos.y, s.pos.z, s.species, s.flags, list, L0, L1, L2, lj, pf, pe,
                          contrib, ncontrib, max_contrib + r);
@@ -485,17 +510,29 @@ __global__ void kb_pair_forces(const BRep *rep, PView<double> c, PView<R> s, con
     }
 }
 
+// skip (if given): the MD step's beginning decided to re-sort, so this
+// launch is the graph's speculative one and the re-sort branch evaluates the
+// forces instead
+template <typename R>
+__global__ void kb_pair_forces(const BRep *rep, PView<double> c, PView<R> s, const int *list, const int *n, int Nmax,
+                               LJDev lj, double *pf, double *pe, unsigned char *contrib, int *ncontrib,
+                               int *max_contrib, double flag_cut_sq, double *csnap, const int *skip)
+{
+    if (skip && *(const volatile int *)skip) return;
+    pair_vblock<R>(blockIdx.x, blockIdx.y, gridDim.x, rep, c, s, list, n, Nmax, lj, pf, pe, contrib, ncontrib,
+                   max_contrib, flag_cut_sq, csnap);
+}
+
 // the three consumers of the pair forces, on disjoint data: solvent
 // particles with one contribution, those with several (per replica, in
 // order), and the colloid sums (list order in the FP64 form, a fixed tree in
-// the FP32 form)
+// the FP32 form); b numbers the gx * 2R + 3R blocks of the three
 template <typename R>
-__global__ void kb_apply_sum(const BRep *rep, int R_, int gx, const int *list, const int *n, int Nmax,
-                             const unsigned char *contrib, const double *pf, const int *ncontrib,
-                             const int *max_contrib, R *fx, R *fy, R *fz, double *cfx, double *cfy, double *cfz,
-                             int *clist, int *cn)
+__device__ __forceinline__ void apply_vblock(int b, const BRep *rep, int R_, int gx, const int *list, const int *n,
+                                             int Nmax, const unsigned char *contrib, const double *pf,
+                                             const int *ncontrib, const int *max_contrib, R *fx, R *fy, R *fz,
+                                             double *cfx, double *cfy, double *cfz, int *clist, int *cn)
 {
-    const int b = blockIdx.x;
     const int n_single = gx * 2 * R_;
     if (b < n_single) {
         const int i = b / gx, bx = b % gx;
@@ -514,11 +551,17 @@ __global__ void kb_apply_sum(const BRep *rep, int R_, int gx, const int *list, c
     }
 }
 
-// md_vel then change_species of every solvent particle (src/md.f90:219-237,
-// programs/single_dimer_pbc.f90:511-542); clearing of the per-particle
-// contribution counters; compute_force_n2, the colloid velocity half and
-// RATTLE's velocity correction per replica (src/neighbor_list.f90:227-264,
-// programs/single_dimer_pbc.f90:356-359, src/md.f90:298-319)
+template <typename R>
+__global__ void kb_apply_sum(const BRep *rep, int R_, int gx, const int *list, const int *n, int Nmax,
+                             const unsigned char *contrib, const double *pf, const int *ncontrib,
+                             const int *max_contrib, R *fx, R *fy, R *fz, double *cfx, double *cfy, double *cfz,
+                             int *clist, int *cn, const int *skip)
+{
+    if (skip && *(const volatile int *)skip) return;
+    apply_vblock<R>(blockIdx.x, rep, R_, gx, list, n, Nmax, contrib, pf, ncontrib, max_contrib, fx, fy, fz, cfx, cfy,
+                    cfz, clist, cn);
+}
+
 // the solvent half over the particle tile t of replica rp, whose colloid
 // positions are a and bb; step is the random-number step of change_species
 template <typename R, int K>
@@ -708,6 +751,73 @@ __global__ void __launch_bounds__(kBT, V::MINB)
         end_colloid(r, rep, c, cs, lj_cc, err);
 }
 
+// The arguments of the MD-step halves: the solvent view v and colloid view c
+// with the force / force_old parity of the step whose forces were computed
+// last, and what the halves read besides.
+template <typename R>
+struct StepArgs {
+    const BTile *tiles;
+    int n_tiles, gx;
+    const BRep *rep;
+    PView<R> v;
+    Vec3<R> old;  // solvent pos_old
+    PView<double> c;
+    R dt, dt_sq;
+    double cut_c, cut_n, prob;
+    const uint64_t *d_step;
+    const int *list, *n;
+    int Nmax;
+    const unsigned char *contrib;
+    int *ncontrib, *max_contrib;
+    const double *csnap;
+    const LJDev *lj_cc;  // in device memory
+    int read_species;
+    unsigned *err;
+};
+
+// block b of the end of step k (RNG step offset step_off) merged with the
+// beginning of step k + 1: [V::FIRST: one block for the colloids] n_tiles
+// particle tiles, gx * 2R counter-clearing blocks, [without V::FIRST: n_col
+// colloid velocity-half blocks].  Returns the thread's largest squared
+// displacement and sets r_tile to the tile's replica (-1 for other blocks).
+template <typename R, typename V>
+__device__ __forceinline__ double eb_vblock(int b, int n_col, const StepArgs<R> &a, const ColloidStep &cs,
+                                            int step_off, int &r_tile)
+{
+    constexpr bool kFirst = V::FIRST;
+    const int n_reset = a.gx * 2 * cs.R;
+    r_tile = -1;
+    if (kFirst && b == 0) {
+        for (int r = threadIdx.x; r < cs.R; r += blockDim.x) {
+            end_colloid(r, a.rep, a.c, cs, *a.lj_cc, a.err);
+            cs.co_max[r] = colloid_begin(r, a.rep, cs.c, cs.cold, cs.c_next, cs.rat, cs.mass, cs.ms, cs.d, cs.dt,
+                                         a.err);
+        }
+        return 0;
+    }
+    b -= kFirst ? 1 : 0;
+    if (b < a.n_tiles) {
+        const BTile t = a.tiles[b];
+        const double *p = a.csnap + 6 * (size_t)t.r;
+        const double ca[3] = {p[0], p[1], p[2]}, cb[3] = {p[3], p[4], p[5]};
+        end_tile<R, V::KE>(t, a.rep[t.r], a.v, ca, cb, a.dt, a.cut_c, a.cut_n, a.prob,
+                           *a.d_step + (uint64_t)step_off);
+        // the beginning half reads what the end half wrote: velocities,
+        // flags, species, force_old entries
+        __syncthreads();
+        r_tile = t.r;
+        return begin_tile<R, V::KB>(t, a.v, a.old, a.v.force_old, a.dt, a.dt_sq, a.read_species);
+    }
+    if (b < a.n_tiles + n_reset) {
+        const int q = b - a.n_tiles;
+        end_reset(q / a.gx, q % a.gx, a.gx, a.list, a.n, a.Nmax, a.contrib, a.ncontrib, a.max_contrib);
+    } else if (!kFirst) {
+        for (int r = (b - a.n_tiles - n_reset) * blockDim.x + threadIdx.x; r < cs.R; r += n_col * blockDim.x)
+            end_colloid(r, a.rep, a.c, cs, *a.lj_cc, a.err);
+    }
+    return 0;
+}
+
 // The end of MD step k and the beginning of MD step k + 1 in one launch
 // (no re-sort falls between them, and both halves see the same force /
 // force_old parity): each particle tile's block runs the end half over its
@@ -721,48 +831,18 @@ __global__ void __launch_bounds__(kBT, V::MINB)
 // block 0 may already be moving the colloids.
 template <typename R, typename V>
 __global__ void __launch_bounds__(kBT, V::MINB)
-    kb_step_end_begin(const BTile *tiles, int n_tiles, int gx, const BRep *rep, PView<R> v, Vec3<R> old,
-                      PView<double> c, R dt, R dt_sq, double cut_c, double cut_n, double prob, const uint64_t *d_step,
-                      int step_off, const int *list, const int *n, int Nmax, const unsigned char *contrib,
-                      int *ncontrib, int *max_contrib, const double *csnap, LJDev lj_cc, unsigned long long *so_max,
-                      unsigned *done, int *resort, int *n_extra, ColloidStep cs, ResortLists rl,
-                      cudaGraphConditionalHandle cond, int use_cond, int read_species, unsigned *err)
+    kb_step_end_begin(StepArgs<R> a, int step_off, unsigned long long *so_max, unsigned *done, int *resort,
+                      int *n_extra, ColloidStep cs, ResortLists rl, cudaGraphConditionalHandle cond, int use_cond,
+                      int *any_out)
 {
     __shared__ int s_last;
     __shared__ int ws[kBT / 32 + 1];
     __shared__ double s_max[kBT / 32];
-    constexpr bool kFirst = V::FIRST;
-    const int n_reset = gx * 2 * cs.R;
-    double m = 0;
-    int r_tile = -1;
-    if (kFirst && blockIdx.x == 0) {
-        for (int r = threadIdx.x; r < cs.R; r += blockDim.x) {
-            end_colloid(r, rep, c, cs, lj_cc, err);
-            cs.co_max[r] = colloid_begin(r, rep, cs.c, cs.cold, cs.c_next, cs.rat, cs.mass, cs.ms, cs.d, cs.dt, err);
-        }
-    } else {
-        const int b = blockIdx.x - (kFirst ? 1 : 0);
-        if (b < n_tiles) {
-            const BTile t = tiles[b];
-            const double *p = csnap + 6 * (size_t)t.r;
-            const double a[3] = {p[0], p[1], p[2]}, bb[3] = {p[3], p[4], p[5]};
-            end_tile<R, V::KE>(t, rep[t.r], v, a, bb, dt, cut_c, cut_n, prob, *d_step + (uint64_t)step_off);
-            // the beginning half reads what the end half wrote: velocities,
-            // flags, species, force_old entries
-            __syncthreads();
-            r_tile = t.r;
-            m = begin_tile<R, V::KB>(t, v, old, v.force_old, dt, dt_sq, read_species);
-        } else if (b < n_tiles + n_reset) {
-            const int q = b - n_tiles;
-            end_reset(q / gx, q % gx, gx, list, n, Nmax, contrib, ncontrib, max_contrib);
-        } else if (!kFirst) {
-            const int nb = gridDim.x - n_tiles - n_reset;
-            for (int r = (b - n_tiles - n_reset) * blockDim.x + threadIdx.x; r < cs.R; r += nb * blockDim.x)
-                end_colloid(r, rep, c, cs, lj_cc, err);
-        }
-    }
+    const int n_col = V::FIRST ? 0 : (cs.R + kBT - 1) / kBT;
+    int r_tile;
+    const double m = eb_vblock<R, V>(blockIdx.x, n_col, a, cs, step_off, r_tile);
     if (!block_done(m, r_tile, so_max, done, s_max, &s_last)) return;
-    begin_tail<kFirst>(rep, so_max, done, resort, n_extra, cs, rl, cond, use_cond, err, ws);
+    begin_tail<V::FIRST>(a.rep, so_max, done, resort, n_extra, cs, rl, cond, use_cond, a.err, ws, any_out);
 }
 
 // ------------------------------------------------------ re-sort / sort
@@ -1151,11 +1231,50 @@ static void note(Batch *b, cudaError_t e)
     if (e != cudaSuccess && b->cap_err == cudaSuccess) b->cap_err = e;
 }
 
-// the program's re-sort test, as an IF node of the graph being captured on
-// st whose body is the re-sort of the flagged replicas; cond was created
+// blocks per colloid of the list kernels: ceil(capacity / (256 x the
+// shape's list entries per thread)), at most 64
+static int list_gx(const Batch *b)
+{
+    const int per = 256 * kListPer[shape_list(b->shape)];
+    const int gx = (b->Nmax + per - 1) / per;
+    return gx > 64 ? 64 : gx < 1 ? 1 : gx;
+}
+
+// the MD-step halves' arguments with force / force_old of the given parity
+template <typename R>
+static StepArgs<R> step_args(const Batch *b, int parity, int gx)
+{
+    const double dt = b->prm.tau / b->prm.N_MD;
+    const double dt_sq = dt * dt / 2;
+    return StepArgs<R>{b->ptile, b->n_ptile, gx, b->rep, live<R>(b->sol, parity), phys<R>(b->sol, 1).pos,
+                       live<double>(b->col, parity), (R)dt, (R)dt_sq, b->prm.cut_sq_C, b->prm.cut_sq_N, b->prm.prob,
+                       b->d_step, b->list, b->nn, b->Nmax, b->contrib, b->ncontrib, b->max_contrib, b->csnap,
+                       b->lj_dev + 1, b->read_species ? 1 : 0, dev_error_word()};
+}
+
+// the MD step's forces: the pair forces, then their three consumers (skip,
+// if given: see kb_pair_forces)
+template <typename R>
+static void force_launches(Batch *b, cudaStream_t st, const int *skip)
+{
+    const PView<R> s = live<R>(b->sol, b->parity);
+    const PView<double> c = live<double>(b->col, b->parity);
+    const int gx = list_gx(b);
+    kb_pair_forces<R><<<dim3(gx, 2 * b->R), 256, 0, st>>>(b->rep, c, s, b->list, b->nn, b->Nmax, b->lj_sc, b->pair_f,
+                                                          b->pair_e, b->contrib, b->ncontrib, b->max_contrib,
+                                                          b->prm.cut_sq_C, b->csnap, skip);
+    kb_apply_sum<R><<<gx * 2 * b->R + 3 * b->R, 256, 0, st>>>(
+        b->rep, b->R, gx, b->list, b->nn, b->Nmax, b->contrib, b->pair_f, b->ncontrib, b->max_contrib, s.force.x,
+        s.force.y, s.force.z, c.force.x, c.force.y, c.force.z, b->clist, b->cn, skip);
+}
+
+// the program's re-sort test, as an IF node of the graph g being captured on
+// st whose body (captured on `nested`) is the re-sort of the flagged
+// replicas, followed by the step's forces when with_forces; cond was created
 // before the kernel that sets it was captured
 template <typename R>
-static void capture_conditional_resort(Batch *b, cudaStream_t st, cudaGraph_t g, cudaGraphConditionalHandle cond)
+static void capture_conditional_resort(Batch *b, cudaStream_t st, cudaGraph_t g, cudaGraphConditionalHandle cond,
+                                       cudaStream_t nested, bool with_forces)
 {
     cudaStreamCaptureStatus cs;
     const cudaGraphNode_t *deps = nullptr;
@@ -1171,10 +1290,11 @@ static void capture_conditional_resort(Batch *b, cudaStream_t st, cudaGraph_t g,
     if (b->cap_err != cudaSuccess) return;
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     note(b, cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
-    note(b, cudaStreamBeginCaptureToGraph(b->body, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    resort_launches<R>(b, b->resort, false, b->body, -1);
+    note(b, cudaStreamBeginCaptureToGraph(nested, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    resort_launches<R>(b, b->resort, false, nested, -1);
+    if (with_forces) force_launches<R>(b, nested, nullptr);
     cudaGraph_t out = nullptr;
-    note(b, cudaStreamEndCapture(b->body, &out));
+    note(b, cudaStreamEndCapture(nested, &out));
 }
 
 // a fresh IF-node handle in the graph being captured on st (0 when not
@@ -1213,41 +1333,41 @@ static void md_step_launches(Batch *b, int k)
         cond = new_cond(b, st);
         kb_step_begin<R, V><<<b->n_ptile + (V::FIRST ? 1 : 0), kBT, 0, st>>>(
             b->ptile, b->rep, s, alt.pos, s.force_old, (R)dt, (R)dt_sq, b->so_max, b->done, b->resort, b->n_extra,
-            cs, rl, cond, use_cond, read_species, dev_error_word());
+            cs, rl, cond, use_cond, read_species, dev_error_word(), b->any);
     }
-    if (b->capturing) {
-        cudaStreamCaptureStatus st_cap;
-        cudaGraph_t g = nullptr;
-        note(b, cudaStreamGetCaptureInfo(st, &st_cap, nullptr, &g, nullptr, nullptr));
-        capture_conditional_resort<R>(b, st, g, cond);
-    } else {
-        resort_launches<R>(b, b->resort, false, st, -1);
-    }
-    // switch_force: the cleared entries become `force`
+    // switch_force: the cleared entries become `force` (the re-sort does not
+    // read the force buffers)
     b->parity ^= 1;
     s = live<R>(b->sol, b->parity);
     c = live<double>(b->col, b->parity);
     cs.c = c;
     cs.c_next = c.force_old;
-    const int per = 256 * kListPer[shape_list(b->shape)];
-    int gx = (b->Nmax + per - 1) / per;
-    if (gx > 64) gx = 64;
-    if (gx < 1) gx = 1;
-    kb_pair_forces<R><<<dim3(gx, 2 * b->R), 256, 0, st>>>(b->rep, c, s, b->list, b->nn, b->Nmax, b->lj_sc, b->pair_f,
-                                                          b->pair_e, b->contrib, b->ncontrib, b->max_contrib,
-                                                          b->prm.cut_sq_C, b->csnap);
-    kb_apply_sum<R><<<gx * 2 * b->R + 3 * b->R, 256, 0, st>>>(
-        b->rep, b->R, gx, b->list, b->nn, b->Nmax, b->contrib, b->pair_f, b->ncontrib, b->max_contrib, s.force.x,
-        s.force.y, s.force.z, c.force.x, c.force.y, c.force.z, b->clist, b->cn);
+    const int gx = list_gx(b);
+    if (b->capturing) {
+        // the re-sort test as an IF node whose body re-sorts and then
+        // evaluates the forces, beside a branch that evaluates them at once
+        // unless the beginning decided to re-sort: the IF node's latency then
+        // overlaps the forces of every step without a re-sort
+        note(b, cudaEventRecord(b->ev_fork, st));
+        note(b, cudaStreamWaitEvent(b->side, b->ev_fork, 0));
+        cudaStreamCaptureStatus st_cap;
+        cudaGraph_t g = nullptr;
+        note(b, cudaStreamGetCaptureInfo(st, &st_cap, nullptr, &g, nullptr, nullptr));
+        capture_conditional_resort<R>(b, st, g, cond, b->body, true);
+        force_launches<R>(b, b->side, b->any);
+        note(b, cudaEventRecord(b->ev_join, b->side));
+        note(b, cudaStreamWaitEvent(st, b->ev_join, 0));
+    } else {
+        resort_launches<R>(b, b->resort, false, st, -1);
+        force_launches<R>(b, st, nullptr);
+    }
     const int n_col_blocks = (b->R + kBT - 1) / kBT;
     const int n_reset = gx * 2 * b->R;
     if (k + 1 < b->prm.N_MD) {
         b->cond_next = new_cond(b, st);
         kb_step_end_begin<R, V><<<(V::FIRST ? 1 : n_col_blocks) + b->n_ptile + n_reset, kBT, 0, st>>>(
-            b->ptile, b->n_ptile, gx, b->rep, s, alt.pos, c, (R)dt, (R)dt_sq, b->prm.cut_sq_C, b->prm.cut_sq_N,
-            b->prm.prob, b->d_step, k, b->list, b->nn, b->Nmax, b->contrib, b->ncontrib, b->max_contrib, b->csnap,
-            b->lj_cc, b->so_max, b->done, b->resort, b->n_extra, cs, rl, b->cond_next, use_cond, read_species,
-            dev_error_word());
+            step_args<R>(b, b->parity, gx), k, b->so_max, b->done, b->resort, b->n_extra, cs, rl, b->cond_next,
+            use_cond, b->any);
     } else {
         b->cond_next = 0;
         kb_step_end<R, V><<<b->n_ptile + n_reset + n_col_blocks, kBT, 0, st>>>(
@@ -1256,19 +1376,23 @@ static void md_step_launches(Batch *b, int k)
     }
 }
 
+template <typename R, int Var>
+static void md_steps(Batch *b)
+{
+    for (int k = 0; k < b->prm.N_MD; k++) md_step_launches<R, typename BVarOf<R, Var>::T>(b, k);
+}
+
 template <typename R>
 static void interval_launches(Batch *b)
 {
     cudaStream_t st = stream();
     const int N_MD = b->prm.N_MD;
-    for (int k = 0; k < N_MD; k++) {
-        switch (shape_var(b->shape)) {
-        case 1: md_step_launches<R, typename BVarOf<R, 1>::T>(b, k); break;
-        case 2: md_step_launches<R, typename BVarOf<R, 2>::T>(b, k); break;
-        case 3: md_step_launches<R, typename BVarOf<R, 3>::T>(b, k); break;
-        case 4: md_step_launches<R, typename BVarOf<R, 4>::T>(b, k); break;
-        default: md_step_launches<R, typename BVarOf<R, 0>::T>(b, k); break;
-        }
+    switch (shape_var(b->shape)) {
+    case 1: md_steps<R, 1>(b); break;
+    case 2: md_steps<R, 2>(b); break;
+    case 3: md_steps<R, 3>(b); break;
+    case 4: md_steps<R, 4>(b); break;
+    default: md_steps<R, 0>(b); break;
     }
     resort_launches<R>(b, nullptr, true, st, N_MD);
     SrdParams q{};
@@ -1328,6 +1452,9 @@ static void free_batch(Batch *b)
     for (auto &e : b->exec)
         if (e) cudaGraphExecDestroy(e);
     if (b->body) cudaStreamDestroy(b->body);
+    if (b->side) cudaStreamDestroy(b->side);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
     rmpcd_particles_destroy(b->sol);
     rmpcd_particles_destroy(b->col);
     void *ptrs[] = {b->rep, b->ptile, b->stile, b->stile_first, b->stile_count, b->tile_sum, b->tile_off, b->count,
@@ -1335,7 +1462,8 @@ static void free_batch(Batch *b)
                     b->contrib, b->ncontrib, b->max_contrib, b->clist, b->cn, b->so_max, b->co_max, b->csnap, b->resort,
                     b->n_extra,
                     b->big, b->n_big, b->rattle[0], b->rattle[1], b->rattle[2], b->vv_mass, b->d_step, b->done,
-                    b->ptile_first, b->ptile_count, b->act_p, b->act_s, b->n_act, b->all_p, b->all_s, b->n_all};
+                    b->ptile_first, b->ptile_count, b->act_p, b->act_s, b->n_act, b->all_p, b->all_s, b->n_all,
+                    b->lj_dev, b->any};
     for (void *q : ptrs) cudaFree(q);
     for (int *l : b->luts) cudaFree(l);
     delete b;
@@ -1550,6 +1678,10 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
               !dalloc(&b->rattle[0], 2 * (size_t)R) && !dalloc(&b->rattle[1], 2 * (size_t)R) &&
               !dalloc(&b->rattle[2], 2 * (size_t)R) && !dalloc(&b->vv_mass, 2 * (size_t)R) && !dalloc(&b->d_step, 1) &&
               !dalloc(&b->done, 1) && cudaStreamCreateWithFlags(&b->body, cudaStreamNonBlocking) == cudaSuccess &&
+              !dalloc(&b->lj_dev, 2) && !dalloc(&b->any, 1) &&
+              cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) == cudaSuccess &&
               !dalloc(&b->ptile_first, R) && !dalloc(&b->ptile_count, R) && !dalloc(&b->act_p, cap_p) &&
               !dalloc(&b->act_s, stl.size()) && !dalloc(&b->n_act, 2) && !dalloc(&b->all_p, cap_p) &&
               !dalloc(&b->all_s, stl.size()) && !dalloc(&b->n_all, 2);
@@ -1597,6 +1729,12 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
     RMPCD_CUDA_TRY(cudaMemsetAsync(b->n_extra, 0, (size_t)R * sizeof(int), st));
     RMPCD_CUDA_TRY(cudaMemsetAsync(b->resort, 0, (size_t)R * sizeof(int), st));
     RMPCD_CUDA_TRY(cudaMemsetAsync(b->done, 0, sizeof(unsigned), st));
+    RMPCD_CUDA_TRY(cudaMemsetAsync(b->any, 0, sizeof(int), st));
+    {
+        const LJDev lj2[2] = {b->lj_sc, b->lj_cc};
+        RMPCD_CUDA_TRY(cudaMemcpyAsync(b->lj_dev, lj2, sizeof(lj2), cudaMemcpyHostToDevice, st));
+        RMPCD_CUDA_TRY(cudaStreamSynchronize(st));  // lj2 goes out of scope
+    }
     d2d(b->stencil, nl[0]->stencil, 3 * (size_t)b->n_stencil * sizeof(int));
     for (int r = 0; r < R; r++) {
         const BRep &p = b->rep_h[r];

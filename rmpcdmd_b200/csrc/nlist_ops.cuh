@@ -580,6 +580,9 @@ __device__ inline void colloid_tree_block(int i, const int *n, int Nmax, const u
             cfz[i] = cfz[i] + b2;
         }
     }
+    // wsum is free again only once warp 0 has read it (a block may go on to
+    // another colloid)
+    __syncthreads();
 }
 
 // compute_force_n2 for colloid m = blockIdx.x with the pair terms evaluated

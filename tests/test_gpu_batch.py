@@ -129,9 +129,14 @@ def test_engine_autotune_runs_real_intervals_and_remembers(rm):
     tuned = drivers(rm, boxes, seeds, 32, 10)
     bt = DimerBatch(tuned)
     res = bt.autotune(1)
-    n = len(DimerBatch.shapes(32))
+    shapes = DimerBatch.shapes(32)
+    n = len(shapes)
     timed = [m for m in res["ms_per_interval"] if m > 0]
-    assert len(timed) > n // 2 and all(m == -1 or m > 0 for m in res["ms_per_interval"])
+    # every tile and variant with one list entry per thread, then the best
+    # of them with the other list setting
+    first = [k for k, s in enumerate(shapes) if s["list_entries_per_thread"] == 1]
+    assert all(res["ms_per_interval"][k] > 0 for k in first) and len(timed) == len(first) + 1
+    assert all(m == -1 or m > 0 for m in res["ms_per_interval"])
     assert res["intervals_run"] == 2 * len(timed)
     assert 0 <= res["best"] < n and bt.shape == res["best"]
     assert res["ms_per_interval"][res["best"]] == min(timed)
