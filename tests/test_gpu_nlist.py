@@ -151,6 +151,60 @@ def test_update_list_fp32_solvent(rm, oracle, rho):
     rm.get_status()
 
 
+def fp32_colloid_force_case(rm, oracle, seed):
+    """compute_force with an FP32 solvent on both sides: the oracle gets the
+    same float positions (its FP64 arithmetic then sees the same inputs)."""
+    L = np.array([24, 20, 22])
+    N = int(L.prod()) * 10
+    (oc, op), (gc, gp) = make_pair(rm, oracle, L, N, seed=seed, precision=32, origin=[-0.5, -0.25, -0.75],
+                                   sorted_=False)
+    op.pos[:] = gp.download("pos")
+    op.sort(oc)
+    gp.sort(gc)
+    C, cutoff = 12, 4.0
+    r = np.random.default_rng(seed + 1)
+    ocol = oracle.Particles(C, 1, [100.0])
+    gcol = rm.ParticleSystem(C, 1, [100.0])
+    ocol.species[:] = 1
+    ocol.pos[:] = r.random((C, 3)) * L
+    upload(gcol, ocol, ("pos", "species"))
+    onl = oracle.NeighborList(C, 12000)
+    gnl = rm.NeighborList(C, 12000)
+    onl.make_stencil(oc, cutoff)
+    gnl.make_stencil(gc, cutoff)
+    onl.update_list(ocol, op, cutoff, oc)
+    gnl.update_list(gcol, gp, cutoff, gc)
+    lj_o = oracle.LJParams([[1.0]], [[1.5]], [[1.5 * TWO16]])
+    lj_g = rm.LJParams([[1.0]], [[1.5]], [[1.5 * TWO16]])
+    e_o = oracle.compute_force(ocol, op, onl, oc.edges, lj_o)
+    e_g = rm.compute_force(gcol, gp, gnl, gc.edges, lj_g)
+    return e_o, e_g, ocol, gcol, op, gp
+
+
+def test_compute_force_fp32_solvent_tree_sums(rm, oracle):
+    """With an FP32 solvent each colloid's force is the FP64 sum of its pair
+    forces by a fixed tree instead of list order: equal to the oracle's
+    list-order sum to FP64 rounding and the same bits on every run; the
+    energy keeps list order (equal bit for bit) and each solvent force is the
+    oracle's, rounded to FP32."""
+    e_o, e_g, ocol, gcol, op, gp = fp32_colloid_force_case(rm, oracle, 7)
+    assert e_g == e_o
+    cf_o, cf_g = ocol.force, gcol.download("force")
+    assert np.isfinite(cf_o).all() and np.abs(cf_o).max() > 1.0
+    assert not np.array_equal(cf_g, np.zeros_like(cf_g))
+    np.testing.assert_allclose(cf_g, cf_o, rtol=0, atol=1e-12 * np.abs(cf_o).max())
+    # a particle with one contribution gets -pf rounded once, as the oracle's
+    # value rounded to FP32; the few with several differ by FP32 rounding
+    sf_o, sf_g = op.force.astype(np.float32), gp.download("force")
+    assert np.isfinite(sf_g).all() and np.count_nonzero(sf_o) > 1000
+    same = np.all(sf_g == sf_o, axis=1)
+    assert same.mean() > 0.99
+    np.testing.assert_allclose(sf_g[~same], sf_o[~same], rtol=1e-5)
+    _, _, _, gcol2, _, _ = fp32_colloid_force_case(rm, oracle, 7)
+    assert np.array_equal(gcol2.download("force"), cf_g)
+    rm.get_status()
+
+
 @pytest.mark.parametrize("C,box", [(200, 20.0), (300, 70.0), (20, 30.0)])
 def test_compute_force_n2(rm, oracle, C, box):
     # box 20: every pair inside the cut; box 70: most pairs beyond it; C = 20:
