@@ -152,7 +152,6 @@ struct rmpcd_dimer_batch {
     uint64_t step = 0;  // host copy of every replica's RNG step
     rmpcd::Masses ms{};
     rmpcd::LJDev lj_sc{}, lj_cc{};
-    rmpcd::LJDev *lj_dev = nullptr;  // device copies of lj_sc, lj_cc
     int parity = 0;  // 0: force = buffer force[0], force_old = force_old[0]; swapped by each MD step
     unsigned *done = nullptr;   // blocks finished in the current step kernel (last-block hand-off)
     bool use_graph = true;
@@ -371,8 +370,10 @@ __device__ __forceinline__ double begin_tile(const BTile &t, const PView<R> &v, 
 }
 
 // the block's maximum displacement (m, one value per thread) into its
-// replica's so_max (r_tile < 0: a block without particles)
-__device__ __forceinline__ void block_max_into(double m, int r_tile, unsigned long long *so_max, double *s_max)
+// replica's so_max (r_tile < 0: a block without particles), then the
+// last-block hand-off: true in the one block of the grid that finishes last
+__device__ __forceinline__ bool block_done(double m, int r_tile, unsigned long long *so_max, unsigned *done,
+                                           double *s_max, int *s_last)
 {
     m = warp_max(m);
     if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = m;
@@ -382,27 +383,11 @@ __device__ __forceinline__ void block_max_into(double m, int r_tile, unsigned lo
         // one atomic per block, skipped when it cannot raise the maximum
         if (r_tile >= 0 && m > __longlong_as_double((long long)__ldcg(so_max + r_tile)))
             atomic_max_nonneg(so_max + r_tile, m);
-    }
-    __syncthreads();
-}
-
-// the last-block hand-off: true in the one block of the grid that finishes
-// last (every block calls it once, after its last write)
-__device__ __forceinline__ bool block_finish(unsigned *done, int *s_last)
-{
-    if (threadIdx.x == 0) {
         __threadfence();
         *s_last = atomicAdd(done, 1u) == gridDim.x - 1;
     }
     __syncthreads();
     return *s_last;
-}
-
-__device__ __forceinline__ bool block_done(double m, int r_tile, unsigned long long *so_max, unsigned *done,
-                                           double *s_max, int *s_last)
-{
-    block_max_into(m, r_tile, so_max, s_max);
-    return block_finish(done, s_last);
 }
 
 // the last block's part of an MD step's beginning: the colloid half of every
@@ -487,21 +472,23 @@ __global__ void __launch_bounds__(kBT, V::MINB)
 // flag_particles_nl of the catalytic bead (programs/single_dimer_pbc.f90:493-509):
 // both only read positions and species and OR bits into flags.  Block (0, i)
 // also copies colloid i's position to csnap[3 i ..], the positions that the
-// step's change_species uses.
-// block bx of the gx blocks of colloid i's list
+// step's change_species uses.  skip (if given): the MD step's beginning
+// decided to re-sort, so this launch is the graph's speculative one and the
+// re-sort branch evaluates the forces instead.
 template <typename R>
-__device__ __forceinline__ void pair_vblock(int bx, int i, int gx, const BRep *rep, const PView<double> &c,
-                                            const PView<R> &s, const int *list, const int *n, int Nmax,
-                                            const LJDev &lj, double *pf, double *pe, unsigned char *contrib,
-                                            int *ncontrib, int *max_contrib, double flag_cut_sq, double *csnap)
+__global__ void kb_pair_forces(const BRep *rep, PView<double> c, PView<R> s, const int *list, const int *n, int Nmax,
+                               LJDev lj, double *pf, double *pe, unsigned char *contrib, int *ncontrib,
+                               int *max_contrib, double flag_cut_sq, double *csnap, const int *skip)
 {
+    if (skip && *(const volatile int *)skip) return;
+    const int i = blockIdx.y;
     const int r = i >> 1;
     const int ni = n[i];
     const double x[3] = {c.pos.x[i], c.pos.y[i], c.pos.z[i]};
-    if (bx == 0 && threadIdx.x < 3) csnap[3 * i + threadIdx.x] = x[threadIdx.x];
+    if (blockIdx.x == 0 && threadIdx.x < 3) csnap[3 * i + threadIdx.x] = x[threadIdx.x];
     const int s1 = c.species[i];
     const double L0 = rep[r].g.edges[0], L1 = rep[r].g.edges[1], L2 = rep[r].g.edges[2];
-    for (int e = bx * blockDim.x + threadIdx.x; e < ni; e += gx * blockDim.x) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ni; e += gridDim.x * blockDim.x) {
         size_t q = (size_t)i * Nmax + e;
         pair_force_entry(q, x, s1, s.pos.x, s.pos.y, s.pos.z, s.species, s.flags, list, L0, L1, L2, lj, pf, pe,
                          contrib, ncontrib, max_contrib + r);
@@ -510,29 +497,18 @@ __device__ __forceinline__ void pair_vblock(int bx, int i, int gx, const BRep *r
     }
 }
 
-// skip (if given): the MD step's beginning decided to re-sort, so this
-// launch is the graph's speculative one and the re-sort branch evaluates the
-// forces instead
-template <typename R>
-__global__ void kb_pair_forces(const BRep *rep, PView<double> c, PView<R> s, const int *list, const int *n, int Nmax,
-                               LJDev lj, double *pf, double *pe, unsigned char *contrib, int *ncontrib,
-                               int *max_contrib, double flag_cut_sq, double *csnap, const int *skip)
-{
-    if (skip && *(const volatile int *)skip) return;
-    pair_vblock<R>(blockIdx.x, blockIdx.y, gridDim.x, rep, c, s, list, n, Nmax, lj, pf, pe, contrib, ncontrib,
-                   max_contrib, flag_cut_sq, csnap);
-}
-
 // the three consumers of the pair forces, on disjoint data: solvent
 // particles with one contribution, those with several (per replica, in
 // order), and the colloid sums (list order in the FP64 form, a fixed tree in
-// the FP32 form); b numbers the gx * 2R + 3R blocks of the three
+// the FP32 form); skip: as kb_pair_forces
 template <typename R>
-__device__ __forceinline__ void apply_vblock(int b, const BRep *rep, int R_, int gx, const int *list, const int *n,
-                                             int Nmax, const unsigned char *contrib, const double *pf,
-                                             const int *ncontrib, const int *max_contrib, R *fx, R *fy, R *fz,
-                                             double *cfx, double *cfy, double *cfz, int *clist, int *cn)
+__global__ void kb_apply_sum(const BRep *rep, int R_, int gx, const int *list, const int *n, int Nmax,
+                             const unsigned char *contrib, const double *pf, const int *ncontrib,
+                             const int *max_contrib, R *fx, R *fy, R *fz, double *cfx, double *cfy, double *cfz,
+                             int *clist, int *cn, const int *skip)
 {
+    if (skip && *(const volatile int *)skip) return;
+    const int b = blockIdx.x;
     const int n_single = gx * 2 * R_;
     if (b < n_single) {
         const int i = b / gx, bx = b % gx;
@@ -549,17 +525,6 @@ __device__ __forceinline__ void apply_vblock(int b, const BRep *rep, int R_, int
     } else {
         colloid_tree_block(b - n_single - R_, n, Nmax, contrib, pf, cfx, cfy, cfz);
     }
-}
-
-template <typename R>
-__global__ void kb_apply_sum(const BRep *rep, int R_, int gx, const int *list, const int *n, int Nmax,
-                             const unsigned char *contrib, const double *pf, const int *ncontrib,
-                             const int *max_contrib, R *fx, R *fy, R *fz, double *cfx, double *cfy, double *cfz,
-                             int *clist, int *cn, const int *skip)
-{
-    if (skip && *(const volatile int *)skip) return;
-    apply_vblock<R>(blockIdx.x, rep, R_, gx, list, n, Nmax, contrib, pf, ncontrib, max_contrib, fx, fy, fz, cfx, cfy,
-                    cfz, clist, cn);
 }
 
 // the solvent half over the particle tile t of replica rp, whose colloid
@@ -770,7 +735,7 @@ struct StepArgs {
     const unsigned char *contrib;
     int *ncontrib, *max_contrib;
     const double *csnap;
-    const LJDev *lj_cc;  // in device memory
+    LJDev lj_cc;
     int read_species;
     unsigned *err;
 };
@@ -789,7 +754,7 @@ __device__ __forceinline__ double eb_vblock(int b, int n_col, const StepArgs<R> 
     r_tile = -1;
     if (kFirst && b == 0) {
         for (int r = threadIdx.x; r < cs.R; r += blockDim.x) {
-            end_colloid(r, a.rep, a.c, cs, *a.lj_cc, a.err);
+            end_colloid(r, a.rep, a.c, cs, a.lj_cc, a.err);
             cs.co_max[r] = colloid_begin(r, a.rep, cs.c, cs.cold, cs.c_next, cs.rat, cs.mass, cs.ms, cs.d, cs.dt,
                                          a.err);
         }
@@ -813,7 +778,7 @@ __device__ __forceinline__ double eb_vblock(int b, int n_col, const StepArgs<R> 
         end_reset(q / a.gx, q % a.gx, a.gx, a.list, a.n, a.Nmax, a.contrib, a.ncontrib, a.max_contrib);
     } else if (!kFirst) {
         for (int r = (b - a.n_tiles - n_reset) * blockDim.x + threadIdx.x; r < cs.R; r += n_col * blockDim.x)
-            end_colloid(r, a.rep, a.c, cs, *a.lj_cc, a.err);
+            end_colloid(r, a.rep, a.c, cs, a.lj_cc, a.err);
     }
     return 0;
 }
@@ -1249,7 +1214,7 @@ static StepArgs<R> step_args(const Batch *b, int parity, int gx)
     return StepArgs<R>{b->ptile, b->n_ptile, gx, b->rep, live<R>(b->sol, parity), phys<R>(b->sol, 1).pos,
                        live<double>(b->col, parity), (R)dt, (R)dt_sq, b->prm.cut_sq_C, b->prm.cut_sq_N, b->prm.prob,
                        b->d_step, b->list, b->nn, b->Nmax, b->contrib, b->ncontrib, b->max_contrib, b->csnap,
-                       b->lj_dev + 1, b->read_species ? 1 : 0, dev_error_word()};
+                       b->lj_cc, b->read_species ? 1 : 0, dev_error_word()};
 }
 
 // the MD step's forces: the pair forces, then their three consumers (skip,
@@ -1463,7 +1428,7 @@ static void free_batch(Batch *b)
                     b->n_extra,
                     b->big, b->n_big, b->rattle[0], b->rattle[1], b->rattle[2], b->vv_mass, b->d_step, b->done,
                     b->ptile_first, b->ptile_count, b->act_p, b->act_s, b->n_act, b->all_p, b->all_s, b->n_all,
-                    b->lj_dev, b->any};
+                    b->any};
     for (void *q : ptrs) cudaFree(q);
     for (int *l : b->luts) cudaFree(l);
     delete b;
@@ -1678,7 +1643,7 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
               !dalloc(&b->rattle[0], 2 * (size_t)R) && !dalloc(&b->rattle[1], 2 * (size_t)R) &&
               !dalloc(&b->rattle[2], 2 * (size_t)R) && !dalloc(&b->vv_mass, 2 * (size_t)R) && !dalloc(&b->d_step, 1) &&
               !dalloc(&b->done, 1) && cudaStreamCreateWithFlags(&b->body, cudaStreamNonBlocking) == cudaSuccess &&
-              !dalloc(&b->lj_dev, 2) && !dalloc(&b->any, 1) &&
+              !dalloc(&b->any, 1) &&
               cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) == cudaSuccess &&
               cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
               cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) == cudaSuccess &&
@@ -1730,11 +1695,6 @@ static int create(Batch **out, int R, rmpcd_particles *const *sol, rmpcd_particl
     RMPCD_CUDA_TRY(cudaMemsetAsync(b->resort, 0, (size_t)R * sizeof(int), st));
     RMPCD_CUDA_TRY(cudaMemsetAsync(b->done, 0, sizeof(unsigned), st));
     RMPCD_CUDA_TRY(cudaMemsetAsync(b->any, 0, sizeof(int), st));
-    {
-        const LJDev lj2[2] = {b->lj_sc, b->lj_cc};
-        RMPCD_CUDA_TRY(cudaMemcpyAsync(b->lj_dev, lj2, sizeof(lj2), cudaMemcpyHostToDevice, st));
-        RMPCD_CUDA_TRY(cudaStreamSynchronize(st));  // lj2 goes out of scope
-    }
     d2d(b->stencil, nl[0]->stencil, 3 * (size_t)b->n_stencil * sizeof(int));
     for (int r = 0; r < R; r++) {
         const BRep &p = b->rep_h[r];
