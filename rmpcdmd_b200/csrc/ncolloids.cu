@@ -24,6 +24,7 @@
 #include <tuple>
 #include <vector>
 
+#include "keys.cuh"
 #include "rmpcd_common.cuh"
 #include "sortcore.cuh"
 #include "state.cuh"
@@ -94,25 +95,73 @@ __device__ inline void stream_vel_gated(const PView<R> &v, long long i, int f, R
     }
 }
 
-// the catch-up of cell_md_pos then cell_md_vel with md_flag = .false.
-// (src/md.f90:79-102, :239-263) over every non-MD cell in one pass (both are
-// per particle, the position step reading the velocity before its update),
-// eight lanes per cell so that a cell's particles are read together
+// The catch-up of cell_md_pos then cell_md_vel with md_flag = .false.
+// (src/md.f90:79-102, :239-263) for every particle outside the MD cells
+// (cellmap: each particle's slot, from the last sort), fused with the key
+// pass of the sort that follows (apply_pbc, the slot in the cells' grid and
+// its count, as k_pbc_key_count): one linear pass, the streamed position kept
+// in registers and written once with its wrap.  Per particle the arithmetic
+// is the catch-up's (the position step reading the velocity before its
+// update) followed by the key pass's.
 template <typename R>
-__global__ void k_other_cells_stream(const int *count, const int *start, const unsigned char *is_md, int S,
-                                     PView<R> v, R dt, R dt_sq)
+__global__ void k_catch_up_key_count(const int *__restrict__ cellmap, const unsigned char *__restrict__ is_md, int N,
+                                     PView<R> v, R dt, R dt_sq, Grid g, double e0, double e1, double e2,
+                                     int *__restrict__ key, int *__restrict__ count)
 {
-    const long long nthreads = (long long)gridDim.x * blockDim.x;
-    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < (long long)S * kLanesPerCell;
-         q += nthreads) {
-        const int s = (int)(q / kLanesPerCell), g = (int)(q % kLanesPerCell);
-        if (is_md[s]) continue;
-        const int a = start[s], c = count[s];
-        for (int i = a + g; i < a + c; i += kLanesPerCell) {
-            const int f = v.flags[i];
-            stream_pos_gated(v, i, f, dt, dt_sq);
-            stream_vel_gated(v, i, f, dt);
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < N; base += stride) {
+        const long long i = base + threadIdx.x;
+        const bool ok = i < N;
+        int slot = -1;
+        if (ok) {
+            R x = v.pos.x[i], y = v.pos.y[i], z = v.pos.z[i];
+            const bool catch_up = !is_md[cellmap[i]];
+            if (catch_up) {
+                const int f = v.flags[i];
+                R fx = 0, fy = 0, fz = 0;
+                if (f & kForceFlags) {
+                    fx = v.force.x[i];
+                    fy = v.force.y[i];
+                    fz = v.force.z[i];
+                }
+                x = x + dt * v.vel.x[i] + dt_sq * fx;
+                y = y + dt * v.vel.y[i] + dt_sq * fy;
+                z = z + dt * v.vel.z[i] + dt_sq * fz;
+                stream_vel_gated(v, i, f, dt);
+            }
+            const int jx = floor_div_edge((double)x, e0), jy = floor_div_edge((double)y, e1),
+                      jz = floor_div_edge((double)z, e2);
+            if (jx) {
+                v.ix[i] += jx;
+                x = x - (R)(jx * e0);
+            }
+            if (jy) {
+                v.iy[i] += jy;
+                y = y - (R)(jy * e1);
+            }
+            if (jz) {
+                v.iz[i] += jz;
+                z = z - (R)(jz * e2);
+            }
+            if (catch_up || jx) v.pos.x[i] = x;
+            if (catch_up || jy) v.pos.y[i] = y;
+            if (catch_up || jz) v.pos.z[i] = z;
+            slot = slot_of(g, (double)x, (double)y, (double)z);
+            key[i] = slot;
         }
+        const unsigned peers = __match_any_sync(0xffffffffu, slot);
+        if (ok && lane == __ffs(peers) - 1) atomicAdd(count + slot, __popc(peers));
+    }
+}
+
+// cellmap[i] = the slot of particle i of the sorted arrays
+__global__ void k_fill_cellmap(const int *count, const int *start, int S, int *cellmap)
+{
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < (long long)S * kLanesPerCell;
+         q += (long long)gridDim.x * blockDim.x) {
+        const int s = (int)(q / kLanesPerCell), g = (int)(q % kLanesPerCell);
+        for (int i = start[s] + g; i < start[s] + count[s]; i += kLanesPerCell) cellmap[i] = s;
     }
 }
 
@@ -233,6 +282,7 @@ struct NcLoop {
     std::vector<double> vv_mass;
     double dt;
     int *md_list = nullptr;  // is_md slots
+    int *cellmap = nullptr;  // slot of every solvent particle (set by each sort)
     int *n_md = nullptr;     // their number (device)
     unsigned long long *h_max = nullptr;  // page-locked landing of the two maxima
     int full_rolls = 2;  // rolls over all N still due since the last sort
@@ -336,14 +386,19 @@ static int roll_clear_t(NcLoop &L)
     return RMPCD_OK;
 }
 
+// the particles outside the MD cells caught up over dtl, and every particle
+// keyed and counted for the sort (k_catch_up_key_count)
 template <typename R>
-static int other_cells_t(NcLoop &L, double dtl)
+static int catch_up_key_t(NcLoop &L, double dtl)
 {
     const double dt_sq = dtl * dtl / 2;
-    const int g = grid_full((long long)L.cells->S * kLanesPerCell, 256);
     rmpcd_cells *c = L.cells;
-    k_other_cells_stream<R><<<g, 256, 0, stream()>>>(c->count, c->start, c->is_md, c->S, cur<R>(L.s), (R)dtl,
-                                                     (R)dt_sq);
+    cudaStream_t st = stream();
+    RMPCD_CUDA_TRY(cudaMemsetAsync(c->count, 0, (size_t)c->S * sizeof(int), st));
+    if (L.s->N > 0)
+        k_catch_up_key_count<R><<<grid_for(L.s->N, 256), 256, 0, st>>>(
+            L.cellmap, c->is_md, L.s->N, cur<R>(L.s), (R)dtl, (R)dt_sq, grid_of(c), c->edges[0], c->edges[1],
+            c->edges[2], L.s->key, c->count);
     RMPCD_CHECK_LAUNCH();
     return RMPCD_OK;
 }
@@ -394,9 +449,9 @@ static int read_displacements(NcLoop &L, double delta_t, double *so_max, double 
 static int catch_up_and_sort(NcLoop &L, bool full_pos_old)
 {
     const double dtl = (L.st->t - L.st->last_sort) * L.dt;
-    int rc = L.s->precision == RMPCD_FP32 ? other_cells_t<float>(L, dtl) : other_cells_t<double>(L, dtl);
+    int rc = L.s->precision == RMPCD_FP32 ? catch_up_key_t<float>(L, dtl) : catch_up_key_t<double>(L, dtl);
     if (!rc) rc = rmpcd_apply_pbc(L.c, L.cells->edges);
-    if (!rc) rc = sort_particles_flagged(L.cells, L.s, L.cells->edges);  // apply_pbc of the solvent + sort
+    if (!rc) rc = sort_keyed_flagged(L.cells, L.s, L.cellmap);  // the solvent's wrap and keys are done
     L.st->last_sort = L.st->t;
     L.full_rolls = 2;
     if (!rc) rc = rmpcd_nlist_update(L.nl, L.c, L.s, L.prm->list_radius, L.cells, nullptr);
@@ -510,11 +565,16 @@ extern "C" int rmpcd_ncolloids_run(rmpcd_particles *solvent, rmpcd_particles *co
     PhaseTimer timer("ncolloids_run");
     RMPCD_CUDA_TRY(cudaMalloc(&L.md_list, (size_t)(cells->S > 0 ? cells->S : 1) * sizeof(int)));
     if (cudaMalloc(&L.n_md, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&L.cellmap, (size_t)(solvent->N > 0 ? solvent->N : 1) * sizeof(int)) != cudaSuccess ||
         cudaHostAlloc(&L.h_max, 2 * sizeof(unsigned long long), cudaHostAllocDefault) != cudaSuccess) {
         cudaFree(L.md_list);
         cudaFree(L.n_md);
+        cudaFree(L.cellmap);
         return fail(RMPCD_ERR_CUDA, "rmpcd_ncolloids_run: allocation failed");
     }
+    // the solvent is sorted on entry: its slots from the cell ranges
+    k_fill_cellmap<<<grid_full((long long)cells->S * kLanesPerCell, 256), 256, 0, stream()>>>(
+        cells->count, cells->start, cells->S, L.cellmap);
     int rc0 = list_md_cells(L);
     for (int k = 0; !rc0 && k < n_intervals; k++) {
         const int i = first_interval + k;
@@ -535,6 +595,7 @@ extern "C" int rmpcd_ncolloids_run(rmpcd_particles *solvent, rmpcd_particles *co
     cudaStreamSynchronize(stream());
     cudaFree(L.md_list);
     cudaFree(L.n_md);
+    cudaFree(L.cellmap);
     cudaFreeHost(L.h_max);
     if (rc0) return rc0;
     return check_dev_error(nullptr);

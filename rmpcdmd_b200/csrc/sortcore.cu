@@ -73,11 +73,12 @@ __global__ void k_pbc_key_count(Grid g, PView<R> v, double e0, double e1, double
 // place every particle inside its cell; the order inside a cell is fixed
 // afterwards by k_segsort.  Each warp handles kPermRounds groups of 32
 // consecutive particles and issues all their cursor atomics before using any
-// result, so the atomic round trips overlap.
+// result, so the atomic round trips overlap.  cellmap (if given) receives the
+// slot of every place: the slot of each particle of the sorted arrays.
 constexpr int kPermRounds = 8;
 
 __global__ void k_perm(const int *__restrict__ key, int N, int *__restrict__ cursor,
-                       int *__restrict__ perm)
+                       int *__restrict__ perm, int *__restrict__ cellmap)
 {
     const int lane = threadIdx.x & 31;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -101,7 +102,11 @@ __global__ void k_perm(const int *__restrict__ key, int N, int *__restrict__ cur
 #pragma unroll
         for (int r = 0; r < kPermRounds; r++) {
             int bb = __shfl_sync(0xffffffffu, b[r], __ffs(peers[r]) - 1);
-            if (k[r] >= 0) perm[bb + __popc(peers[r] & lt)] = (int)(base + r * 32 + lane);
+            if (k[r] >= 0) {
+                const int place = bb + __popc(peers[r] & lt);
+                perm[place] = (int)(base + r * 32 + lane);
+                if (cellmap) cellmap[place] = k[r];
+            }
         }
     }
 }
@@ -234,17 +239,17 @@ int count_and_scan(rmpcd_cells *c, rmpcd_particles *p, bool)
     return count_and_scan_t<double>(c, p);
 }
 
-int build_perm_unsorted(rmpcd_cells *c, rmpcd_particles *p)
+int build_perm_unsorted(rmpcd_cells *c, rmpcd_particles *p, int *cellmap)
 {
     if (p->N == 0) return RMPCD_OK;
-    k_perm<<<grid_for(p->N, 256), 256, 0, stream()>>>(p->key, p->N, c->cursor, p->perm);
+    k_perm<<<grid_for(p->N, 256), 256, 0, stream()>>>(p->key, p->N, c->cursor, p->perm, cellmap);
     RMPCD_CHECK_LAUNCH();
     return RMPCD_OK;
 }
 
-int build_perm(rmpcd_cells *c, rmpcd_particles *p)
+int build_perm(rmpcd_cells *c, rmpcd_particles *p, int *cellmap)
 {
-    int rc = build_perm_unsorted(c, p);
+    int rc = build_perm_unsorted(c, p, cellmap);
     if (rc) return rc;
     return sort_perm_segments(c, p);
 }
@@ -302,6 +307,26 @@ int gather_all(rmpcd_particles *p)
 }
 
 template <typename R>
+static int sort_keyed_flagged_t(rmpcd_cells *c, rmpcd_particles *p, int *cellmap)
+{
+    {
+        PhaseTimer t("count");
+        int rc = exclusive_scan(c->count, c->start, c->cursor, c->S, c->scan_tmp, nullptr, stream());
+        if (rc) return rc;
+    }
+    PhaseTimer t("sort");
+    int rc = build_perm(c, p, cellmap);
+    if (rc) return rc;
+    return gather_t<R>(p, true);
+}
+
+int sort_keyed_flagged(rmpcd_cells *c, rmpcd_particles *p, int *cellmap)
+{
+    if (p->precision == RMPCD_FP32) return sort_keyed_flagged_t<float>(c, p, cellmap);
+    return sort_keyed_flagged_t<double>(c, p, cellmap);
+}
+
+template <typename R>
 static int sort_particles_flagged_t(rmpcd_cells *c, rmpcd_particles *p, const double edges[3])
 {
     {
@@ -312,13 +337,8 @@ static int sort_particles_flagged_t(rmpcd_cells *c, rmpcd_particles *p, const do
             k_pbc_key_count<R><<<grid_for(p->N, 256), 256, 0, st>>>(grid_of(c), cur<R>(p), edges[0], edges[1],
                                                                    edges[2], p->N, p->key, c->count);
         RMPCD_CHECK_LAUNCH();
-        int rc = exclusive_scan(c->count, c->start, c->cursor, c->S, c->scan_tmp, nullptr, st);
-        if (rc) return rc;
     }
-    PhaseTimer t("sort");
-    int rc = build_perm(c, p);
-    if (rc) return rc;
-    return gather_t<R>(p, true);
+    return sort_keyed_flagged_t<R>(c, p, nullptr);
 }
 
 int sort_particles_flagged(rmpcd_cells *c, rmpcd_particles *p, const double edges[3])

@@ -20,11 +20,11 @@ namespace rmpcd {
 // key[] and count/start/cursor of p under the current origin of c
 int count_and_scan(rmpcd_cells *c, rmpcd_particles *p, bool keep_key);
 // perm[] from key[] and cursor[] (cell order fixed, in-cell order arbitrary)
-int build_perm_unsorted(rmpcd_cells *c, rmpcd_particles *p);
+int build_perm_unsorted(rmpcd_cells *c, rmpcd_particles *p, int *cellmap = nullptr);
 // ascending sort of every cell's perm segment (uses cursor[] and key[] as scratch)
 int sort_perm_segments(rmpcd_cells *c, rmpcd_particles *p);
 // both of the above
-int build_perm(rmpcd_cells *c, rmpcd_particles *p);
+int build_perm(rmpcd_cells *c, rmpcd_particles *p, int *cellmap = nullptr);
 // gather every field through perm into the other buffer and flip buffers
 int gather_all(rmpcd_particles *p);
 // full sort
@@ -36,6 +36,10 @@ int sort_positions(rmpcd_cells *c, const rmpcd_particles *from, rmpcd_particles 
 // state compute_force and its flag roll maintain): those entries are written
 // as zeros instead of being gathered
 int sort_particles_flagged(rmpcd_cells *c, rmpcd_particles *p, const double edges[3]);
+// the same sort after its key pass (p->key holds every particle's slot in the
+// cells' grid, c->count their counts): scan, placement and gated gather;
+// cellmap (if given) receives the slot of every particle of the sorted arrays
+int sort_keyed_flagged(rmpcd_cells *c, rmpcd_particles *p, int *cellmap);
 // ascending merge sort of the *n_big queued cells big[] of more than 64
 // particles (tmp: scratch of the extent of perm)
 void launch_segsort_big(const int *start, const int *count, const int *big, const int *n_big, int *perm,
