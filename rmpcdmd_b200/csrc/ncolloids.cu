@@ -58,9 +58,10 @@ constexpr int kLanesPerCell = 8;
 // arithmetic is that of md_pos / md_vel with the zero entry, bit for bit.
 constexpr int kForceFlags = (1 << MD_BIT) | (1 << PAST_MD_BIT);
 
-// md_pos of one particle (src/md.f90:61-77 form)
+// md_pos of one particle (src/md.f90:61-77 form): its new position, from
+// the velocity before md_vel (flags f), for the caller to store
 template <typename R>
-__device__ inline void stream_pos_gated(const PView<R> &v, long long i, int f, R dt, R dt_sq)
+__device__ inline void moved_pos(const PView<R> &v, long long i, int f, R dt, R dt_sq, R &x, R &y, R &z)
 {
     R fx = 0, fy = 0, fz = 0;
     if (f & kForceFlags) {
@@ -68,9 +69,9 @@ __device__ inline void stream_pos_gated(const PView<R> &v, long long i, int f, R
         fy = v.force.y[i];
         fz = v.force.z[i];
     }
-    v.pos.x[i] = v.pos.x[i] + dt * v.vel.x[i] + dt_sq * fx;
-    v.pos.y[i] = v.pos.y[i] + dt * v.vel.y[i] + dt_sq * fy;
-    v.pos.z[i] = v.pos.z[i] + dt * v.vel.z[i] + dt_sq * fz;
+    x = v.pos.x[i] + dt * v.vel.x[i] + dt_sq * fx;
+    y = v.pos.y[i] + dt * v.vel.y[i] + dt_sq * fy;
+    z = v.pos.z[i] + dt * v.vel.z[i] + dt_sq * fz;
 }
 
 // md_vel of one particle (src/md.f90:219-237 form)
@@ -115,20 +116,16 @@ __global__ void k_catch_up_key_count(const int *__restrict__ cellmap, const unsi
         const bool ok = i < N;
         int slot = -1;
         if (ok) {
-            R x = v.pos.x[i], y = v.pos.y[i], z = v.pos.z[i];
+            R x, y, z;
             const bool catch_up = !is_md[cellmap[i]];
             if (catch_up) {
                 const int f = v.flags[i];
-                R fx = 0, fy = 0, fz = 0;
-                if (f & kForceFlags) {
-                    fx = v.force.x[i];
-                    fy = v.force.y[i];
-                    fz = v.force.z[i];
-                }
-                x = x + dt * v.vel.x[i] + dt_sq * fx;
-                y = y + dt * v.vel.y[i] + dt_sq * fy;
-                z = z + dt * v.vel.z[i] + dt_sq * fz;
+                moved_pos(v, i, f, dt, dt_sq, x, y, z);
                 stream_vel_gated(v, i, f, dt);
+            } else {
+                x = v.pos.x[i];
+                y = v.pos.y[i];
+                z = v.pos.z[i];
             }
             const int jx = floor_div_edge((double)x, e0), jy = floor_div_edge((double)y, e1),
                       jz = floor_div_edge((double)z, e2);
@@ -165,19 +162,40 @@ __global__ void k_fill_cellmap(const int *count, const int *start, int S, int *c
     }
 }
 
-// cell_md_pos / cell_md_vel with md_flag = .true. (src/md.f90:79-102,
-// :239-263) over the listed MD cells, eight lanes per cell
+// cell_md_pos with md_flag = .true. (src/md.f90:79-102) over the listed MD
+// cells, eight lanes per cell, fused with cell_maximum_displacement over the
+// same cells (src/particle_system.f90:380-410): each new position is measured
+// against pos_old as it is written (the value that is stored); the squared
+// maximum goes to *out
 template <typename R>
-__global__ void k_md_cells_pos(const int *list, const int *n_list, const int *count, const int *start, PView<R> v,
-                               R dt, R dt_sq)
+__global__ void k_md_cells_pos_disp(const int *list, const int *n_list, const int *count, const int *start,
+                                    PView<R> v, Vec3<R> old, R dt, R dt_sq, unsigned long long *out)
 {
     const long long n = (long long)*n_list * kLanesPerCell;
+    double m = 0;
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
         const int s = list[q / kLanesPerCell], g = (int)(q % kLanesPerCell);
         const int a = start[s], c = count[s];
-        for (int i = a + g; i < a + c; i += kLanesPerCell) stream_pos_gated(v, i, v.flags[i], dt, dt_sq);
+        for (int i = a + g; i < a + c; i += kLanesPerCell) {
+            R x, y, z;
+            moved_pos(v, i, v.flags[i], dt, dt_sq, x, y, z);
+            v.pos.x[i] = x;
+            v.pos.y[i] = y;
+            v.pos.z[i] = z;
+            if (v.species[i] >= 0) {
+                const double d0 = (double)x - (double)old.x[i];
+                const double d1 = (double)y - (double)old.y[i];
+                const double d2 = (double)z - (double)old.z[i];
+                const double r = d0 * d0 + d1 * d1 + d2 * d2;
+                m = m > r ? m : r;
+            }
+        }
     }
+    warp_max_into(out, m);
 }
+
+// cell_md_vel with md_flag = .true. (src/md.f90:239-263) over the listed MD
+// cells, eight lanes per cell
 
 template <typename R>
 __global__ void k_md_cells_vel(const int *list, const int *n_list, const int *count, const int *start, PView<R> v,
@@ -208,24 +226,6 @@ __global__ void k_md_cells_copy_pos(const int *list, const int *n_list, const in
             old.z[i] = pos.z[i];
         }
     }
-}
-
-// cell_maximum_displacement over the listed cells (src/particle_system.f90:380-410)
-template <typename R>
-__global__ void k_md_cells_max_disp(const int *list, const int *n_list, const int *count, const int *start,
-                                    Vec3<R> pos, Vec3<R> old, const int *species, unsigned long long *out)
-{
-    const long long n = (long long)*n_list * kLanesPerCell;
-    double m = 0;
-    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-        const int s = list[q / kLanesPerCell], g = (int)(q % kLanesPerCell);
-        const int a = start[s], c = count[s];
-        for (int i = a + g; i < a + c; i += kLanesPerCell) {
-            const double r = disp_sq_one(pos, old, species, i);
-            m = m > r ? m : r;
-        }
-    }
-    warp_max_into(out, m);
 }
 
 // the roll + clear below restricted to the listed MD cells.  Between two
@@ -339,12 +339,16 @@ static int list_md_cells(NcLoop &L)
     return RMPCD_OK;
 }
 
+// cell_md_pos over the MD cells and their maximum displacement (into the
+// solvent's d_max)
 template <typename R>
-static int md_cells_pos_t(NcLoop &L)
+static int md_cells_pos_disp_t(NcLoop &L)
 {
+    cudaStream_t st = stream();
+    RMPCD_CUDA_TRY(cudaMemsetAsync(L.s->d_max, 0, 8, st));
     const R dt = (R)L.dt, dt_sq = (R)(L.dt * L.dt / 2);
-    k_md_cells_pos<R><<<md_cells_grid(), 256, 0, stream()>>>(L.md_list, L.n_md, L.cells->count,
-                                                                       L.cells->start, cur<R>(L.s), dt, dt_sq);
+    k_md_cells_pos_disp<R><<<md_cells_grid(), 256, 0, st>>>(L.md_list, L.n_md, L.cells->count, L.cells->start,
+                                                           cur<R>(L.s), alt<R>(L.s).pos, dt, dt_sq, L.s->d_max);
     RMPCD_CHECK_LAUNCH();
     return RMPCD_OK;
 }
@@ -354,19 +358,6 @@ static int md_cells_vel_t(NcLoop &L)
 {
     k_md_cells_vel<R><<<md_cells_grid(), 256, 0, stream()>>>(L.md_list, L.n_md, L.cells->count,
                                                                        L.cells->start, cur<R>(L.s), (R)L.dt);
-    RMPCD_CHECK_LAUNCH();
-    return RMPCD_OK;
-}
-
-template <typename R>
-static int md_cells_max_disp_t(NcLoop &L)
-{
-    cudaStream_t st = stream();
-    RMPCD_CUDA_TRY(cudaMemsetAsync(L.s->d_max, 0, 8, st));
-    PView<R> a = cur<R>(L.s), b = alt<R>(L.s);
-    k_md_cells_max_disp<R><<<md_cells_grid(), 256, 0, st>>>(L.md_list, L.n_md, L.cells->count,
-                                                                      L.cells->start, a.pos, b.pos, a.species,
-                                                                      L.s->d_max);
     RMPCD_CHECK_LAUNCH();
     return RMPCD_OK;
 }
@@ -415,12 +406,12 @@ static int md_cells_copy_pos_t(NcLoop &L)
 
 #define NC_DISPATCH(L, fn) ((L).s->precision == RMPCD_FP32 ? fn<float>(L) : fn<double>(L))
 
-// the displacement maxima of the MD step: solvent over is_md cells (floored
-// at max_v * delta_t) and colloids, read with one synchronisation
+// the displacement maxima of the MD step (the solvent's over the MD cells,
+// floored at max_v * delta_t when read, was taken with its positions) and the
+// colloids', read with one synchronisation
 static int launch_displacements(NcLoop &L)
 {
-    int rc = NC_DISPATCH(L, md_cells_max_disp_t);
-    if (!rc) rc = launch_max_disp(L.c);
+    int rc = launch_max_disp(L.c);
     if (rc) return rc;
     unsigned long long *bits = L.h_max;
     RMPCD_CUDA_TRY(cudaMemcpyAsync(bits, L.s->d_max, 8, cudaMemcpyDeviceToHost, stream()));
@@ -464,7 +455,7 @@ static int catch_up_and_sort(NcLoop &L, bool full_pos_old)
 // md_loop up to the displacement maxima (programs/n_colloids_pbc.f90:221-229)
 static int issue_part_a(NcLoop &L)
 {
-    int rc = NC_DISPATCH(L, md_cells_pos_t);
+    int rc = NC_DISPATCH(L, md_cells_pos_disp_t);
     if (!rc) rc = rmpcd_colloid_vv_pos(L.c, L.dt, L.vv_mass.data());
     if (!rc) rc = launch_displacements(L);
     return rc;
