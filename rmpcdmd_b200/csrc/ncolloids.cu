@@ -166,8 +166,10 @@ __global__ void k_fill_cellmap(const int *count, const int *start, int S, int *c
 // cells, eight lanes per cell, fused with cell_maximum_displacement over the
 // same cells (src/particle_system.f90:380-410): each new position is measured
 // against pos_old as it is written (the value that is stored); the squared
-// maximum goes to *out
-template <typename R>
+// maximum goes to *out.  kVel: the previous MD step's cell_md_vel
+// (src/md.f90:239-263) runs first, particle by particle (nothing changes the
+// flags or forces between the two)
+template <typename R, bool kVel>
 __global__ void k_md_cells_pos_disp(const int *list, const int *n_list, const int *count, const int *start,
                                     PView<R> v, Vec3<R> old, R dt, R dt_sq, unsigned long long *out)
 {
@@ -177,8 +179,10 @@ __global__ void k_md_cells_pos_disp(const int *list, const int *n_list, const in
         const int s = list[q / kLanesPerCell], g = (int)(q % kLanesPerCell);
         const int a = start[s], c = count[s];
         for (int i = a + g; i < a + c; i += kLanesPerCell) {
+            const int f = v.flags[i];
+            if (kVel) stream_vel_gated(v, i, f, dt);
             R x, y, z;
-            moved_pos(v, i, v.flags[i], dt, dt_sq, x, y, z);
+            moved_pos(v, i, f, dt, dt_sq, x, y, z);
             v.pos.x[i] = x;
             v.pos.y[i] = y;
             v.pos.z[i] = z;
@@ -339,16 +343,22 @@ static int list_md_cells(NcLoop &L)
     return RMPCD_OK;
 }
 
-// cell_md_pos over the MD cells and their maximum displacement (into the
-// solvent's d_max)
+// cell_md_pos over the MD cells, after the previous MD step's cell_md_vel
+// when that is due, and their maximum displacement (into the solvent's d_max)
 template <typename R>
-static int md_cells_pos_disp_t(NcLoop &L)
+static int md_cells_pos_disp_t(NcLoop &L, bool vel_due)
 {
     cudaStream_t st = stream();
     RMPCD_CUDA_TRY(cudaMemsetAsync(L.s->d_max, 0, 8, st));
     const R dt = (R)L.dt, dt_sq = (R)(L.dt * L.dt / 2);
-    k_md_cells_pos_disp<R><<<md_cells_grid(), 256, 0, st>>>(L.md_list, L.n_md, L.cells->count, L.cells->start,
-                                                           cur<R>(L.s), alt<R>(L.s).pos, dt, dt_sq, L.s->d_max);
+    const PView<R> v = cur<R>(L.s);
+    const Vec3<R> old = alt<R>(L.s).pos;
+    if (vel_due)
+        k_md_cells_pos_disp<R, true><<<md_cells_grid(), 256, 0, st>>>(L.md_list, L.n_md, L.cells->count,
+                                                                     L.cells->start, v, old, dt, dt_sq, L.s->d_max);
+    else
+        k_md_cells_pos_disp<R, false><<<md_cells_grid(), 256, 0, st>>>(L.md_list, L.n_md, L.cells->count,
+                                                                      L.cells->start, v, old, dt, dt_sq, L.s->d_max);
     RMPCD_CHECK_LAUNCH();
     return RMPCD_OK;
 }
@@ -453,38 +463,53 @@ static int catch_up_and_sort(NcLoop &L, bool full_pos_old)
 }
 
 // md_loop up to the displacement maxima (programs/n_colloids_pbc.f90:221-229)
-static int issue_part_a(NcLoop &L)
+// (vel_due: the previous MD step's velocity halves, of the solvent's MD cells
+// and of the colloids, run first)
+static int issue_part_a(NcLoop &L, bool vel_due)
 {
-    int rc = NC_DISPATCH(L, md_cells_pos_disp_t);
+    int rc = L.s->precision == RMPCD_FP32 ? md_cells_pos_disp_t<float>(L, vel_due)
+                                          : md_cells_pos_disp_t<double>(L, vel_due);
+    if (!rc && vel_due) rc = rmpcd_colloid_vv_vel(L.c, L.dt, L.vv_mass.data());
     if (!rc) rc = rmpcd_colloid_vv_pos(L.c, L.dt, L.vv_mass.data());
     if (!rc) rc = launch_displacements(L);
     return rc;
 }
 
-// md_loop after the re-sort test (programs/n_colloids_pbc.f90:243-254), the
-// force switch done; energies only when asked for (they synchronise)
+// md_loop after the re-sort test (programs/n_colloids_pbc.f90:243-254) up to
+// the velocity halves, the force switch done; energies only when asked for
+// (they synchronise).  The velocity halves run with the next MD step's
+// position pass, or in vel_tail after the interval's last MD step.
 static int issue_part_b(NcLoop &L, double *e1, double *e2)
 {
     int rc = NC_DISPATCH(L, roll_clear_t);
     if (!rc) rc = rmpcd_particles_zero_force(L.c);
     if (!rc) rc = compute_force_impl(L.c, L.s, L.nl, L.cells->edges, L.lj_sc, e1, false);
     if (!rc) rc = rmpcd_compute_force_n2(L.c, L.cells->edges, L.lj_cc, e2);
-    if (!rc) rc = NC_DISPATCH(L, md_cells_vel_t);
+    return rc;
+}
+
+// the velocity halves of the interval's last MD step
+static int vel_tail(NcLoop &L)
+{
+    int rc = NC_DISPATCH(L, md_cells_vel_t);
     if (!rc) rc = rmpcd_colloid_vv_vel(L.c, L.dt, L.vv_mass.data());
     return rc;
 }
 
-// one pass of md_loop (programs/n_colloids_pbc.f90:221-254)
-static int md_step(NcLoop &L, bool want_energy)
+// one pass of md_loop (programs/n_colloids_pbc.f90:221-254); vel_due: the
+// previous MD step's velocity halves are still to run (every step of an
+// interval but its first)
+static int md_step(NcLoop &L, bool want_energy, bool vel_due)
 {
     const double dt = L.dt;
     L.st->t += 1;
     int rc;
     if (L.graphs) {
-        const NcLoop::Key ka{L.s->pos[L.s->cur][0], L.s->force[L.s->cur][0], L.c->force[L.c->cur][0], 0};
-        rc = replay(L.part_a, ka, [&] { return issue_part_a(L); });
+        const NcLoop::Key ka{L.s->pos[L.s->cur][0], L.s->force[L.s->cur][0], L.c->force[L.c->cur][0],
+                             vel_due ? 1 : 0};
+        rc = replay(L.part_a, ka, [&] { return issue_part_a(L, vel_due); });
     } else {
-        rc = issue_part_a(L);
+        rc = issue_part_a(L, vel_due);
     }
     double so_max = 0, co_max = 0;
     if (!rc) rc = read_displacements(L, dt * (L.st->t - L.st->last_sort), &so_max, &co_max);
@@ -571,11 +596,12 @@ extern "C" int rmpcd_ncolloids_run(rmpcd_particles *solvent, rmpcd_particles *co
         const int i = first_interval + k;
         int rc = 0;
         for (int j = 0; !rc && j < params->N_MD; j++) {
-            rc = md_step(L, j == params->N_MD - 1);
+            rc = md_step(L, j == params->N_MD - 1, j > 0);
             // the first MD step runs uncaptured (it allocates the force
             // scratch on a first use); graphs stay off while phase timers run
             L.graphs = g_nc_graphs && !timers_on();
         }
+        if (!rc) rc = vel_tail(L);
         if (!rc) rc = rmpcd_cells_random_shift(cells, rng);
         if (!rc) rc = catch_up_and_sort(L, k == n_intervals - 1);
         if (!rc)
