@@ -12,12 +12,18 @@
 //     (particles with MD or PAST_MD set: every other entry is exactly zero),
 //     over all N for the first two MD steps after a sort and over the MD
 //     cells after that;
-//   * the two displacement maxima of an MD step are read with one
-//     synchronisation, and there is no per-call host overhead;
+//   * the re-sort test of an MD step (its two displacement maxima against
+//     the skin) runs on the device in the host's double arithmetic, and the
+//     host reads its decision with one synchronisation; there is no per-call
+//     host overhead;
 //   * an MD step without energies is two replayed CUDA graphs: the part up
-//     to the displacement maxima, and the part after the re-sort decision
-//     (flag roll, forces, velocity updates), each captured once per set of
-//     buffers it touches (the sort and the force switch exchange buffers).
+//     to the re-sort test, and the part after the re-sort decision (flag
+//     roll, forces), each captured once per set of buffers it touches (the
+//     sort and the force switch exchange buffers).  The second is queued
+//     behind an IF node on the device's decision before the host reads it,
+//     so the GPU evaluates the forces while the host waits; on a step that
+//     re-sorts the IF node skips them and the host issues the sort, then the
+//     forces.
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -275,6 +281,37 @@ __global__ void k_roll_clear(int *flags, Vec3<R> force, long long N)
     }
 }
 
+// The program's re-sort test (programs/n_colloids_pbc.f90:230-231) on the
+// device, in the host's double arithmetic: ctl[0] counts the MD steps since
+// the last sort (delta_t = dt * ctl[0]), ctl[1] receives the decision.  The
+// maxima are the squared displacements taken by the MD step's position pass
+// (solvent, floored at max_v * delta_t) and by k_max_disp (colloids).
+__global__ void k_nc_resort_test(const unsigned long long *so_bits, const unsigned long long *co_bits, int *ctl,
+                                 double dt, double max_v, double skin)
+{
+    const int n = ctl[0] + 1;
+    ctl[0] = n;
+    const double delta_t = __dmul_rn(dt, (double)n);
+    const double a = sqrt(__longlong_as_double((long long)*so_bits));
+    const double b = __dmul_rn(max_v, delta_t);
+    const double so_max = a > b ? a : b;
+    const double co_max = sqrt(__longlong_as_double((long long)*co_bits));
+    ctl[1] = (co_max >= __dmul_rn(skin, 0.1)) || (so_max >= __dmul_rn(skin, 0.9)) ? 1 : 0;
+}
+
+// the IF node of a speculatively queued force part runs its body only when
+// the MD step's re-sort test said no
+__global__ void k_nc_set_cond(const int *ctl, cudaGraphConditionalHandle cond)
+{
+    cudaGraphSetConditional(cond, ctl[1] ? 0u : 1u);
+}
+
+__global__ void k_nc_set_since(int *ctl, int since)
+{
+    ctl[0] = since;
+    ctl[1] = 0;
+}
+
 struct NcLoop {
     rmpcd_particles *s, *c;
     rmpcd_cells *cells;
@@ -288,17 +325,22 @@ struct NcLoop {
     int *md_list = nullptr;  // is_md slots
     int *cellmap = nullptr;  // slot of every solvent particle (set by each sort)
     int *n_md = nullptr;     // their number (device)
-    unsigned long long *h_max = nullptr;  // page-locked landing of the two maxima
+    int *ctl = nullptr;      // device: MD steps since the last sort, re-sort decision
+    int *h_ctl = nullptr;    // page-locked landing of ctl
+    cudaEvent_t ev_a = nullptr;  // end of the MD step's part up to the re-sort test
     int full_rolls = 2;  // rolls over all N still due since the last sort
-    // replayed parts of an MD step, keyed by the buffers they use
+    // replayed parts of an MD step, keyed by the buffers they use; part_bs is
+    // part_b behind an IF node on the step's re-sort decision
     using Key = std::tuple<const void *, const void *, const void *, int>;
-    std::map<Key, cudaGraphExec_t> part_a, part_b;
+    std::map<Key, cudaGraphExec_t> part_a, part_b, part_bs;
     bool graphs = false;
+    bool speculate = true;  // queue part_bs before the host reads the decision
 
     ~NcLoop()
     {
         for (auto &kv : part_a) cudaGraphExecDestroy(kv.second);
         for (auto &kv : part_b) cudaGraphExecDestroy(kv.second);
+        for (auto &kv : part_bs) cudaGraphExecDestroy(kv.second);
     }
 };
 
@@ -416,30 +458,32 @@ static int md_cells_copy_pos_t(NcLoop &L)
 
 #define NC_DISPATCH(L, fn) ((L).s->precision == RMPCD_FP32 ? fn<float>(L) : fn<double>(L))
 
-// the displacement maxima of the MD step (the solvent's over the MD cells,
-// floored at max_v * delta_t when read, was taken with its positions) and the
-// colloids', read with one synchronisation
+// the displacement maxima of the MD step (the solvent's over the MD cells was
+// taken with its positions) and the colloids', the re-sort test on the
+// device, and its decision copied to the host
 static int launch_displacements(NcLoop &L)
 {
     int rc = launch_max_disp(L.c);
     if (rc) return rc;
-    unsigned long long *bits = L.h_max;
-    RMPCD_CUDA_TRY(cudaMemcpyAsync(bits, L.s->d_max, 8, cudaMemcpyDeviceToHost, stream()));
-    RMPCD_CUDA_TRY(cudaMemcpyAsync(bits + 1, L.c->d_max, 8, cudaMemcpyDeviceToHost, stream()));
+    cudaStream_t st = stream();
+    k_nc_resort_test<<<1, 1, 0, st>>>(L.s->d_max, L.c->d_max, L.ctl, L.dt, L.cells->max_v, L.prm->skin);
+    RMPCD_CHECK_LAUNCH();
+    RMPCD_CUDA_TRY(cudaMemcpyAsync(L.h_ctl, L.ctl, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     return RMPCD_OK;
 }
 
-static int read_displacements(NcLoop &L, double delta_t, double *so_max, double *co_max)
+// the re-sort decision of the MD step, once the stream has reached its copy
+// (after the whole stream when ev is null)
+static int read_resort(NcLoop &L, cudaEvent_t ev, bool *resort)
 {
-    int rc = sync();
-    if (rc) return rc;
-    unsigned long long *bits = L.h_max;
-    double m0, m1;
-    memcpy(&m0, bits, 8);
-    memcpy(&m1, bits + 1, 8);
-    const double a = sqrt(m0), b = L.cells->max_v * delta_t;
-    *so_max = a > b ? a : b;
-    *co_max = sqrt(m1);
+    if (ev) {
+        const cudaError_t e = cudaEventSynchronize(ev);
+        if (e != cudaSuccess) return fail(RMPCD_ERR_CUDA, "n_colloids step: %s", cudaGetErrorString(e));
+    } else {
+        const int rc = sync();
+        if (rc) return rc;
+    }
+    *resort = ((volatile int *)L.h_ctl)[1] != 0;
     return RMPCD_OK;
 }
 
@@ -454,6 +498,8 @@ static int catch_up_and_sort(NcLoop &L, bool full_pos_old)
     if (!rc) rc = rmpcd_apply_pbc(L.c, L.cells->edges);
     if (!rc) rc = sort_keyed_flagged(L.cells, L.s, L.cellmap);  // the solvent's wrap and keys are done
     L.st->last_sort = L.st->t;
+    if (!rc && cudaMemsetAsync(L.ctl, 0, sizeof(int), stream()) != cudaSuccess)
+        rc = fail(RMPCD_ERR_CUDA, "n_colloids sort: step counter reset failed");
     L.full_rolls = 2;
     if (!rc) rc = rmpcd_nlist_update(L.nl, L.c, L.s, L.prm->list_radius, L.cells, nullptr);
     if (!rc) rc = list_md_cells(L);
@@ -488,6 +534,60 @@ static int issue_part_b(NcLoop &L, double *e1, double *e2)
     return rc;
 }
 
+// part_b behind an IF node that runs it only when the MD step's re-sort test
+// (already queued) said no: captured once per key into a graph made of
+// k_nc_set_cond and the IF node, whose body is captured from issue_part_b.
+// Returns RMPCD_ERR_CUDA, with the stream out of capture, when the graph cannot
+// be built; the caller then issues the step without speculation.
+static int replay_spec(NcLoop &L, const NcLoop::Key &key)
+{
+    cudaStream_t st = stream();
+    auto it = L.part_bs.find(key);
+    if (it == L.part_bs.end()) {
+        cudaGraph_t g = nullptr, out = nullptr;
+        cudaGraphConditionalHandle cond = 0;
+        cudaError_t e = cudaGraphCreate(&g, 0);
+        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault);
+        if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        cudaGraph_t body = nullptr;
+        if (e == cudaSuccess) {
+            k_nc_set_cond<<<1, 1, 0, st>>>(L.ctl, cond);
+            e = cudaGetLastError();
+            cudaStreamCaptureStatus cs;
+            const cudaGraphNode_t *deps = nullptr;
+            size_t nd = 0;
+            if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &nd);
+            cudaGraphNodeParams cp{};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = cond;
+            cp.conditional.type = cudaGraphCondTypeIf;
+            cp.conditional.size = 1;
+            cudaGraphNode_t node = nullptr;
+            if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, deps, nd, &cp);
+            if (e == cudaSuccess) body = cp.conditional.phGraph_out[0];
+            const cudaError_t ee = cudaStreamEndCapture(st, &out);
+            if (e == cudaSuccess) e = ee;
+        }
+        int rc = RMPCD_OK;
+        if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            rc = issue_part_b(L, nullptr, nullptr);
+            const cudaError_t ee = cudaStreamEndCapture(st, &out);
+            if (e == cudaSuccess) e = ee;
+        }
+        cudaGraphExec_t x = nullptr;
+        if (e == cudaSuccess && !rc) e = cudaGraphInstantiate(&x, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess || rc) {
+            cudaGetLastError();
+            return fail(RMPCD_ERR_CUDA, "n_colloids speculative step: %s", cudaGetErrorString(e));
+        }
+        it = L.part_bs.emplace(key, x).first;
+    }
+    RMPCD_CUDA_TRY(cudaGraphLaunch(it->second, st));
+    return RMPCD_OK;
+}
+
 // the velocity halves of the interval's last MD step
 static int vel_tail(NcLoop &L)
 {
@@ -496,30 +596,11 @@ static int vel_tail(NcLoop &L)
     return rc;
 }
 
-// one pass of md_loop (programs/n_colloids_pbc.f90:221-254); vel_due: the
-// previous MD step's velocity halves are still to run (every step of an
-// interval but its first)
-static int md_step(NcLoop &L, bool want_energy, bool vel_due)
+// md_loop after the re-sort (programs/n_colloids_pbc.f90:243-254): the force
+// switch, then part_b (replayed, or issued with the energies when asked for)
+static int md_step_forces(NcLoop &L, bool want_energy)
 {
-    const double dt = L.dt;
-    L.st->t += 1;
-    int rc;
-    if (L.graphs) {
-        const NcLoop::Key ka{L.s->pos[L.s->cur][0], L.s->force[L.s->cur][0], L.c->force[L.c->cur][0],
-                             vel_due ? 1 : 0};
-        rc = replay(L.part_a, ka, [&] { return issue_part_a(L, vel_due); });
-    } else {
-        rc = issue_part_a(L, vel_due);
-    }
-    double so_max = 0, co_max = 0;
-    if (!rc) rc = read_displacements(L, dt * (L.st->t - L.st->last_sort), &so_max, &co_max);
-    if (rc) return rc;
-    if ((co_max >= L.prm->skin * 0.1) || (so_max >= L.prm->skin * 0.9)) {
-        rc = catch_up_and_sort(L, false);
-        if (rc) return rc;
-        L.st->n_extra_sorting += 1;
-    }
-    rc = rmpcd_particles_switch_force(L.s);
+    int rc = rmpcd_particles_switch_force(L.s);
     if (!rc) rc = rmpcd_particles_switch_force(L.c);
     if (rc) return rc;
     if (L.graphs && !want_energy) {
@@ -541,6 +622,72 @@ static int md_step(NcLoop &L, bool want_energy, bool vel_due)
         L.st->e2 = e2;
     }
     return rc;
+}
+
+// one pass of md_loop (programs/n_colloids_pbc.f90:221-254); vel_due: the
+// previous MD step's velocity halves are still to run (every step of an
+// interval but its first)
+static int md_step(NcLoop &L, bool want_energy, bool vel_due)
+{
+    L.st->t += 1;
+    int rc;
+    if (L.graphs) {
+        const NcLoop::Key ka{L.s->pos[L.s->cur][0], L.s->force[L.s->cur][0], L.c->force[L.c->cur][0],
+                             vel_due ? 1 : 0};
+        rc = replay(L.part_a, ka, [&] { return issue_part_a(L, vel_due); });
+    } else {
+        rc = issue_part_a(L, vel_due);
+    }
+    if (rc) return rc;
+    if (L.graphs && L.speculate && !want_energy) {
+        // queue the force part before reading the decision: while the host
+        // waits for it, the GPU has the forces to evaluate (or, on a step that
+        // re-sorts, an IF node that skips them)
+        RMPCD_CUDA_TRY(cudaEventRecord(L.ev_a, stream()));
+        rc = rmpcd_particles_switch_force(L.s);
+        if (!rc) rc = rmpcd_particles_switch_force(L.c);
+        if (rc) return rc;
+        const int before = L.full_rolls;
+        const bool fz[4] = {L.s->force_zero, L.s->force_old_zero, L.c->force_zero, L.c->force_old_zero};
+        const NcLoop::Key kb{L.s->pos[L.s->cur][0], L.s->force[L.s->cur][0], L.c->force[L.c->cur][0],
+                             before > 0 ? 1 : 0};
+        const int rs = replay_spec(L, kb);
+        bool resort = false;
+        rc = read_resort(L, L.ev_a, &resort);
+        if (rc) return rc;
+        if (!rs && !resort) {
+            L.full_rolls = before > 0 ? before - 1 : 0;
+            L.s->force_zero = false;
+            L.c->force_zero = false;
+            return RMPCD_OK;
+        }
+        // the queued part did nothing (or was not built): undo the host-side
+        // bookkeeping of its capture and the force switch, then go on as below
+        if (rs) L.speculate = false;
+        L.full_rolls = before;
+        L.s->force_zero = fz[0];
+        L.s->force_old_zero = fz[1];
+        L.c->force_zero = fz[2];
+        L.c->force_old_zero = fz[3];
+        rc = rmpcd_particles_switch_force(L.s);
+        if (!rc) rc = rmpcd_particles_switch_force(L.c);
+        if (rc) return rc;
+        if (resort) {
+            rc = catch_up_and_sort(L, false);
+            if (rc) return rc;
+            L.st->n_extra_sorting += 1;
+        }
+        return md_step_forces(L, want_energy);
+    }
+    bool resort = false;
+    rc = read_resort(L, nullptr, &resort);
+    if (rc) return rc;
+    if (resort) {
+        rc = catch_up_and_sort(L, false);
+        if (rc) return rc;
+        L.st->n_extra_sorting += 1;
+    }
+    return md_step_forces(L, want_energy);
 }
 
 }  // namespace rmpcd
@@ -582,15 +729,20 @@ extern "C" int rmpcd_ncolloids_run(rmpcd_particles *solvent, rmpcd_particles *co
     RMPCD_CUDA_TRY(cudaMalloc(&L.md_list, (size_t)(cells->S > 0 ? cells->S : 1) * sizeof(int)));
     if (cudaMalloc(&L.n_md, sizeof(int)) != cudaSuccess ||
         cudaMalloc(&L.cellmap, (size_t)(solvent->N > 0 ? solvent->N : 1) * sizeof(int)) != cudaSuccess ||
-        cudaHostAlloc(&L.h_max, 2 * sizeof(unsigned long long), cudaHostAllocDefault) != cudaSuccess) {
+        cudaMalloc(&L.ctl, 2 * sizeof(int)) != cudaSuccess ||
+        cudaHostAlloc(&L.h_ctl, 2 * sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
+        cudaEventCreateWithFlags(&L.ev_a, cudaEventDisableTiming) != cudaSuccess) {
         cudaFree(L.md_list);
         cudaFree(L.n_md);
         cudaFree(L.cellmap);
+        cudaFree(L.ctl);
+        if (L.h_ctl) cudaFreeHost(L.h_ctl);
         return fail(RMPCD_ERR_CUDA, "rmpcd_ncolloids_run: allocation failed");
     }
     // the solvent is sorted on entry: its slots from the cell ranges
     k_fill_cellmap<<<grid_full((long long)cells->S * kLanesPerCell, 256), 256, 0, stream()>>>(
         cells->count, cells->start, cells->S, L.cellmap);
+    k_nc_set_since<<<1, 1, 0, stream()>>>(L.ctl, state->t - state->last_sort);
     int rc0 = list_md_cells(L);
     for (int k = 0; !rc0 && k < n_intervals; k++) {
         const int i = first_interval + k;
@@ -613,7 +765,9 @@ extern "C" int rmpcd_ncolloids_run(rmpcd_particles *solvent, rmpcd_particles *co
     cudaFree(L.md_list);
     cudaFree(L.n_md);
     cudaFree(L.cellmap);
-    cudaFreeHost(L.h_max);
+    cudaFree(L.ctl);
+    cudaFreeHost(L.h_ctl);
+    cudaEventDestroy(L.ev_a);
     if (rc0) return rc0;
     return check_dev_error(nullptr);
 }
