@@ -27,10 +27,13 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <memory>
+#include <mutex>
 #include <tuple>
 #include <vector>
 
 #include "keys.cuh"
+#include "nlist_ops.cuh"
 #include "rmpcd_common.cuh"
 #include "sortcore.cuh"
 #include "state.cuh"
@@ -238,6 +241,18 @@ __global__ void k_md_cells_copy_pos(const int *list, const int *n_list, const in
     }
 }
 
+// zero_force of the colloids (the entries that the step's compute_force and
+// compute_force_n2 accumulate into), done by the first threads of the solvent
+// roll that starts the step's force part
+__device__ inline void zero_colloid_force(const Vec3<double> &cf, int nc)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nc; q += gridDim.x * blockDim.x) {
+        cf.x[q] = 0;
+        cf.y[q] = 0;
+        cf.z[q] = 0;
+    }
+}
+
 // the roll + clear below restricted to the listed MD cells.  Between two
 // sorts the list is fixed and compute_force flags only list entries, which
 // lie in MD cells; so once two rolls have run over every particle after a
@@ -247,8 +262,9 @@ __global__ void k_md_cells_copy_pos(const int *list, const int *n_list, const in
 // same flags and forces as rolling all N.
 template <typename R>
 __global__ void k_md_cells_roll_clear(const int *list, const int *n_list, const int *count, const int *start,
-                                      int *flags, Vec3<R> force)
+                                      int *flags, Vec3<R> force, Vec3<double> cf, int nc)
 {
+    zero_colloid_force(cf, nc);
     const long long n = (long long)*n_list * kLanesPerCell;
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
         const int s = list[q / kLanesPerCell], g = (int)(q % kLanesPerCell);
@@ -268,8 +284,9 @@ __global__ void k_md_cells_roll_clear(const int *list, const int *n_list, const 
 // zero_force of the solvent fused with the PAST_MD/MD roll: only entries of
 // particles with MD or PAST_MD set can be non-zero
 template <typename R>
-__global__ void k_roll_clear(int *flags, Vec3<R> force, long long N)
+__global__ void k_roll_clear(int *flags, Vec3<R> force, long long N, Vec3<double> cf, int nc)
 {
+    zero_colloid_force(cf, nc);
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
         const int f = flags[i];
         if (f & ((1 << MD_BIT) | (1 << PAST_MD_BIT))) {
@@ -285,9 +302,9 @@ __global__ void k_roll_clear(int *flags, Vec3<R> force, long long N)
 // device, in the host's double arithmetic: ctl[0] counts the MD steps since
 // the last sort (delta_t = dt * ctl[0]), ctl[1] receives the decision.  The
 // maxima are the squared displacements taken by the MD step's position pass
-// (solvent, floored at max_v * delta_t) and by k_max_disp (colloids).
-__global__ void k_nc_resort_test(const unsigned long long *so_bits, const unsigned long long *co_bits, int *ctl,
-                                 double dt, double max_v, double skin)
+// (solvent, floored at max_v * delta_t) and of the colloids.
+__device__ inline void nc_resort_test(unsigned long long *so_bits, double co_sq, int *ctl, double dt,
+                                      double max_v, double skin)
 {
     const int n = ctl[0] + 1;
     ctl[0] = n;
@@ -295,8 +312,40 @@ __global__ void k_nc_resort_test(const unsigned long long *so_bits, const unsign
     const double a = sqrt(__longlong_as_double((long long)*so_bits));
     const double b = __dmul_rn(max_v, delta_t);
     const double so_max = a > b ? a : b;
-    const double co_max = sqrt(__longlong_as_double((long long)*co_bits));
+    const double co_max = sqrt(co_sq);
     ctl[1] = (co_max >= __dmul_rn(skin, 0.1)) || (so_max >= __dmul_rn(skin, 0.9)) ? 1 : 0;
+    *so_bits = 0;  // cleared for the next MD step's position pass
+}
+
+// The colloid part of an MD step up to the re-sort test, one block: the
+// previous MD step's velocity half when due, the position half (the colloid
+// velocity Verlet of programs/n_colloids_pbc.f90:222-224, :248-249), the
+// colloids' largest displacement since the last sort (maximum_displacement,
+// src/particle_system.f90:357-378; a maximum, so the same in any order), then
+// the re-sort test.  Each colloid's updates are those of rmpcd_colloid_vv_vel
+// and rmpcd_colloid_vv_pos, which touch no other colloid.
+constexpr int kNcColloidThreads = 256;
+
+template <bool kVel>
+__global__ void __launch_bounds__(kNcColloidThreads)
+    k_nc_colloid_begin(PView<double> c, Vec3<double> c_old, const double *mass, double dt,
+                       unsigned long long *so_bits, int *ctl, double max_v, double skin)
+{
+    __shared__ double s_m[kNcColloidThreads / 32];
+    double m = 0;
+    for (int i = threadIdx.x; i < c.N; i += blockDim.x) {
+        if (kVel) colloid_vv_vel_one(c, i, mass[i], dt);
+        colloid_vv_pos_one(c, i, mass[i], dt);
+        const double r = disp_sq_one(c.pos, c_old, c.species, i);
+        m = m > r ? m : r;
+    }
+    m = warp_max(m);
+    if ((threadIdx.x & 31) == 0) s_m[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kNcColloidThreads / 32; w++) m = m > s_m[w] ? m : s_m[w];
+        nc_resort_test(so_bits, m, ctl, dt, max_v, skin);
+    }
 }
 
 // the IF node of a speculatively queued force part runs its body only when
@@ -326,8 +375,13 @@ struct NcLoop {
     int *cellmap = nullptr;  // slot of every solvent particle (set by each sort)
     int *n_md = nullptr;     // their number (device)
     int *ctl = nullptr;      // device: MD steps since the last sort, re-sort decision
+    double *d_mass = nullptr;  // velocity-Verlet masses of the colloids (device)
     int *h_ctl = nullptr;    // page-locked landing of ctl
     cudaEvent_t ev_a = nullptr;  // end of the MD step's part up to the re-sort test
+    // second stream of the force evaluation (colloid sums and colloid-colloid
+    // forces beside the solvent force application)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int full_rolls = 2;  // rolls over all N still due since the last sort
     // replayed parts of an MD step, keyed by the buffers they use; part_bs is
     // part_b behind an IF node on the step's re-sort decision
@@ -335,14 +389,121 @@ struct NcLoop {
     std::map<Key, cudaGraphExec_t> part_a, part_b, part_bs;
     bool graphs = false;
     bool speculate = true;  // queue part_bs before the host reads the decision
+    // what the captured graphs depend on besides their keys (see nc_signature)
+    std::vector<unsigned long long> sig;
 
     ~NcLoop()
     {
         for (auto &kv : part_a) cudaGraphExecDestroy(kv.second);
         for (auto &kv : part_b) cudaGraphExecDestroy(kv.second);
         for (auto &kv : part_bs) cudaGraphExecDestroy(kv.second);
+        cudaFree(md_list);
+        cudaFree(n_md);
+        cudaFree(cellmap);
+        cudaFree(ctl);
+        cudaFree(d_mass);
+        if (h_ctl) cudaFreeHost(h_ctl);
+        if (ev_a) cudaEventDestroy(ev_a);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (side) cudaStreamDestroy(side);
     }
 };
+
+// Everything a captured MD-step graph bakes in besides the buffers of its key:
+// the device, the handles and every device array of theirs that a graph can touch, the
+// sizes, the box, max_v, the LJ tables (passed by value to the kernels) and
+// the step parameters.  The loop's scratch and graphs are kept for the next
+// call while this is unchanged.
+static std::vector<unsigned long long> nc_signature(const rmpcd_particles *s, const rmpcd_particles *c,
+                                                     const rmpcd_cells *cells, const rmpcd_nlist *nl,
+                                                     const rmpcd_lj *lj_sc, const rmpcd_lj *lj_cc,
+                                                     const rmpcd_ncolloids_params *prm)
+{
+    std::vector<unsigned long long> v;
+    int dev = -1;
+    cudaGetDevice(&dev);
+    v.push_back((unsigned long long)dev);
+    auto add = [&](const void *p) { v.push_back((unsigned long long)(uintptr_t)p); };
+    auto num = [&](double x) {
+        unsigned long long b;
+        memcpy(&b, &x, 8);
+        v.push_back(b);
+    };
+    auto bytes = [&](const void *p, size_t n) {
+        for (size_t o = 0; o < n; o += 8) {
+            unsigned long long b = 0;
+            memcpy(&b, (const char *)p + o, n - o < 8 ? n - o : 8);
+            v.push_back(b);
+        }
+    };
+    for (const rmpcd_particles *p : {s, c}) {
+        add(p);
+        v.push_back((unsigned long long)p->N);
+        v.push_back((unsigned long long)p->precision);
+        for (int b = 0; b < 2; b++) {
+            for (int k = 0; k < 3; k++) {
+                add(p->pos[b][k]);
+                add(p->vel[b][k]);
+                add(p->force[b][k]);
+                add(p->force_old[b][k]);
+                add(p->image[b][k]);
+            }
+            add(p->id[b]);
+            add(p->species[b]);
+            add(p->flags[b]);
+        }
+        add(p->d_max);
+    }
+    add(cells);
+    v.push_back((unsigned long long)cells->S);
+    for (int k = 0; k < 3; k++) num(cells->edges[k]);
+    num(cells->max_v);
+    add(cells->count);
+    add(cells->start);
+    add(cells->is_md);
+    add(cells->is_reac);
+    add(nl);
+    v.push_back((unsigned long long)nl->Npoints);
+    v.push_back((unsigned long long)nl->Nmax);
+    v.push_back((unsigned long long)nl->max_i);
+    for (int k = 0; k < 3; k++) v.push_back((unsigned long long)nl->box_cells[k]);
+    add(nl->list);
+    add(nl->n);
+    add(nl->pair_f);
+    add(nl->pair_e);
+    add(nl->contrib);
+    add(nl->ncontrib);
+    add(nl->d_status);
+    add(nl->mkeys);
+    add(nl->e_pre);
+    const LJDev a = lj_dev(lj_sc), b = lj_dev(lj_cc);
+    bytes(&a, sizeof a);
+    bytes(&b, sizeof b);
+    num(prm->tau);
+    v.push_back((unsigned long long)prm->N_MD);
+    num(prm->skin);
+    return v;
+}
+
+// scratch, events and the second stream of a loop
+static int nc_alloc(NcLoop &L, int S, int N, int C)
+{
+    if (cudaMalloc(&L.md_list, (size_t)(S > 0 ? S : 1) * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&L.n_md, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&L.cellmap, (size_t)(N > 0 ? N : 1) * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&L.ctl, 2 * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&L.d_mass, (size_t)(C > 0 ? C : 1) * sizeof(double)) != cudaSuccess ||
+        cudaHostAlloc(&L.h_ctl, 2 * sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
+        cudaEventCreateWithFlags(&L.ev_a, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&L.ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&L.ev_join, cudaEventDisableTiming) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&L.side, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(RMPCD_ERR_CUDA, "rmpcd_ncolloids_run: allocation failed");
+    }
+    return RMPCD_OK;
+}
 
 // run issue() once under stream capture the first time `key` is seen, then
 // replay the instantiated graph
@@ -386,12 +547,12 @@ static int list_md_cells(NcLoop &L)
 }
 
 // cell_md_pos over the MD cells, after the previous MD step's cell_md_vel
-// when that is due, and their maximum displacement (into the solvent's d_max)
+// when that is due, and their maximum displacement (into the solvent's d_max,
+// zero on entry: cleared when the loop starts and by each re-sort test)
 template <typename R>
 static int md_cells_pos_disp_t(NcLoop &L, bool vel_due)
 {
     cudaStream_t st = stream();
-    RMPCD_CUDA_TRY(cudaMemsetAsync(L.s->d_max, 0, 8, st));
     const R dt = (R)L.dt, dt_sq = (R)(L.dt * L.dt / 2);
     const PView<R> v = cur<R>(L.s);
     const Vec3<R> old = alt<R>(L.s).pos;
@@ -418,14 +579,18 @@ template <typename R>
 static int roll_clear_t(NcLoop &L)
 {
     PView<R> v = cur<R>(L.s);
+    const Vec3<double> cf = cur<double>(L.c).force;
+    const int nc = L.c->N;
     if (L.full_rolls > 0) {
-        if (L.s->N > 0) k_roll_clear<R><<<grid_for(L.s->N, 256), 256, 0, stream()>>>(v.flags, v.force, L.s->N);
+        const long long n = L.s->N > nc ? L.s->N : nc;
+        k_roll_clear<R><<<grid_for(n > 0 ? n : 1, 256), 256, 0, stream()>>>(v.flags, v.force, L.s->N, cf, nc);
         L.full_rolls--;
     } else {
         k_md_cells_roll_clear<R><<<md_cells_grid(), 256, 0, stream()>>>(L.md_list, L.n_md, L.cells->count,
-                                                                        L.cells->start, v.flags, v.force);
+                                                                        L.cells->start, v.flags, v.force, cf, nc);
     }
     RMPCD_CHECK_LAUNCH();
+    L.c->force_zero = true;
     return RMPCD_OK;
 }
 
@@ -458,15 +623,20 @@ static int md_cells_copy_pos_t(NcLoop &L)
 
 #define NC_DISPATCH(L, fn) ((L).s->precision == RMPCD_FP32 ? fn<float>(L) : fn<double>(L))
 
-// the displacement maxima of the MD step (the solvent's over the MD cells was
-// taken with its positions) and the colloids', the re-sort test on the
-// device, and its decision copied to the host
-static int launch_displacements(NcLoop &L)
+// the colloid part of the MD step and the re-sort test (the solvent's
+// maximum displacement over the MD cells was taken with its positions), and
+// the decision copied to the host
+static int colloid_begin(NcLoop &L, bool vel_due)
 {
-    int rc = launch_max_disp(L.c);
-    if (rc) return rc;
     cudaStream_t st = stream();
-    k_nc_resort_test<<<1, 1, 0, st>>>(L.s->d_max, L.c->d_max, L.ctl, L.dt, L.cells->max_v, L.prm->skin);
+    const PView<double> c = cur<double>(L.c);
+    const Vec3<double> c_old = alt<double>(L.c).pos;
+    if (vel_due)
+        k_nc_colloid_begin<true><<<1, kNcColloidThreads, 0, st>>>(c, c_old, L.d_mass, L.dt, L.s->d_max, L.ctl,
+                                                                  L.cells->max_v, L.prm->skin);
+    else
+        k_nc_colloid_begin<false><<<1, kNcColloidThreads, 0, st>>>(c, c_old, L.d_mass, L.dt, L.s->d_max, L.ctl,
+                                                                   L.cells->max_v, L.prm->skin);
     RMPCD_CHECK_LAUNCH();
     RMPCD_CUDA_TRY(cudaMemcpyAsync(L.h_ctl, L.ctl, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     return RMPCD_OK;
@@ -515,9 +685,7 @@ static int issue_part_a(NcLoop &L, bool vel_due)
 {
     int rc = L.s->precision == RMPCD_FP32 ? md_cells_pos_disp_t<float>(L, vel_due)
                                           : md_cells_pos_disp_t<double>(L, vel_due);
-    if (!rc && vel_due) rc = rmpcd_colloid_vv_vel(L.c, L.dt, L.vv_mass.data());
-    if (!rc) rc = rmpcd_colloid_vv_pos(L.c, L.dt, L.vv_mass.data());
-    if (!rc) rc = launch_displacements(L);
+    if (!rc) rc = colloid_begin(L, vel_due);
     return rc;
 }
 
@@ -527,8 +695,12 @@ static int issue_part_a(NcLoop &L, bool vel_due)
 // position pass, or in vel_tail after the interval's last MD step.
 static int issue_part_b(NcLoop &L, double *e1, double *e2)
 {
-    int rc = NC_DISPATCH(L, roll_clear_t);
-    if (!rc) rc = rmpcd_particles_zero_force(L.c);
+    int rc = NC_DISPATCH(L, roll_clear_t);  // zero_force of the colloids included
+    if (!e1 && !e2) {
+        const ForceN2Branch n2{L.lj_cc, L.side, L.ev_fork, L.ev_join};
+        if (!rc) rc = compute_force_impl(L.c, L.s, L.nl, L.cells->edges, L.lj_sc, nullptr, false, &n2);
+        return rc;
+    }
     if (!rc) rc = compute_force_impl(L.c, L.s, L.nl, L.cells->edges, L.lj_sc, e1, false);
     if (!rc) rc = rmpcd_compute_force_n2(L.c, L.cells->edges, L.lj_cc, e2);
     return rc;
@@ -695,6 +867,10 @@ static int md_step(NcLoop &L, bool want_energy, bool vel_due)
 using namespace rmpcd;
 
 static bool g_nc_graphs = true;
+// the loop kept from the last call (scratch and captured graphs), and the
+// lock that one thread at a time holds while it runs on it
+static std::mutex g_nc_mutex;
+static NcLoop *g_nc_loop = nullptr;
 
 extern "C" int rmpcd_ncolloids_set_graphs(int on)
 {
@@ -713,7 +889,31 @@ extern "C" int rmpcd_ncolloids_run(rmpcd_particles *solvent, rmpcd_particles *co
     RMPCD_ARG(n_intervals >= 0 && params->N_MD >= 1 && params->tau > 0, "n_intervals >= 0, N_MD >= 1, tau > 0");
     RMPCD_ARG(!thermostat || T, "a thermostatted run needs the temperatures T");
     RMPCD_ARG(colloids->precision == RMPCD_FP64, "colloids must be FP64");
-    NcLoop L;
+    // the loop of the previous call is reused (scratch and graphs) when its
+    // signature matches; a call that finds it in use by another thread runs
+    // on a loop of its own
+    std::unique_lock<std::mutex> lk(g_nc_mutex, std::try_to_lock);
+    std::unique_ptr<NcLoop> own;
+    NcLoop *Lp = nullptr;
+    std::vector<unsigned long long> sig;
+    const bool keep = lk.owns_lock() && g_nc_graphs;
+    if (keep) {
+        sig = nc_signature(solvent, colloids, cells, nl, solvent_colloid, colloid_colloid, params);
+        if (g_nc_loop && g_nc_loop->sig == sig) {
+            Lp = g_nc_loop;
+        } else if (g_nc_loop) {
+            cudaStreamSynchronize(stream());
+            delete g_nc_loop;
+            g_nc_loop = nullptr;
+        }
+    }
+    if (!Lp) {
+        own.reset(new NcLoop);
+        Lp = own.get();
+        const int rc = nc_alloc(*Lp, cells->S, solvent->N, colloids->N);
+        if (rc) return rc;
+    }
+    NcLoop &L = *Lp;
     L.s = solvent;
     L.c = colloids;
     L.cells = cells;
@@ -725,24 +925,17 @@ extern "C" int rmpcd_ncolloids_run(rmpcd_particles *solvent, rmpcd_particles *co
     L.st = state;
     L.vv_mass.assign((size_t)colloids->N, params->mass);
     L.dt = params->tau / params->N_MD;
+    L.full_rolls = 2;
+    L.graphs = false;
     PhaseTimer timer("ncolloids_run");
-    RMPCD_CUDA_TRY(cudaMalloc(&L.md_list, (size_t)(cells->S > 0 ? cells->S : 1) * sizeof(int)));
-    if (cudaMalloc(&L.n_md, sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&L.cellmap, (size_t)(solvent->N > 0 ? solvent->N : 1) * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&L.ctl, 2 * sizeof(int)) != cudaSuccess ||
-        cudaHostAlloc(&L.h_ctl, 2 * sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
-        cudaEventCreateWithFlags(&L.ev_a, cudaEventDisableTiming) != cudaSuccess) {
-        cudaFree(L.md_list);
-        cudaFree(L.n_md);
-        cudaFree(L.cellmap);
-        cudaFree(L.ctl);
-        if (L.h_ctl) cudaFreeHost(L.h_ctl);
-        return fail(RMPCD_ERR_CUDA, "rmpcd_ncolloids_run: allocation failed");
-    }
+    if (colloids->N > 0)
+        RMPCD_CUDA_TRY(cudaMemcpyAsync(L.d_mass, L.vv_mass.data(), (size_t)colloids->N * sizeof(double),
+                                       cudaMemcpyHostToDevice, stream()));
     // the solvent is sorted on entry: its slots from the cell ranges
     k_fill_cellmap<<<grid_full((long long)cells->S * kLanesPerCell, 256), 256, 0, stream()>>>(
         cells->count, cells->start, cells->S, L.cellmap);
     k_nc_set_since<<<1, 1, 0, stream()>>>(L.ctl, state->t - state->last_sort);
+    RMPCD_CUDA_TRY(cudaMemsetAsync(solvent->d_max, 0, 8, stream()));
     int rc0 = list_md_cells(L);
     for (int k = 0; !rc0 && k < n_intervals; k++) {
         const int i = first_interval + k;
@@ -762,12 +955,20 @@ extern "C" int rmpcd_ncolloids_run(rmpcd_particles *solvent, rmpcd_particles *co
         rc0 = rc;
     }
     cudaStreamSynchronize(stream());
-    cudaFree(L.md_list);
-    cudaFree(L.n_md);
-    cudaFree(L.cellmap);
-    cudaFree(L.ctl);
-    cudaFreeHost(L.h_ctl);
-    cudaEventDestroy(L.ev_a);
+    if (keep) {
+        if (rc0) {
+            // an error drops the kept loop
+            if (Lp == g_nc_loop) {
+                delete g_nc_loop;
+                g_nc_loop = nullptr;
+            }
+        } else if (own) {
+            // the force scratch may have been allocated by this call: the
+            // signature is taken again before the loop is kept
+            L.sig = nc_signature(solvent, colloids, cells, nl, solvent_colloid, colloid_colloid, params);
+            g_nc_loop = own.release();
+        }
+    }
     if (rc0) return rc0;
     return check_dev_error(nullptr);
 }

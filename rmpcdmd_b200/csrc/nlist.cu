@@ -91,10 +91,15 @@ __global__ void k_apply_single(const int *list, const int *n, int Nmax, const un
 
 template <typename R>
 __global__ void k_apply_multi(const int *list, const int *n, int C, int Nmax, const unsigned char *contrib,
-                              const double *pf, const int *ncontrib, const int *max_contrib, int serial,
+                              const double *pf, const int *ncontrib, int *max_contrib, int serial,
                               R *fx, R *fy, R *fz, const unsigned long long *mkeys, int *m_count)
 {
-    if (*max_contrib < 2) return;
+    // the largest contribution count, read by every thread before thread 0
+    // clears it for the next evaluation
+    const int mc = *max_contrib;
+    __syncthreads();
+    if (threadIdx.x == 0) *max_contrib = 0;
+    if (mc < 2) return;
     const int m = *m_count;
     if (!apply_multi_sorted_block(mkeys, m, pf, fx, fy, fz))
         apply_multi_block(list, n, C, Nmax, contrib, pf, ncontrib, serial, fx, fy, fz);
@@ -457,8 +462,22 @@ int rmpcd_compute_force(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist 
 
 namespace rmpcd {
 
+// the force kernels of compute_force_n2 (src/neighbor_list.f90:227-264) on st
+static void launch_force_n2(rmpcd_particles *ps, const double L[3], const rmpcd_lj *lj, cudaStream_t st)
+{
+    const int C = ps->N;
+    PView<double> v = cur<double>(ps);
+    LJDev ld = lj_dev(lj);
+    if (C <= 32)
+        k_force_n2<<<1, 32, 0, st>>>(v.pos.x, v.pos.y, v.pos.z, v.species, C, L[0], L[1], L[2], ld, v.force.x,
+                                     v.force.y, v.force.z);
+    else
+        k_force_n2_blocks<<<C, kNlBlockThreads, 0, st>>>(v.pos.x, v.pos.y, v.pos.z, v.species, C, L[0], L[1], L[2],
+                                                         ld, v.force.x, v.force.y, v.force.z);
+}
+
 int compute_force_impl(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist *nl, const double L[3],
-                       const rmpcd_lj *lj, double *energy, bool roll_flags)
+                       const rmpcd_lj *lj, double *energy, bool roll_flags, const ForceN2Branch *n2)
 {
     RMPCD_ARG(ps1 && ps2 && nl && L && lj, "null argument");
     RMPCD_ARG(ps1->precision == RMPCD_FP64, "compute_force: ps1 (colloids) must be FP64");
@@ -474,7 +493,9 @@ int compute_force_impl(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist *
     int *cn = nl->d_status + 16;
     int *clist = nl->d_status + 16 + 2 * nl->Npoints;
     double *e_out = (double *)ps1->d_sums;
-    RMPCD_CUDA_TRY(cudaMemsetAsync(max_contrib, 0, sizeof(int), s));
+    // k_apply_multi leaves max_contrib at zero and the scratch starts at zero,
+    // so the n_colloids loop (n2 given) skips this clear; other callers keep it
+    if (!n2) RMPCD_CUDA_TRY(cudaMemsetAsync(max_contrib, 0, sizeof(int), s));
     ps2->force_zero = false;
     ps1->force_zero = false;
     if (C > 0) {
@@ -493,6 +514,41 @@ int compute_force_impl(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist *
                                                       v.pos.z, v.species, v.flags, nl->list, nl->n, nl->Nmax, L[0],
                                                       L[1], L[2], ld, nl->pair_f, nl->pair_e, nl->contrib,
                                                       nl->ncontrib, max_contrib);
+        } else {
+            PView<double> v = cur<double>(ps2);
+            k_pair_forces<double><<<grid, 256, 0, s>>>(cv.pos.x, cv.pos.y, cv.pos.z, cv.species, v.pos.x, v.pos.y,
+                                                       v.pos.z, v.species, v.flags, nl->list, nl->n, nl->Nmax, L[0],
+                                                       L[1], L[2], ld, nl->pair_f, nl->pair_e, nl->contrib,
+                                                       nl->ncontrib, max_contrib);
+        }
+        // the colloid sums (and with n2 the colloid-colloid forces after them)
+        // only read the pair terms and write the colloid forces: with n2 they
+        // run on the second stream while the solvent forces are applied
+        const bool fork = n2 && !energy;
+        cudaStream_t sc = s;
+        if (fork) {
+            RMPCD_CUDA_TRY(cudaEventRecord(n2->ev_fork, s));
+            RMPCD_CUDA_TRY(cudaStreamWaitEvent(n2->side, n2->ev_fork, 0));
+            sc = n2->side;
+        }
+        // the colloid sums: list order in the FP64 form, the fixed tree in the
+        // FP32 form (whose energy still needs the compacted entries)
+        if (ps2->precision == RMPCD_FP32) {
+            k_colloid_tree<<<C, kNlBlockThreads, 0, sc>>>(nl->n, nl->Nmax, nl->contrib, nl->pair_f, cv.force.x,
+                                                          cv.force.y, cv.force.z);
+            if (energy)
+                k_colloid_sum<false><<<C, kNlThreads, 0, sc>>>(nl->n, nl->Nmax, nl->contrib, nl->pair_f, cv.force.x,
+                                                               cv.force.y, cv.force.z, clist, cn);
+        } else {
+            k_colloid_sum<true><<<C, kNlThreads, 0, sc>>>(nl->n, nl->Nmax, nl->contrib, nl->pair_f, cv.force.x,
+                                                          cv.force.y, cv.force.z, clist, cn);
+        }
+        if (fork) {
+            launch_force_n2(ps1, L, n2->lj_cc, sc);
+            RMPCD_CUDA_TRY(cudaEventRecord(n2->ev_join, sc));
+        }
+        if (ps2->precision == RMPCD_FP32) {
+            PView<float> v = cur<float>(ps2);
             k_apply_single<float><<<grid, 256, 0, s>>>(nl->list, nl->n, nl->Nmax, nl->contrib, nl->pair_f,
                                                        nl->ncontrib, v.force.x, v.force.y, v.force.z, nl->mkeys, m_count);
             k_apply_multi<float><<<1, 1024, 0, s>>>(nl->list, nl->n, C, nl->Nmax, nl->contrib, nl->pair_f,
@@ -500,30 +556,15 @@ int compute_force_impl(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist *
                                                    m_count);
         } else {
             PView<double> v = cur<double>(ps2);
-            k_pair_forces<double><<<grid, 256, 0, s>>>(cv.pos.x, cv.pos.y, cv.pos.z, cv.species, v.pos.x, v.pos.y,
-                                                       v.pos.z, v.species, v.flags, nl->list, nl->n, nl->Nmax, L[0],
-                                                       L[1], L[2], ld, nl->pair_f, nl->pair_e, nl->contrib,
-                                                       nl->ncontrib, max_contrib);
             k_apply_single<double><<<grid, 256, 0, s>>>(nl->list, nl->n, nl->Nmax, nl->contrib, nl->pair_f,
                                                         nl->ncontrib, v.force.x, v.force.y, v.force.z, nl->mkeys, m_count);
             k_apply_multi<double><<<1, 1024, 0, s>>>(nl->list, nl->n, C, nl->Nmax, nl->contrib, nl->pair_f,
                                                     nl->ncontrib, max_contrib, serial, v.force.x, v.force.y, v.force.z, nl->mkeys,
                                                    m_count);
         }
-        // the colloid sums: list order in the FP64 form, the fixed tree in the
-        // FP32 form (whose energy still needs the compacted entries)
-        if (ps2->precision == RMPCD_FP32) {
-            k_colloid_tree<<<C, kNlBlockThreads, 0, s>>>(nl->n, nl->Nmax, nl->contrib, nl->pair_f, cv.force.x,
-                                                         cv.force.y, cv.force.z);
-            if (energy)
-                k_colloid_sum<false><<<C, kNlThreads, 0, s>>>(nl->n, nl->Nmax, nl->contrib, nl->pair_f, cv.force.x,
-                                                              cv.force.y, cv.force.z, clist, cn);
-        } else {
-            k_colloid_sum<true><<<C, kNlThreads, 0, s>>>(nl->n, nl->Nmax, nl->contrib, nl->pair_f, cv.force.x,
-                                                         cv.force.y, cv.force.z, clist, cn);
-        }
         k_reset_contrib<<<grid, 256, 0, s>>>(nl->list, nl->n, nl->Nmax, nl->contrib, nl->ncontrib);
         if (energy) k_energy<<<1, 1024, 0, s>>>(cn, clist, C, nl->Nmax, nl->pair_e, nl->e_pre, e_out);
+        if (fork) RMPCD_CUDA_TRY(cudaStreamWaitEvent(s, n2->ev_join, 0));
         RMPCD_CHECK_LAUNCH();
     }
     if (energy) {
@@ -569,12 +610,7 @@ int rmpcd_compute_force_n2(rmpcd_particles *ps, const double L[3], const rmpcd_l
                                                 ps->n2_terms);
             k_energy_sum<<<1, 1024, 0, s>>>(ps->n2_terms, np, e_out);
         }
-        if (C <= 32)
-            k_force_n2<<<1, 32, 0, s>>>(v.pos.x, v.pos.y, v.pos.z, v.species, C, L[0], L[1], L[2], ld, v.force.x,
-                                        v.force.y, v.force.z);
-        else
-            k_force_n2_blocks<<<C, kNlBlockThreads, 0, s>>>(v.pos.x, v.pos.y, v.pos.z, v.species, C, L[0], L[1], L[2],
-                                                            ld, v.force.x, v.force.y, v.force.z);
+        launch_force_n2(ps, L, lj, s);
         RMPCD_CHECK_LAUNCH();
     }
     if (energy) {

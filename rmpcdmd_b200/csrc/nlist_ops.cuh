@@ -588,7 +588,9 @@ __device__ inline void colloid_tree_block(int i, const int *n, int Nmax, const u
 // compute_force_n2 for colloid m = blockIdx.x with the pair terms evaluated
 // by the whole block: term k (from colloid k != m) goes to shared memory in
 // chunks and thread 0 accumulates the chunk in k order, so the sum is the
-// sequential one of force_n2_one
+// sequential one of force_n2_one.  A term from k < m is stored negated
+// (a - f and a + (-f) round alike), so the chain is one add per interacting
+// colloid, with no branch between the loads of the next terms.
 __device__ inline void force_n2_block(int m, const double *px, const double *py, const double *pz, const int *sp,
                                       int C, double L0, double L1, double L2, const LJDev &lj, double *fx,
                                       double *fy, double *fz)
@@ -604,6 +606,7 @@ __device__ inline void force_n2_block(int m, const double *px, const double *py,
     for (int k0 = 0; k0 < C; k0 += kNlBlockThreads) {
         const int k = k0 + threadIdx.x;
         unsigned char h = 0;
+        double f0 = 0, f1 = 0, f2 = 0;
         if (k < C && k != m) {
             int i = k < m ? k : m, j = k < m ? m : k;
             double d0 = min_image_d(px[i] - px[j], L0);
@@ -614,26 +617,31 @@ __device__ inline void force_n2_block(int m, const double *px, const double *py,
             if (r_sq <= lj.cut_sq[(s1 - 1) + lj.n1 * (s2 - 1)]) {
                 int tt = (s2 - 1) + lj.n1 * (s1 - 1);
                 double fr = lj_force_over_r(r_sq, lj.epsilon[tt], lj.sigma[tt]);
-                term[0][threadIdx.x] = fr * d0;
-                term[1][threadIdx.x] = fr * d1;
-                term[2][threadIdx.x] = fr * d2;
-                h = k < m ? 1 : 2;
+                f0 = fr * d0;
+                f1 = fr * d1;
+                f2 = fr * d2;
+                if (k < m) {
+                    f0 = -f0;
+                    f1 = -f1;
+                    f2 = -f2;
+                }
+                h = 1;
             }
         }
+        term[0][threadIdx.x] = f0;
+        term[1][threadIdx.x] = f1;
+        term[2][threadIdx.x] = f2;
         has[threadIdx.x] = h;
         __syncthreads();
         if (threadIdx.x == 0) {
             const int n = min(kNlBlockThreads, C - k0);
+#pragma unroll 8
             for (int q = 0; q < n; q++) {
-                if (has[q] == 1) {
-                    a0 = a0 - term[0][q];
-                    a1 = a1 - term[1][q];
-                    a2 = a2 - term[2][q];
-                } else if (has[q] == 2) {
-                    a0 = a0 + term[0][q];
-                    a1 = a1 + term[1][q];
-                    a2 = a2 + term[2][q];
-                }
+                const bool on = has[q] != 0;
+                const double u0 = term[0][q], u1 = term[1][q], u2 = term[2][q];
+                a0 = on ? a0 + u0 : a0;
+                a1 = on ? a1 + u1 : a1;
+                a2 = on ? a2 + u2 : a2;
             }
         }
         __syncthreads();

@@ -49,10 +49,20 @@ void launch_segsort_big(const int *start, const int *count, const int *big, cons
 // particles of is_md cells (src/particle_system.f90:357-410)
 int launch_max_disp(rmpcd_particles *p);
 int launch_cell_max_disp(rmpcd_cells *c, rmpcd_particles *p);
+// compute_force_n2 of the colloids run right after compute_force, with the
+// colloid sums, on a second stream beside the solvent force application
+// (the two branches write disjoint arrays; each array sees the arithmetic
+// of the two calls in sequence)
+struct ForceN2Branch {
+    const rmpcd_lj *lj_cc;      // colloid-colloid parameters of compute_force_n2
+    cudaStream_t side;
+    cudaEvent_t ev_fork, ev_join;
+};
 // compute_force (src/neighbor_list.f90:159-225); roll_flags = false leaves
-// the PAST_MD/MD roll to the caller (which must then have done it)
+// the PAST_MD/MD roll to the caller (which must then have done it).  n2 (no
+// energy only): also compute_force_n2 of ps1, as above.
 int compute_force_impl(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist *nl, const double L[3],
-                       const rmpcd_lj *lj, double *energy, bool roll_flags);
+                       const rmpcd_lj *lj, double *energy, bool roll_flags, const ForceN2Branch *n2 = nullptr);
 // largest cell handled by sort_segment; larger ones go to launch_segsort_big
 constexpr int kSmallSegmentMax = 64;
 

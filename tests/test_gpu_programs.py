@@ -175,6 +175,49 @@ def test_bulk_shapes_give_identical_results(rm, oracle, precision):
         rm.set_bulk_shape(precision, keep)
 
 
+def test_n_colloids_native_loop_kept_between_calls(rm):
+    """rmpcd_ncolloids_run keeps its scratch and captured MD-step graphs for
+    the next call on the same systems and parameters, and rebuilds them when
+    the systems change: calls alternating between two systems (and a change
+    of skin) give the states of the same calls made without alternation, and
+    of the same calls with graphs off."""
+    from rmpcdmd_b200._capi import call
+    from rmpcdmd_b200.programs import NColloidsPBC
+
+    def make(seed):
+        return NColloidsPBC(L=(20, 20, 20), rho=10, N_MD=10, N_colloids=6, seed=seed, precision=32)
+
+    a, b, a_ref, b_ref, a_off = make(3), make(4), make(3), make(4), make(3)
+    for k in range(3):
+        a.thermalise(1)
+        b.thermalise(1)
+        if k == 1:
+            a.skin = b.skin = 0.9 * a.skin
+    for k in range(3):
+        a_ref.thermalise(1)
+        if k == 1:
+            a_ref.skin = 0.9 * a_ref.skin
+    for k in range(3):
+        b_ref.thermalise(1)
+        if k == 1:
+            b_ref.skin = 0.9 * b_ref.skin
+    call("rmpcd_ncolloids_set_graphs", 0)
+    try:
+        for k in range(3):
+            a_off.thermalise(1)
+            if k == 1:
+                a_off.skin = 0.9 * a_off.skin
+    finally:
+        call("rmpcd_ncolloids_set_graphs", 1)
+    for x, y in ((a, a_ref), (b, b_ref), (a, a_off)):
+        for f in ("pos", "vel", "image", "id", "flags", "force", "force_old"):
+            assert np.array_equal(x.solvent.download(f), y.solvent.download(f)), f
+        for f in ("pos", "vel", "force"):
+            assert np.array_equal(x.colloids.download(f), y.colloids.download(f)), f
+        assert x.n_extra_sorting == y.n_extra_sorting
+    assert a.n_extra_sorting > 0
+
+
 @pytest.mark.parametrize("precision,graphs", [(64, True), (32, True), (64, False)])
 def test_n_colloids_native_loop_matches_call_by_call(rm, precision, graphs):
     """rmpcd_ncolloids_run issues the program's calls in C; the state after
