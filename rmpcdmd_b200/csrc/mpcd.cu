@@ -22,6 +22,116 @@ __global__ void k_simple_mpcd(const int *__restrict__ count, const int *__restri
         srd_slot<R>(count[s], start[s], s, 0, vx, vy, vz, species, q);
 }
 
+// The MPC-AT normals of simple_mpcd_step (src/mpcd.f90:144-160): for every
+// particle i with species > 0, (R)(rng::normal(seed, step, i, k) * t_factor)
+// for k = 0, 1, 2 into n[k][i].  Each deviate is the first accepted of the
+// attempts t = 0, 1, ... of rng::normal, so the values are rng::normal's.  A
+// warp's 32 particles (96 deviates) share its lanes: every lane tries one
+// attempt per round, and a rejected attempt queues the deviate's next attempt
+// for a later round, so no lane waits while another repeats a rejection (a
+// deviate drawn by one thread costs its warp the slowest lane's attempts).
+constexpr int kAtThreads = 256;
+constexpr int kAtJobs = 96;  // deviates of one warp: 32 particles x 3
+
+__device__ inline unsigned short at_job(int p, int k, int t) { return (unsigned short)(p | (k << 5) | (t << 7)); }
+
+template <typename R>
+__global__ void __launch_bounds__(kAtThreads) k_at_normals(const int *__restrict__ species, long long N, SrdParams q,
+                                                           R *nx, R *ny, R *nz)
+{
+    __shared__ unsigned short jobs[kAtThreads / 32][2][kAtJobs];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned below = lanemask_lt();
+    R *out[3] = {nx, ny, nz};
+    const long long warps = (long long)gridDim.x * (kAtThreads / 32);
+    for (long long base = ((long long)blockIdx.x * (kAtThreads / 32) + w) * 32; base < N; base += warps * 32) {
+        unsigned short *cur = jobs[w][0], *next = jobs[w][1];
+        // round 0: every lane the attempt 0 of its own particle's deviates
+        const long long i = base + lane;
+        const bool act = i < N && species[i] > 0;
+        int nq = 0;
+        for (int k = 0; k < 3; k++) {
+            double z = 0;
+            const bool ok = act && rng::normal_attempt(q.seed, q.step, (uint32_t)i, (uint32_t)k, 0u, &z);
+            if (ok) out[k][i] = (R)(z * q.t_factor);
+            const unsigned rej = __ballot_sync(0xffffffffu, act && !ok);
+            if (act && !ok) cur[nq + __popc(rej & below)] = at_job(lane, k, 1);
+            nq += __popc(rej);
+        }
+        __syncwarp();
+        // later rounds: the queued attempts, 32 at a time
+        while (nq > 0) {
+            int nn = 0;
+            for (int j0 = 0; j0 < nq; j0 += 32) {
+                const bool have = j0 + lane < nq;
+                const unsigned jb = have ? cur[j0 + lane] : 0u;
+                const int p = jb & 31, k = (jb >> 5) & 3, t = (int)(jb >> 7);
+                const long long ii = base + p;
+                double z = 0;
+                bool ok = false;
+                if (have) {
+                    // rng::normal gives 0 once its attempts are spent
+                    ok = t >= (int)rng::kNormalAttempts ||
+                         rng::normal_attempt(q.seed, q.step, (uint32_t)ii, (uint32_t)k, (uint32_t)t, &z);
+                    if (ok) out[k][ii] = (R)(z * q.t_factor);
+                }
+                const unsigned rej = __ballot_sync(0xffffffffu, have && !ok);
+                if (have && !ok) next[nn + __popc(rej & below)] = at_job(p, k, t + 1);
+                nn += __popc(rej);
+            }
+            __syncwarp();
+            unsigned short *tmp = cur;
+            cur = next;
+            next = tmp;
+            nq = nn;
+        }
+    }
+}
+
+// simple_mpcd_step with the MPC-AT thermostat given the normals of
+// k_at_normals: the thermostat branch of srd_slot (src/mpcd.f90:126-160) with
+// each normal read instead of drawn; vel = normal + dv (hydro) or the normal,
+// as srd_slot's store and later add.
+template <typename R>
+__global__ void k_at_cells(const int *__restrict__ count, const int *__restrict__ start, int S, R *vx, R *vy, R *vz,
+                           const int *__restrict__ species, int hydro, const R *__restrict__ nx,
+                           const R *__restrict__ ny, const R *__restrict__ nz)
+{
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
+        const int n = count[s];
+        if (n <= 1) continue;
+        const long long a = start[s];
+        int n_eff = 0;
+        CellSum<R> sx, sy, sz, wx, wy, wz;
+        for (long long i = a; i < a + n; i++) {
+            if (species[i] > 0) {
+                sx.add(vx[i]);
+                sy.add(vy[i]);
+                sz.add(vz[i]);
+                wx.add(nx[i]);
+                wy.add(ny[i]);
+                wz.add(nz[i]);
+                n_eff++;
+            }
+        }
+        if (n_eff <= 1) continue;
+        const R lv[3] = {sx.value() / n_eff, sy.value() / n_eff, sz.value() / n_eff};
+        const R dv[3] = {lv[0] - wx.value() / n_eff, lv[1] - wy.value() / n_eff, lv[2] - wz.value() / n_eff};
+        for (long long i = a; i < a + n; i++) {
+            if (species[i] <= 0) continue;
+            if (hydro) {
+                vx[i] = nx[i] + dv[0];
+                vy[i] = ny[i] + dv[1];
+                vz[i] = nz[i] + dv[2];
+            } else {
+                vx[i] = nx[i];
+                vy[i] = ny[i];
+                vz[i] = nz[i];
+            }
+        }
+    }
+}
+
 // wall_mpcd_step, src/mpcd.f90:193-337
 template <typename R>
 __global__ void k_wall_mpcd(const int *__restrict__ count, const int *__restrict__ start, int S,
@@ -467,11 +577,26 @@ int rmpcd_simple_mpcd_step(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r, int
     SrdParams q = srd_params(p, c, r, has_alpha, alpha, thermostat, T, hydro);
     cudaStream_t s = stream();
     int g = grid_full(c->S, 128);
-    DISPATCH_R(p,
-               ({ PView<float> v = cur<float>(p);
-                  k_simple_mpcd<float><<<g, 128, 0, s>>>(c->count, c->start, c->S, v.vel.x, v.vel.y, v.vel.z, v.species, q); }),
-               ({ PView<double> v = cur<double>(p);
-                  k_simple_mpcd<double><<<g, 128, 0, s>>>(c->count, c->start, c->S, v.vel.x, v.vel.y, v.vel.z, v.species, q); }));
+    if (thermostat && !q.gauss && p->N > 0) {
+        // the normals first, into the sort target's velocity arrays (free
+        // between sorts), then the cells
+        const int gn = grid_full(((long long)p->N + 31) / 32 * 32, kAtThreads);
+        DISPATCH_R(p,
+                   ({ PView<float> v = cur<float>(p), t = alt<float>(p);
+                      k_at_normals<float><<<gn, kAtThreads, 0, s>>>(v.species, p->N, q, t.vel.x, t.vel.y, t.vel.z);
+                      k_at_cells<float><<<g, 128, 0, s>>>(c->count, c->start, c->S, v.vel.x, v.vel.y, v.vel.z,
+                                                          v.species, q.hydro, t.vel.x, t.vel.y, t.vel.z); }),
+                   ({ PView<double> v = cur<double>(p), t = alt<double>(p);
+                      k_at_normals<double><<<gn, kAtThreads, 0, s>>>(v.species, p->N, q, t.vel.x, t.vel.y, t.vel.z);
+                      k_at_cells<double><<<g, 128, 0, s>>>(c->count, c->start, c->S, v.vel.x, v.vel.y, v.vel.z,
+                                                           v.species, q.hydro, t.vel.x, t.vel.y, t.vel.z); }));
+    } else {
+        DISPATCH_R(p,
+                   ({ PView<float> v = cur<float>(p);
+                      k_simple_mpcd<float><<<g, 128, 0, s>>>(c->count, c->start, c->S, v.vel.x, v.vel.y, v.vel.z, v.species, q); }),
+                   ({ PView<double> v = cur<double>(p);
+                      k_simple_mpcd<double><<<g, 128, 0, s>>>(c->count, c->start, c->S, v.vel.x, v.vel.y, v.vel.z, v.species, q); }));
+    }
     RMPCD_CHECK_LAUNCH();
     r->step++;
     return RMPCD_OK;

@@ -303,7 +303,7 @@ __global__ void k_roll_clear(int *flags, Vec3<R> force, long long N, Vec3<double
 // the last sort (delta_t = dt * ctl[0]), ctl[1] receives the decision.  The
 // maxima are the squared displacements taken by the MD step's position pass
 // (solvent, floored at max_v * delta_t) and of the colloids.
-__device__ inline void nc_resort_test(unsigned long long *so_bits, double co_sq, int *ctl, double dt,
+__device__ inline void nc_resort_test(unsigned long long *so_bits, double co_sq, int *ctl, int *h_ctl, double dt,
                                       double max_v, double skin)
 {
     const int n = ctl[0] + 1;
@@ -313,7 +313,12 @@ __device__ inline void nc_resort_test(unsigned long long *so_bits, double co_sq,
     const double b = __dmul_rn(max_v, delta_t);
     const double so_max = a > b ? a : b;
     const double co_max = sqrt(co_sq);
-    ctl[1] = (co_max >= __dmul_rn(skin, 0.1)) || (so_max >= __dmul_rn(skin, 0.9)) ? 1 : 0;
+    const int resort = (co_max >= __dmul_rn(skin, 0.1)) || (so_max >= __dmul_rn(skin, 0.9)) ? 1 : 0;
+    ctl[1] = resort;
+    // the host's copy (page-locked, mapped): read once the stream has passed
+    // this kernel
+    ((volatile int *)h_ctl)[1] = resort;
+    __threadfence_system();
     *so_bits = 0;  // cleared for the next MD step's position pass
 }
 
@@ -329,7 +334,7 @@ constexpr int kNcColloidThreads = 256;
 template <bool kVel>
 __global__ void __launch_bounds__(kNcColloidThreads)
     k_nc_colloid_begin(PView<double> c, Vec3<double> c_old, const double *mass, double dt,
-                       unsigned long long *so_bits, int *ctl, double max_v, double skin)
+                       unsigned long long *so_bits, int *ctl, int *h_ctl, double max_v, double skin)
 {
     __shared__ double s_m[kNcColloidThreads / 32];
     double m = 0;
@@ -344,7 +349,7 @@ __global__ void __launch_bounds__(kNcColloidThreads)
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int w = 1; w < kNcColloidThreads / 32; w++) m = m > s_m[w] ? m : s_m[w];
-        nc_resort_test(so_bits, m, ctl, dt, max_v, skin);
+        nc_resort_test(so_bits, m, ctl, h_ctl, dt, max_v, skin);
     }
 }
 
@@ -376,7 +381,8 @@ struct NcLoop {
     int *n_md = nullptr;     // their number (device)
     int *ctl = nullptr;      // device: MD steps since the last sort, re-sort decision
     double *d_mass = nullptr;  // velocity-Verlet masses of the colloids (device)
-    int *h_ctl = nullptr;    // page-locked landing of ctl
+    int *h_ctl = nullptr;    // page-locked, device-mapped copy of the decision (written by the kernel)
+    int *h_ctl_dev = nullptr;  // its device address
     cudaEvent_t ev_a = nullptr;  // end of the MD step's part up to the re-sort test
     // second stream of the force evaluation (colloid sums and colloid-colloid
     // forces beside the solvent force application)
@@ -494,7 +500,8 @@ static int nc_alloc(NcLoop &L, int S, int N, int C)
         cudaMalloc(&L.cellmap, (size_t)(N > 0 ? N : 1) * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&L.ctl, 2 * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&L.d_mass, (size_t)(C > 0 ? C : 1) * sizeof(double)) != cudaSuccess ||
-        cudaHostAlloc(&L.h_ctl, 2 * sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
+        cudaHostAlloc(&L.h_ctl, 2 * sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer(&L.h_ctl_dev, L.h_ctl, 0) != cudaSuccess ||
         cudaEventCreateWithFlags(&L.ev_a, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&L.ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&L.ev_join, cudaEventDisableTiming) != cudaSuccess ||
@@ -624,8 +631,8 @@ static int md_cells_copy_pos_t(NcLoop &L)
 #define NC_DISPATCH(L, fn) ((L).s->precision == RMPCD_FP32 ? fn<float>(L) : fn<double>(L))
 
 // the colloid part of the MD step and the re-sort test (the solvent's
-// maximum displacement over the MD cells was taken with its positions), and
-// the decision copied to the host
+// maximum displacement over the MD cells was taken with its positions), whose
+// kernel also writes the decision to the host
 static int colloid_begin(NcLoop &L, bool vel_due)
 {
     cudaStream_t st = stream();
@@ -633,12 +640,11 @@ static int colloid_begin(NcLoop &L, bool vel_due)
     const Vec3<double> c_old = alt<double>(L.c).pos;
     if (vel_due)
         k_nc_colloid_begin<true><<<1, kNcColloidThreads, 0, st>>>(c, c_old, L.d_mass, L.dt, L.s->d_max, L.ctl,
-                                                                  L.cells->max_v, L.prm->skin);
+                                                                  L.h_ctl_dev, L.cells->max_v, L.prm->skin);
     else
         k_nc_colloid_begin<false><<<1, kNcColloidThreads, 0, st>>>(c, c_old, L.d_mass, L.dt, L.s->d_max, L.ctl,
-                                                                   L.cells->max_v, L.prm->skin);
+                                                                   L.h_ctl_dev, L.cells->max_v, L.prm->skin);
     RMPCD_CHECK_LAUNCH();
-    RMPCD_CUDA_TRY(cudaMemcpyAsync(L.h_ctl, L.ctl, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     return RMPCD_OK;
 }
 

@@ -107,24 +107,39 @@ __host__ __device__ inline void sphere(uint64_t seed, uint64_t step, uint32_t in
     n2 = 1.0;
 }
 
-// Standard normal deviate by Leva's ratio-of-uniforms method (J. L. Leva,
-// "A fast normal random number generator", ACM TOMS 18(4):449-453, 1992).
-// The quadratic bounds decide almost every draw without a logarithm and the
-// returned value v/u is plain arithmetic, so host and device agree.
+// Attempt t of a standard normal deviate by Leva's ratio-of-uniforms method
+// (J. L. Leva, "A fast normal random number generator", ACM TOMS
+// 18(4):449-453, 1992): true, with the deviate in *out, when the attempt is
+// accepted.  The quadratic bounds decide almost every attempt without a
+// logarithm and the returned value v/u is plain arithmetic, so host and
+// device agree.
+__host__ __device__ inline bool normal_attempt(uint64_t seed, uint64_t step, uint32_t index, uint32_t sub,
+                                               uint32_t t, double *out)
+{
+    double w0, w1;
+    uniform2(seed, step, index, GAUSS, (sub << 16) | t, w0, w1);
+    double u = 1.0 - w0;
+    double v = 1.7156 * (w1 - 0.5);
+    double x = u - 0.449871;
+    double y = fabs(v) + 0.386595;
+    double q = x * x + y * (0.19600 * y - 0.25472 * x);
+    if (q < 0.27597 || (q <= 0.27846 && v * v <= -4.0 * log(u) * u * u)) {
+        *out = v / u;
+        return true;
+    }
+    return false;
+}
+
+// attempts allowed per deviate; after them the deviate is 0
+constexpr uint32_t kNormalAttempts = 256u;
+
+// The first accepted of attempts 0, 1, ... (0.0 if none of kNormalAttempts is)
 __host__ __device__ inline double normal(uint64_t seed, uint64_t step, uint32_t index,
                                          uint32_t sub)
 {
-    for (uint32_t t = 0; t < 256u; t++) {
-        double w0, w1;
-        uniform2(seed, step, index, GAUSS, (sub << 16) | t, w0, w1);
-        double u = 1.0 - w0;
-        double v = 1.7156 * (w1 - 0.5);
-        double x = u - 0.449871;
-        double y = fabs(v) + 0.386595;
-        double q = x * x + y * (0.19600 * y - 0.25472 * x);
-        if (q < 0.27597) return v / u;
-        if (q > 0.27846) continue;
-        if (v * v <= -4.0 * log(u) * u * u) return v / u;
+    for (uint32_t t = 0; t < kNormalAttempts; t++) {
+        double z;
+        if (normal_attempt(seed, step, index, sub, t, &z)) return z;
     }
     return 0.0;
 }

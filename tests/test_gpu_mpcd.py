@@ -61,6 +61,25 @@ def test_simple_mpcd_step_thermostat(rm, oracle, hydro):
     assert_same(gp, op, ("vel",))
 
 
+@pytest.mark.parametrize("hydro", [True, False])
+def test_simple_mpcd_step_thermostat_fp32_draws(rm, oracle, hydro):
+    """FP32 MPC-AT: the normals drawn on the device (the attempts of a warp's
+    deviates shared by its lanes) give the velocities of the same deviates,
+    computed by the oracle's generator, injected into the per-cell path."""
+    L, N = [8, 8, 8], 5120
+    sp = species_mix(N, 5)
+    _, (gc, gp) = make_pair(rm, oracle, L, N, seed=6, species=sp, precision=32)
+    _, (gc2, gp2) = make_pair(rm, oracle, L, N, seed=6, species=sp, precision=32)
+    seed, step = 5, 4
+    g = np.array([[oracle.normal(seed, step, i, k) for k in range(3)] for i in range(N)])
+    gp2.set_gauss(g)
+    rm.simple_mpcd_step(gp, gc, rm.Rng(seed, step), thermostat=True, T=0.5, hydro=hydro)
+    rm.simple_mpcd_step(gp2, gc2, rm.Rng(seed, step), thermostat=True, T=0.5, hydro=hydro)
+    v, v2 = gp.download("vel"), gp2.download("vel")
+    assert np.array_equal(v, v2)
+    assert not np.array_equal(v, make_pair(rm, oracle, L, N, seed=6, species=sp, precision=32)[1][1].download("vel"))
+
+
 def test_thermostat_stop_conditions(rm, oracle):
     (oc, op), (gc, gp) = make_pair(rm, oracle, [4, 4, 4], 640, seed=1)
     with pytest.raises(rm.RmpcdError):
