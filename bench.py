@@ -739,9 +739,14 @@ def profile_dimer(args):
 def profile_ncolloids(args):
     """A fixed n_colloids_pbc workload for profilers: 128^3, rho = 10,
     args.profile_ncolloids colloids, FP32 solvent, one thermostatted interval
-    of the native loop (rmpcd_ncolloids_run) after one warm-up interval."""
+    of the native loop (rmpcd_ncolloids_run) after one warm-up interval, with
+    its MD steps launched one by one (kernel profilers do not see into the
+    conditional nodes of the replayed graphs)."""
     import rmpcdmd_b200 as rm
+    from rmpcdmd_b200._capi import call
     from rmpcdmd_b200.programs import NColloidsPBC
+
+    call("rmpcd_ncolloids_set_graphs", 0)
 
     g = NColloidsPBC(L=(128, 128, 128), rho=RHO, N_MD=DIMER_N_MD, N_colloids=args.profile_ncolloids, seed=SEED,
                      volume_correction=False, precision=32)
@@ -749,6 +754,83 @@ def profile_ncolloids(args):
     g._native(1, True, [g.T_init], 10)
     rm.synchronize()
     print(f"profile_ncolloids: {args.profile_ncolloids} colloids, {g.N} particles, 2 intervals")
+
+
+def kernel_timeline(run, label):
+    """The kernels `run()` puts on the GPU, with their device start and end
+    times as CUPTI records them (through torch.profiler), so concurrent and
+    graph-launched kernels appear with their real, warm-cache durations:
+    prints the span of the run, the time at least one kernel or copy was
+    busy, and per kernel its launches, total and share of the busy time."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    torch.zeros(1, device="cuda")
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        run()
+    rows = sorted((e.start_ns(), e.duration_ns(), e.name()) for e in prof.profiler.kineto_results.events()
+                  if e.device_type().name == "CUDA")
+    if not rows:
+        print(f"{label}: no device activity recorded")
+        return
+    t0, busy = rows[0][0], 0
+    s0, e0 = rows[0][0], rows[0][0] + rows[0][1]
+    for st, d, _ in rows[1:]:
+        if st > e0:
+            busy += e0 - s0
+            s0, e0 = st, st + d
+        else:
+            e0 = max(e0, st + d)
+    busy += e0 - s0
+    span = max(st + d for st, d, _ in rows) - t0
+    agg = {}
+    for _, d, n in rows:
+        k = n.split("(")[0]
+        c, t = agg.get(k, (0, 0))
+        agg[k] = (c + 1, t + d)
+    print(f"{label}: span {span / 1e3:.1f} us, busy {busy / 1e3:.1f} us, {len(rows)} kernels and copies")
+    print("| kernel | launches | total us | share of busy |")
+    print("|---|---|---|---|")
+    for k, (c, t) in sorted(agg.items(), key=lambda kv: -kv[1][1]):
+        print(f"| {k} | {c} | {t / 1e3:.1f} | {100 * t / busy:.1f} % |")
+
+
+def timeline(args):
+    """One interval of n_colloids_pbc (128^3, 200 colloids, thermostatted,
+    after two warm-up intervals) or of one 32^3 single dimer (batched engine,
+    graph on, after autotuning and warm-up), FP32 solvent, through
+    kernel_timeline."""
+    import rmpcdmd_b200 as rm
+
+    if args.timeline == "ncolloids":
+        from rmpcdmd_b200.programs import NColloidsPBC
+
+        g = NColloidsPBC(L=(128, 128, 128), rho=RHO, N_MD=DIMER_N_MD, N_colloids=200, seed=SEED,
+                         volume_correction=False, precision=32)
+        g.thermalise(1)
+        g.thermalise(1)
+        rm.synchronize()
+
+        def run():
+            g.thermalise(1)
+            rm.synchronize()
+
+        kernel_timeline(run, "n_colloids 128^3, 200 colloids, FP32, one thermostatted interval (100 MD steps)")
+    else:
+        from rmpcdmd_b200.programs import DimerBatch, SingleDimerPBC
+
+        d = [SingleDimerPBC(L=(32, 32, 32), rho=RHO, N_MD=DIMER_N_MD, seed=SEED, list_capacity=DIMER_LIST_CAPACITY,
+                            precision=32)]
+        b = DimerBatch(d, use_graph=True)
+        b.autotune(1)
+        b.run(2)
+        rm.synchronize()
+
+        def run():
+            b.run(1)
+            rm.synchronize()
+
+        kernel_timeline(run, "single dimer 32^3, FP32 solvent, engine with its interval graph, one interval")
 
 
 def main(argv=None):
@@ -771,12 +853,16 @@ def main(argv=None):
                     help="with --profile-dimer: every replica in an L^3 box instead of the drawn sides")
     ap.add_argument("--cpu-table", action="store_true",
                     help="only time the CPU restatement on samples of every configuration (baseline table)")
+    ap.add_argument("--timeline", choices=["ncolloids", "dimer32"], default=None,
+                    help="only print the kernel timeline of one interval of the named workload")
     ap.add_argument("--profile-dimer", type=int, default=0, metavar="R",
                     help="only run one interval of R batched dimer replicas (graph off), for profilers")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
-    if args.cpu_table:
+    if args.timeline:
+        timeline(args)
+    elif args.cpu_table:
         cpu_table(args)
     elif args.profile_dimer:
         profile_dimer(args)

@@ -315,10 +315,9 @@ __device__ inline void nc_resort_test(unsigned long long *so_bits, double co_sq,
     const double co_max = sqrt(co_sq);
     const int resort = (co_max >= __dmul_rn(skin, 0.1)) || (so_max >= __dmul_rn(skin, 0.9)) ? 1 : 0;
     ctl[1] = resort;
-    // the host's copy (page-locked, mapped): read once the stream has passed
-    // this kernel
+    // the host's copy (page-locked, mapped): read after an event or stream
+    // synchronisation past this kernel, which orders it for the host
     ((volatile int *)h_ctl)[1] = resort;
-    __threadfence_system();
     *so_bits = 0;  // cleared for the next MD step's position pass
 }
 
