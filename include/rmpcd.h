@@ -408,8 +408,13 @@ int rmpcd_bulk_autotune(const int L[3], int precision, double tau, int n_interva
  * rescale_every (> 0), rescale_cells(T_rescale).  The calls and their order
  * are those of the program, so the results equal the same calls made one by
  * one; the loop state (MD step counters, re-sort count, the energies e1, e2
- * of each interval's last MD step) is carried in *state.  No module
- * counterpart in the reference. */
+ * of each interval's last MD step) is carried in *state.  The call keeps its
+ * scratch (about 4 B per slot and 4 B per solvent particle) and its captured
+ * MD-step graphs for the next call, and reuses them while the handles, their
+ * device arrays, the box, the LJ tables and tau, N_MD and skin are the same;
+ * other arguments make it rebuild them.  A call made while another thread is
+ * inside this function works with scratch of its own.  No module counterpart
+ * in the reference. */
 typedef struct rmpcd_ncolloids_params {
     double tau;          /* dt = tau / N_MD */
     int N_MD;
