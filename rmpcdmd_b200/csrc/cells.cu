@@ -112,6 +112,7 @@ int rmpcd_cells_init(rmpcd_cells **out, const int L[3], double a, int has_walls)
 int rmpcd_cells_destroy(rmpcd_cells *c)
 {
     if (!c) return RMPCD_OK;
+    ncolloids_forget(c);
     cudaStreamSynchronize(stream());
     free_cells(c);
     return RMPCD_OK;

@@ -877,6 +877,21 @@ static bool g_nc_graphs = true;
 static std::mutex g_nc_mutex;
 static NcLoop *g_nc_loop = nullptr;
 
+namespace rmpcd {
+
+void ncolloids_forget(const void *handle)
+{
+    std::lock_guard<std::mutex> lk(g_nc_mutex);
+    NcLoop *L = g_nc_loop;
+    if (L && (handle == L->s || handle == L->c || handle == L->cells || handle == L->nl)) {
+        cudaStreamSynchronize(stream());
+        delete L;
+        g_nc_loop = nullptr;
+    }
+}
+
+}  // namespace rmpcd
+
 extern "C" int rmpcd_ncolloids_set_graphs(int on)
 {
     g_nc_graphs = on != 0;

@@ -337,6 +337,7 @@ int rmpcd_nlist_init(rmpcd_nlist **out, int Npoints, int Nmax)
 int rmpcd_nlist_destroy(rmpcd_nlist *nl)
 {
     if (!nl) return RMPCD_OK;
+    ncolloids_forget(nl);
     cudaStreamSynchronize(stream());
     cudaFree(nl->list);
     cudaFree(nl->n);

@@ -397,6 +397,7 @@ int rmpcd_particles_init(rmpcd_particles **out, int Nmax, int n_species, const d
 int rmpcd_particles_destroy(rmpcd_particles *p)
 {
     if (!p) return RMPCD_OK;
+    ncolloids_forget(p);
     cudaStreamSynchronize(stream());
     free_particles(p);
     return RMPCD_OK;

@@ -63,6 +63,9 @@ struct ForceN2Branch {
 // energy only): also compute_force_n2 of ps1, as above.
 int compute_force_impl(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist *nl, const double L[3],
                        const rmpcd_lj *lj, double *energy, bool roll_flags, const ForceN2Branch *n2 = nullptr);
+// drops the n_colloids loop kept between calls if it refers to `handle` (a
+// particle system, cell system or neighbor list being destroyed)
+void ncolloids_forget(const void *handle);
 // largest cell handled by sort_segment; larger ones go to launch_segsort_big
 constexpr int kSmallSegmentMax = 64;
 
