@@ -714,8 +714,9 @@ static int issue_part_b(NcLoop &L, double *e1, double *e2)
 // part_b behind an IF node that runs it only when the MD step's re-sort test
 // (already queued) said no: captured once per key into a graph made of
 // k_nc_set_cond and the IF node, whose body is captured from issue_part_b.
-// Returns RMPCD_ERR_CUDA, with the stream out of capture, when the graph cannot
-// be built; the caller then issues the step without speculation.
+// Returns RMPCD_ERR_CUDA, with the stream out of capture and no error message
+// recorded, when the graph cannot be built; the caller then issues the step
+// without speculation.
 static int replay_spec(NcLoop &L, const NcLoop::Key &key)
 {
     cudaStream_t st = stream();
@@ -757,7 +758,7 @@ static int replay_spec(NcLoop &L, const NcLoop::Key &key)
         if (g) cudaGraphDestroy(g);
         if (e != cudaSuccess || rc) {
             cudaGetLastError();
-            return fail(RMPCD_ERR_CUDA, "n_colloids speculative step: %s", cudaGetErrorString(e));
+            return RMPCD_ERR_CUDA;
         }
         it = L.part_bs.emplace(key, x).first;
     }
