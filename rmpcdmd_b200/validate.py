@@ -14,7 +14,8 @@ the same seeds:
   bond direction (catalytic minus noncatalytic bead), averaged over an
   ensemble of replicas run by the batched engine, with its standard error.
 
-``python -m rmpcdmd_b200.validate [--quick]`` prints one JSON object.
+``python -m rmpcdmd_b200.validate [--quick | --bulk L INTERVALS]`` prints one
+JSON object.
 """
 from __future__ import annotations
 
@@ -43,8 +44,15 @@ def _bulk(L, precision, seed, n_intervals):
     rng = A.Rng(seed)
     cells.random_shift(rng)
     p.sort(cells)
-    order = np.argsort(p.download("id"))
-    v0 = p.download("vel")[order]
+    def by_id():
+        # velocities in particle-id order (ids are a permutation of a
+        # contiguous range): one scatter instead of a sort
+        ids, v = p.download("id"), p.download("vel")
+        out = np.empty_like(v)
+        out[ids - ids.min()] = v
+        return out
+
+    v0 = by_id()
     norm = float((v0 * v0).sum())
     mom, temp, vacf, ekin = [], [], [1.0], []
     s = A.velocity_sums(p)
@@ -56,8 +64,7 @@ def _bulk(L, precision, seed, n_intervals):
         mom.append(s[1:].copy())
         ekin.append(s[0] / 2)
         temp.append(A.compute_temperature(p, cells))
-        v = p.download("vel")[np.argsort(p.download("id"))]
-        vacf.append(float((v0 * v).sum()) / norm)
+        vacf.append(float((v0 * by_id()).sum()) / norm)
     mom = np.array(mom)
     scale = N * np.sqrt(KT)
     step_drift = np.abs(np.diff(mom, axis=0)).max() / scale
@@ -183,9 +190,13 @@ def paired_propulsion_check(L=16, replicas=8, n_intervals=40, skip=3, seed0=2000
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--quick", action="store_true", help="small sizes (a minute)")
+    ap.add_argument("--bulk", type=int, nargs=2, metavar=("L", "INTERVALS"),
+                    help="only the bulk check, on an L^3 box for INTERVALS intervals")
     a = ap.parse_args(argv)
     t0 = time.perf_counter()
-    if a.quick:
+    if a.bulk:
+        out = dict(bulk=bulk_check(L=a.bulk[0], n_intervals=a.bulk[1]))
+    elif a.quick:
         out = dict(bulk=bulk_check(L=24, n_intervals=20),
                    propulsion=propulsion_check(L=16, replicas=16, n_intervals=30, skip=5),
                    paired=paired_propulsion_check(L=16, replicas=8, n_intervals=20, skip=3))
