@@ -14,8 +14,8 @@ the same seeds:
   bond direction (catalytic minus noncatalytic bead), averaged over an
   ensemble of replicas run by the batched engine, with its standard error.
 
-``python -m rmpcdmd_b200.validate [--quick | --bulk L INTERVALS]`` prints one
-JSON object.
+``python -m rmpcdmd_b200.validate [--quick | --bulk L INTERVALS | --paired L
+REPLICAS INTERVALS]`` prints one JSON object.
 """
 from __future__ import annotations
 
@@ -161,6 +161,12 @@ def paired_propulsion_check(L=16, replicas=8, n_intervals=40, skip=3, seed0=2000
             d.interval()
     disp64 = np.zeros((replicas, n_intervals))
     delta = np.zeros((replicas, n_intervals))
+    nb64 = np.zeros((replicas, n_intervals))   # change of the B count over the interval (FP64)
+    nb_delta = np.zeros((replicas, n_intervals))  # FP32 twin minus FP64
+
+    def n_b(x):
+        return int((x.solvent.download("species") == 2).sum())
+
     for t in range(n_intervals):
         for r in range(replicas):
             d, w = d64[r], tw[r]
@@ -169,12 +175,16 @@ def paired_propulsion_check(L=16, replicas=8, n_intervals=40, skip=3, seed0=2000
             u = x0[0] - x0[1]
             u = u / np.linalg.norm(u)
             c0 = (x0[0] + x0[1]) / 2
+            b0 = n_b(d)
             d.interval()
             w.interval()
             a = float(((_unwrapped(d)[0] + _unwrapped(d)[1]) / 2 - c0) @ u)
             b = float(((_unwrapped(w)[0] + _unwrapped(w)[1]) / 2 - c0) @ u)
             disp64[r, t] = a
             delta[r, t] = b - a
+            b64 = n_b(d)
+            nb64[r, t] = b64 - b0
+            nb_delta[r, t] = n_b(w) - b64
     n = delta.size
     bias = float(delta.mean())
     # replicas are independent; intervals of one replica are nearly so for
@@ -182,9 +192,15 @@ def paired_propulsion_check(L=16, replicas=8, n_intervals=40, skip=3, seed0=2000
     bias_err = float(delta.std(ddof=1) / np.sqrt(n))
     v = float(disp64.mean())
     v_err = float(disp64.mean(axis=1).std(ddof=1) / np.sqrt(replicas)) if replicas > 1 else float("nan")
+    # B species: the net change of the B count per interval (reactions A -> B
+    # at the catalytic bead less refuelling B -> A far away), FP64, and the
+    # paired FP32-minus-FP64 difference of the count after the interval
     return dict(L=L, replicas=replicas, intervals=n_intervals, skipped=skip, samples=n, bias=bias,
                 bias_err=bias_err, delta_std=float(delta.std(ddof=1)), delta_abs_max=float(np.abs(delta).max()),
-                v_prop_fp64=v, v_prop_fp64_err=v_err)
+                v_prop_fp64=v, v_prop_fp64_err=v_err,
+                b_change_fp64=float(nb64.mean()), b_change_fp64_err=float(nb64.std(ddof=1) / np.sqrt(n)),
+                b_bias=float(nb_delta.mean()), b_bias_err=float(nb_delta.std(ddof=1) / np.sqrt(n)),
+                b_delta_abs_max=float(np.abs(nb_delta).max()))
 
 
 def main(argv=None):
@@ -192,10 +208,15 @@ def main(argv=None):
     ap.add_argument("--quick", action="store_true", help="small sizes (a minute)")
     ap.add_argument("--bulk", type=int, nargs=2, metavar=("L", "INTERVALS"),
                     help="only the bulk check, on an L^3 box for INTERVALS intervals")
+    ap.add_argument("--paired", type=int, nargs=3, metavar=("L", "REPLICAS", "INTERVALS"),
+                    help="only the paired dimer check, on L^3 boxes")
     a = ap.parse_args(argv)
     t0 = time.perf_counter()
     if a.bulk:
         out = dict(bulk=bulk_check(L=a.bulk[0], n_intervals=a.bulk[1]))
+    elif a.paired:
+        out = dict(paired=paired_propulsion_check(L=a.paired[0], replicas=a.paired[1], n_intervals=a.paired[2],
+                                                  skip=2))
     elif a.quick:
         out = dict(bulk=bulk_check(L=24, n_intervals=20),
                    propulsion=propulsion_check(L=16, replicas=16, n_intervals=30, skip=5),
