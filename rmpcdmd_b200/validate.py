@@ -12,10 +12,12 @@ the same seeds:
 * single_dimer_pbc (programs/single_dimer_pbc.f90): the dimer's propulsion
   velocity, the centre-of-mass displacement per interval projected on the
   bond direction (catalytic minus noncatalytic bead), averaged over an
-  ensemble of replicas run by the batched engine, with its standard error.
+  ensemble of replicas run by the batched engine, with its standard error;
+* n_colloids_pbc: the colloids' mean-squared displacement per interval,
+  paired (an FP32 twin restarted from the FP64 state every interval).
 
 ``python -m rmpcdmd_b200.validate [--quick | --bulk L INTERVALS | --paired L
-REPLICAS INTERVALS]`` prints one JSON object.
+REPLICAS INTERVALS | --colloids L COLLOIDS INTERVALS]`` prints one JSON object.
 """
 from __future__ import annotations
 
@@ -28,7 +30,7 @@ import numpy as np
 
 from . import api as A
 from ._capi import call
-from .programs import DimerBatch, SingleDimerPBC
+from .programs import DimerBatch, NColloidsPBC, SingleDimerPBC
 
 KT = 1.0 / 3.0
 
@@ -203,6 +205,52 @@ def paired_propulsion_check(L=16, replicas=8, n_intervals=40, skip=3, seed0=2000
                 b_delta_abs_max=float(np.abs(nb_delta).max()))
 
 
+def _sync_nc_twin(twin: NColloidsPBC, d: NColloidsPBC) -> None:
+    """twin (FP32 solvent) <- the state of d (FP64) at an interval boundary,
+    where every solvent particle is caught up and sorted: the solvent arrays
+    rounded to single precision, the colloids as they are, the grid origin,
+    the random-number step and the loop counters; then the program's
+    catch-up and sort with nothing to catch up, which sorts the twin's
+    rounded positions and rebuilds its list and pos_old."""
+    for f in ("pos", "vel", "force", "force_old", "image", "id", "species", "flags"):
+        twin.solvent.upload(f, d.solvent.download(f))
+    for f in ("pos", "vel", "force", "force_old", "image", "species"):
+        twin.colloids.upload(f, d.colloids.download(f))
+    twin.cells.origin = d.cells.origin
+    twin.rng.step = d.rng.step
+    twin.t, twin.last_sort = d.t, d.last_sort
+    twin._catch_up_and_sort()
+
+
+def paired_colloids_check(L=128, n_colloids=200, n_intervals=20, skip=2, seed=3000):
+    """n_colloids_pbc: the FP32 form's bias on the colloids' mean-squared
+    displacement per interval, paired as in paired_propulsion_check: at every
+    interval boundary of a plain FP64 run an FP32 twin takes its state, both
+    run one production interval with the same random numbers, and the
+    difference of the colloids' mean |displacement|^2 over the interval is
+    recorded (programs/n_colloids_pbc.f90:304-324)."""
+    kw = dict(L=(L, L, L), rho=10, N_MD=100, N_colloids=n_colloids, seed=seed, volume_correction=False)
+    d = NColloidsPBC(precision=A.FP64, **kw)
+    tw = NColloidsPBC(precision=A.FP32, **kw)
+    d.thermalise(skip)
+    msd64 = np.zeros(n_intervals)
+    delta = np.zeros(n_intervals)
+    dmax = 0.0
+    for t in range(n_intervals):
+        _sync_nc_twin(tw, d)
+        x0 = _unwrapped(d)
+        d.run(1)
+        tw.run(1)
+        a, b = _unwrapped(d) - x0, _unwrapped(tw) - x0
+        msd64[t] = float((a * a).sum(axis=1).mean())
+        delta[t] = float((b * b).sum(axis=1).mean()) - msd64[t]
+        dmax = max(dmax, float(np.abs(b - a).max()))
+    return dict(L=L, colloids=n_colloids, intervals=n_intervals, msd_per_interval_fp64=float(msd64.mean()),
+                msd_per_interval_fp64_err=float(msd64.std(ddof=1) / np.sqrt(n_intervals)),
+                msd_bias=float(delta.mean()), msd_bias_err=float(delta.std(ddof=1) / np.sqrt(n_intervals)),
+                displacement_diff_abs_max=dmax)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--quick", action="store_true", help="small sizes (a minute)")
@@ -210,10 +258,15 @@ def main(argv=None):
                     help="only the bulk check, on an L^3 box for INTERVALS intervals")
     ap.add_argument("--paired", type=int, nargs=3, metavar=("L", "REPLICAS", "INTERVALS"),
                     help="only the paired dimer check, on L^3 boxes")
+    ap.add_argument("--colloids", type=int, nargs=3, metavar=("L", "COLLOIDS", "INTERVALS"),
+                    help="only the paired n_colloids_pbc check")
     a = ap.parse_args(argv)
     t0 = time.perf_counter()
     if a.bulk:
         out = dict(bulk=bulk_check(L=a.bulk[0], n_intervals=a.bulk[1]))
+    elif a.colloids:
+        out = dict(colloids=paired_colloids_check(L=a.colloids[0], n_colloids=a.colloids[1],
+                                                  n_intervals=a.colloids[2]))
     elif a.paired:
         out = dict(paired=paired_propulsion_check(L=a.paired[0], replicas=a.paired[1], n_intervals=a.paired[2],
                                                   skip=2))
