@@ -411,7 +411,8 @@ int rmpcd_bulk_autotune(const int L[3], int precision, double tau, int n_interva
  * of each interval's last MD step) is carried in *state.  The call keeps its
  * scratch (about 4 B per slot and 4 B per solvent particle) and its captured
  * MD-step graphs for the next call, and reuses them while the handles, their
- * device arrays, the box, the LJ tables and tau, N_MD and skin are the same;
+ * device arrays, the box, the LJ tables and tau, N_MD, skin and mass are the
+ * same;
  * other arguments make it rebuild them.  A call made while another thread is
  * inside this function works with scratch of its own.  No module counterpart
  * in the reference. */

@@ -13,17 +13,15 @@
 //     over all N for the first two MD steps after a sort and over the MD
 //     cells after that;
 //   * the re-sort test of an MD step (its two displacement maxima against
-//     the skin) runs on the device in the host's double arithmetic, and the
-//     host reads its decision with one synchronisation; there is no per-call
-//     host overhead;
-//   * an MD step without energies is two replayed CUDA graphs: the part up
-//     to the re-sort test, and the part after the re-sort decision (flag
-//     roll, forces), each captured once per set of buffers it touches (the
-//     sort and the force switch exchange buffers).  The second is queued
-//     behind an IF node on the device's decision before the host reads it,
-//     so the GPU evaluates the forces while the host waits; on a step that
-//     re-sorts the IF node skips them and the host issues the sort, then the
-//     forces.
+//     the skin) runs on the device in the host's double arithmetic and
+//     writes its decision to page-locked mapped host memory;
+//   * an MD step without energies is one replayed CUDA graph, captured once
+//     per set of buffers it touches (the sort and the force switch exchange
+//     buffers): the part up to the re-sort test, then the part after it
+//     (flag roll, forces) with every kernel gated by the device's decision.
+//     The host reads the decision as soon as the kernel writes it, while the
+//     forces run; on a step that re-sorts the gated kernels return at once
+//     and the host issues the sort, then the forces.
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -262,8 +260,9 @@ __device__ inline void zero_colloid_force(const Vec3<double> &cf, int nc)
 // same flags and forces as rolling all N.
 template <typename R>
 __global__ void k_md_cells_roll_clear(const int *list, const int *n_list, const int *count, const int *start,
-                                      int *flags, Vec3<R> force, Vec3<double> cf, int nc)
+                                      int *flags, Vec3<R> force, Vec3<double> cf, int nc, const int *gate)
 {
+    if (gate && *gate) return;
     zero_colloid_force(cf, nc);
     const long long n = (long long)*n_list * kLanesPerCell;
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
@@ -284,8 +283,9 @@ __global__ void k_md_cells_roll_clear(const int *list, const int *n_list, const 
 // zero_force of the solvent fused with the PAST_MD/MD roll: only entries of
 // particles with MD or PAST_MD set can be non-zero
 template <typename R>
-__global__ void k_roll_clear(int *flags, Vec3<R> force, long long N, Vec3<double> cf, int nc)
+__global__ void k_roll_clear(int *flags, Vec3<R> force, long long N, Vec3<double> cf, int nc, const int *gate)
 {
+    if (gate && *gate) return;
     zero_colloid_force(cf, nc);
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
         const int f = flags[i];
@@ -300,7 +300,9 @@ __global__ void k_roll_clear(int *flags, Vec3<R> force, long long N, Vec3<double
 
 // The program's re-sort test (programs/n_colloids_pbc.f90:230-231) on the
 // device, in the host's double arithmetic: ctl[0] counts the MD steps since
-// the last sort (delta_t = dt * ctl[0]), ctl[1] receives the decision.  The
+// the last sort (delta_t = dt * ctl[0]), ctl[1] receives the decision and
+// ctl[2] counts the tests; the host's mapped copy gets the decision, then the
+// count (h_ctl[1], h_ctl[0]), so a host that sees the count sees the decision.  The
 // maxima are the squared displacements taken by the MD step's position pass
 // (solvent, floored at max_v * delta_t) and of the colloids.
 __device__ inline void nc_resort_test(unsigned long long *so_bits, double co_sq, int *ctl, int *h_ctl, double dt,
@@ -315,9 +317,11 @@ __device__ inline void nc_resort_test(unsigned long long *so_bits, double co_sq,
     const double co_max = sqrt(co_sq);
     const int resort = (co_max >= __dmul_rn(skin, 0.1)) || (so_max >= __dmul_rn(skin, 0.9)) ? 1 : 0;
     ctl[1] = resort;
-    // the host's copy (page-locked, mapped): read after an event or stream
-    // synchronisation past this kernel, which orders it for the host
+    const int seq = ctl[2] + 1;
+    ctl[2] = seq;
     ((volatile int *)h_ctl)[1] = resort;
+    __threadfence_system();
+    ((volatile int *)h_ctl)[0] = seq;
     *so_bits = 0;  // cleared for the next MD step's position pass
 }
 
@@ -332,14 +336,14 @@ constexpr int kNcColloidThreads = 256;
 
 template <bool kVel>
 __global__ void __launch_bounds__(kNcColloidThreads)
-    k_nc_colloid_begin(PView<double> c, Vec3<double> c_old, const double *mass, double dt,
+    k_nc_colloid_begin(PView<double> c, Vec3<double> c_old, double mass, double dt,
                        unsigned long long *so_bits, int *ctl, int *h_ctl, double max_v, double skin)
 {
     __shared__ double s_m[kNcColloidThreads / 32];
     double m = 0;
     for (int i = threadIdx.x; i < c.N; i += blockDim.x) {
-        if (kVel) colloid_vv_vel_one(c, i, mass[i], dt);
-        colloid_vv_pos_one(c, i, mass[i], dt);
+        if (kVel) colloid_vv_vel_one(c, i, mass, dt);
+        colloid_vv_pos_one(c, i, mass, dt);
         const double r = disp_sq_one(c.pos, c_old, c.species, i);
         m = m > r ? m : r;
     }
@@ -352,17 +356,11 @@ __global__ void __launch_bounds__(kNcColloidThreads)
     }
 }
 
-// the IF node of a speculatively queued force part runs its body only when
-// the MD step's re-sort test said no
-__global__ void k_nc_set_cond(const int *ctl, cudaGraphConditionalHandle cond)
-{
-    cudaGraphSetConditional(cond, ctl[1] ? 0u : 1u);
-}
-
 __global__ void k_nc_set_since(int *ctl, int since)
 {
     ctl[0] = since;
     ctl[1] = 0;
+    ctl[2] = 0;
 }
 
 struct NcLoop {
@@ -379,21 +377,21 @@ struct NcLoop {
     int *cellmap = nullptr;  // slot of every solvent particle (set by each sort)
     int *n_md = nullptr;     // their number (device)
     int *ctl = nullptr;      // device: MD steps since the last sort, re-sort decision
-    double *d_mass = nullptr;  // velocity-Verlet masses of the colloids (device)
     int *h_ctl = nullptr;    // page-locked, device-mapped copy of the decision (written by the kernel)
     int *h_ctl_dev = nullptr;  // its device address
-    cudaEvent_t ev_a = nullptr;  // end of the MD step's part up to the re-sort test
     // second stream of the force evaluation (colloid sums and colloid-colloid
     // forces beside the solvent force application)
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int full_rolls = 2;  // rolls over all N still due since the last sort
-    // replayed parts of an MD step, keyed by the buffers they use; part_bs is
-    // part_b behind an IF node on the step's re-sort decision
+    // replayed parts of an MD step, keyed by the buffers they use: part_a up
+    // to the re-sort test, part_b the forces, and step = part_a then part_b
+    // gated by the test's decision (the key's last entry: vel_due + 2 full)
     using Key = std::tuple<const void *, const void *, const void *, int>;
-    std::map<Key, cudaGraphExec_t> part_a, part_b, part_bs;
+    std::map<Key, cudaGraphExec_t> part_a, part_b, step;
     bool graphs = false;
-    bool speculate = true;  // queue part_bs before the host reads the decision
+    unsigned seq = 0;  // re-sort tests issued in this call
+    cudaEvent_t ev_step = nullptr;  // end of the last step graph
     // what the captured graphs depend on besides their keys (see nc_signature)
     std::vector<unsigned long long> sig;
 
@@ -401,14 +399,13 @@ struct NcLoop {
     {
         for (auto &kv : part_a) cudaGraphExecDestroy(kv.second);
         for (auto &kv : part_b) cudaGraphExecDestroy(kv.second);
-        for (auto &kv : part_bs) cudaGraphExecDestroy(kv.second);
+        for (auto &kv : step) cudaGraphExecDestroy(kv.second);
         cudaFree(md_list);
         cudaFree(n_md);
         cudaFree(cellmap);
         cudaFree(ctl);
-        cudaFree(d_mass);
         if (h_ctl) cudaFreeHost(h_ctl);
-        if (ev_a) cudaEventDestroy(ev_a);
+        if (ev_step) cudaEventDestroy(ev_step);
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
         if (side) cudaStreamDestroy(side);
@@ -418,7 +415,7 @@ struct NcLoop {
 // Everything a captured MD-step graph bakes in besides the buffers of its key:
 // the device, the handles and every device array of theirs that a graph can touch, the
 // sizes, the box, max_v, the LJ tables (passed by value to the kernels) and
-// the step parameters.  The loop's scratch and graphs are kept for the next
+// the step parameters (tau, N_MD, skin and the colloid mass).  The loop's scratch and graphs are kept for the next
 // call while this is unchanged.
 static std::vector<unsigned long long> nc_signature(const rmpcd_particles *s, const rmpcd_particles *c,
                                                      const rmpcd_cells *cells, const rmpcd_nlist *nl,
@@ -488,20 +485,20 @@ static std::vector<unsigned long long> nc_signature(const rmpcd_particles *s, co
     num(prm->tau);
     v.push_back((unsigned long long)prm->N_MD);
     num(prm->skin);
+    num(prm->mass);
     return v;
 }
 
 // scratch, events and the second stream of a loop
-static int nc_alloc(NcLoop &L, int S, int N, int C)
+static int nc_alloc(NcLoop &L, int S, int N)
 {
     if (cudaMalloc(&L.md_list, (size_t)(S > 0 ? S : 1) * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&L.n_md, sizeof(int)) != cudaSuccess ||
         cudaMalloc(&L.cellmap, (size_t)(N > 0 ? N : 1) * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&L.ctl, 2 * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&L.d_mass, (size_t)(C > 0 ? C : 1) * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&L.ctl, 3 * sizeof(int)) != cudaSuccess ||
         cudaHostAlloc(&L.h_ctl, 2 * sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
         cudaHostGetDevicePointer(&L.h_ctl_dev, L.h_ctl, 0) != cudaSuccess ||
-        cudaEventCreateWithFlags(&L.ev_a, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&L.ev_step, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&L.ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&L.ev_join, cudaEventDisableTiming) != cudaSuccess ||
         cudaStreamCreateWithFlags(&L.side, cudaStreamNonBlocking) != cudaSuccess) {
@@ -582,18 +579,19 @@ static int md_cells_vel_t(NcLoop &L)
 }
 
 template <typename R>
-static int roll_clear_t(NcLoop &L)
+static int roll_clear_t(NcLoop &L, const int *gate)
 {
     PView<R> v = cur<R>(L.s);
     const Vec3<double> cf = cur<double>(L.c).force;
     const int nc = L.c->N;
     if (L.full_rolls > 0) {
         const long long n = L.s->N > nc ? L.s->N : nc;
-        k_roll_clear<R><<<grid_for(n > 0 ? n : 1, 256), 256, 0, stream()>>>(v.flags, v.force, L.s->N, cf, nc);
+        k_roll_clear<R><<<grid_for(n > 0 ? n : 1, 256), 256, 0, stream()>>>(v.flags, v.force, L.s->N, cf, nc, gate);
         L.full_rolls--;
     } else {
         k_md_cells_roll_clear<R><<<md_cells_grid(), 256, 0, stream()>>>(L.md_list, L.n_md, L.cells->count,
-                                                                        L.cells->start, v.flags, v.force, cf, nc);
+                                                                        L.cells->start, v.flags, v.force, cf, nc,
+                                                                        gate);
     }
     RMPCD_CHECK_LAUNCH();
     L.c->force_zero = true;
@@ -638,28 +636,45 @@ static int colloid_begin(NcLoop &L, bool vel_due)
     const PView<double> c = cur<double>(L.c);
     const Vec3<double> c_old = alt<double>(L.c).pos;
     if (vel_due)
-        k_nc_colloid_begin<true><<<1, kNcColloidThreads, 0, st>>>(c, c_old, L.d_mass, L.dt, L.s->d_max, L.ctl,
+        k_nc_colloid_begin<true><<<1, kNcColloidThreads, 0, st>>>(c, c_old, L.prm->mass, L.dt, L.s->d_max, L.ctl,
                                                                   L.h_ctl_dev, L.cells->max_v, L.prm->skin);
     else
-        k_nc_colloid_begin<false><<<1, kNcColloidThreads, 0, st>>>(c, c_old, L.d_mass, L.dt, L.s->d_max, L.ctl,
+        k_nc_colloid_begin<false><<<1, kNcColloidThreads, 0, st>>>(c, c_old, L.prm->mass, L.dt, L.s->d_max, L.ctl,
                                                                    L.h_ctl_dev, L.cells->max_v, L.prm->skin);
     RMPCD_CHECK_LAUNCH();
     return RMPCD_OK;
 }
 
-// the re-sort decision of the MD step, once the stream has reached its copy
-// (after the whole stream when ev is null)
-static int read_resort(NcLoop &L, cudaEvent_t ev, bool *resort)
+// the re-sort decision of the MD step, after a synchronisation of the stream
+static int read_resort(NcLoop &L, bool *resort)
 {
-    if (ev) {
-        const cudaError_t e = cudaEventSynchronize(ev);
-        if (e != cudaSuccess) return fail(RMPCD_ERR_CUDA, "n_colloids step: %s", cudaGetErrorString(e));
-    } else {
-        const int rc = sync();
-        if (rc) return rc;
-    }
+    const int rc = sync();
+    if (rc) return rc;
     *resort = ((volatile int *)L.h_ctl)[1] != 0;
     return RMPCD_OK;
+}
+
+// the re-sort decision of test number seq, read from the mapped copy as soon
+// as the kernel has written it, while the rest of the step graph runs; the
+// step graph's end event bounds the wait (once it has completed, the decision
+// is there or the step failed)
+static int wait_resort(NcLoop &L, unsigned seq, bool *resort)
+{
+    volatile int *h = (volatile int *)L.h_ctl;
+    for (unsigned long it = 1;; it++) {
+        if ((unsigned)h[0] == seq) {
+            *resort = h[1] != 0;
+            return RMPCD_OK;
+        }
+        if ((it & 1023ul) == 0) {
+            const cudaError_t e = cudaEventQuery(L.ev_step);
+            if (e == cudaSuccess) {
+                if ((unsigned)h[0] == seq) continue;
+                return fail(RMPCD_ERR_CUDA, "n_colloids step: re-sort decision %u missing after its step", seq);
+            }
+            if (e != cudaErrorNotReady) return fail(RMPCD_ERR_CUDA, "n_colloids step: %s", cudaGetErrorString(e));
+        }
+    }
 }
 
 // stream the non-MD cells over the time since the last sort, wrap, sort,
@@ -697,73 +712,21 @@ static int issue_part_a(NcLoop &L, bool vel_due)
 // md_loop after the re-sort test (programs/n_colloids_pbc.f90:243-254) up to
 // the velocity halves, the force switch done; energies only when asked for
 // (they synchronise).  The velocity halves run with the next MD step's
-// position pass, or in vel_tail after the interval's last MD step.
-static int issue_part_b(NcLoop &L, double *e1, double *e2)
+// position pass, or in vel_tail after the interval's last MD step.  gate
+// (without energies): a device word that, when non-zero, makes every kernel
+// of the part return at once.
+static int issue_part_b(NcLoop &L, double *e1, double *e2, const int *gate = nullptr)
 {
-    int rc = NC_DISPATCH(L, roll_clear_t);  // zero_force of the colloids included
+    // zero_force of the colloids included in the roll
+    int rc = L.s->precision == RMPCD_FP32 ? roll_clear_t<float>(L, gate) : roll_clear_t<double>(L, gate);
     if (!e1 && !e2) {
-        const ForceN2Branch n2{L.lj_cc, L.side, L.ev_fork, L.ev_join};
+        const ForceN2Branch n2{L.lj_cc, L.side, L.ev_fork, L.ev_join, gate};
         if (!rc) rc = compute_force_impl(L.c, L.s, L.nl, L.cells->edges, L.lj_sc, nullptr, false, &n2);
         return rc;
     }
     if (!rc) rc = compute_force_impl(L.c, L.s, L.nl, L.cells->edges, L.lj_sc, e1, false);
     if (!rc) rc = rmpcd_compute_force_n2(L.c, L.cells->edges, L.lj_cc, e2);
     return rc;
-}
-
-// part_b behind an IF node that runs it only when the MD step's re-sort test
-// (already queued) said no: captured once per key into a graph made of
-// k_nc_set_cond and the IF node, whose body is captured from issue_part_b.
-// Returns RMPCD_ERR_CUDA, with the stream out of capture and no error message
-// recorded, when the graph cannot be built; the caller then issues the step
-// without speculation.
-static int replay_spec(NcLoop &L, const NcLoop::Key &key)
-{
-    cudaStream_t st = stream();
-    auto it = L.part_bs.find(key);
-    if (it == L.part_bs.end()) {
-        cudaGraph_t g = nullptr, out = nullptr;
-        cudaGraphConditionalHandle cond = 0;
-        cudaError_t e = cudaGraphCreate(&g, 0);
-        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault);
-        if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-        cudaGraph_t body = nullptr;
-        if (e == cudaSuccess) {
-            k_nc_set_cond<<<1, 1, 0, st>>>(L.ctl, cond);
-            e = cudaGetLastError();
-            cudaStreamCaptureStatus cs;
-            const cudaGraphNode_t *deps = nullptr;
-            size_t nd = 0;
-            if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &nd);
-            cudaGraphNodeParams cp{};
-            cp.type = cudaGraphNodeTypeConditional;
-            cp.conditional.handle = cond;
-            cp.conditional.type = cudaGraphCondTypeIf;
-            cp.conditional.size = 1;
-            cudaGraphNode_t node = nullptr;
-            if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, deps, nd, &cp);
-            if (e == cudaSuccess) body = cp.conditional.phGraph_out[0];
-            const cudaError_t ee = cudaStreamEndCapture(st, &out);
-            if (e == cudaSuccess) e = ee;
-        }
-        int rc = RMPCD_OK;
-        if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-        if (e == cudaSuccess) {
-            rc = issue_part_b(L, nullptr, nullptr);
-            const cudaError_t ee = cudaStreamEndCapture(st, &out);
-            if (e == cudaSuccess) e = ee;
-        }
-        cudaGraphExec_t x = nullptr;
-        if (e == cudaSuccess && !rc) e = cudaGraphInstantiate(&x, g, 0);
-        if (g) cudaGraphDestroy(g);
-        if (e != cudaSuccess || rc) {
-            cudaGetLastError();
-            return RMPCD_ERR_CUDA;
-        }
-        it = L.part_bs.emplace(key, x).first;
-    }
-    RMPCD_CUDA_TRY(cudaGraphLaunch(it->second, st));
-    return RMPCD_OK;
 }
 
 // the velocity halves of the interval's last MD step
@@ -808,7 +771,57 @@ static int md_step_forces(NcLoop &L, bool want_energy)
 static int md_step(NcLoop &L, bool want_energy, bool vel_due)
 {
     L.st->t += 1;
+    const unsigned seq = ++L.seq;
     int rc;
+    if (L.graphs && !want_energy) {
+        // the whole MD step as one graph: part_a, then part_b gated by the
+        // step's re-sort decision, which the host reads from mapped memory
+        // while the forces run; on a step that re-sorts the gated part does
+        // nothing and the host issues the sort, then the forces
+        const int before = L.full_rolls;
+        const bool fz[4] = {L.s->force_zero, L.s->force_old_zero, L.c->force_zero, L.c->force_old_zero};
+        const NcLoop::Key ks{L.s->pos[L.s->cur][0], L.s->force[L.s->cur][0], L.c->force[L.c->cur][0],
+                             (vel_due ? 1 : 0) + (before > 0 ? 2 : 0)};
+        bool captured = false;
+        rc = replay(L.step, ks, [&] {
+            captured = true;
+            int r = issue_part_a(L, vel_due);
+            if (!r) r = rmpcd_particles_switch_force(L.s);
+            if (!r) r = rmpcd_particles_switch_force(L.c);
+            if (!r) r = issue_part_b(L, nullptr, nullptr, L.ctl + 1);
+            return r;
+        });
+        if (rc) return rc;
+        // a replay does the capture's host-side force switch here
+        if (!captured) {
+            rc = rmpcd_particles_switch_force(L.s);
+            if (!rc) rc = rmpcd_particles_switch_force(L.c);
+            if (rc) return rc;
+        }
+        RMPCD_CUDA_TRY(cudaEventRecord(L.ev_step, stream()));
+        bool resort = false;
+        rc = wait_resort(L, seq, &resort);
+        if (rc) return rc;
+        if (!resort) {
+            L.full_rolls = before > 0 ? before - 1 : 0;
+            L.s->force_zero = false;
+            L.c->force_zero = false;
+            return RMPCD_OK;
+        }
+        // the gated part did nothing: back to the state before the force
+        // switch, then the sort and the forces
+        L.full_rolls = before;
+        L.s->force_zero = fz[0];
+        L.s->force_old_zero = fz[1];
+        L.c->force_zero = fz[2];
+        L.c->force_old_zero = fz[3];
+        rc = rmpcd_particles_switch_force(L.s);
+        if (!rc) rc = rmpcd_particles_switch_force(L.c);
+        if (!rc) rc = catch_up_and_sort(L, false);
+        if (rc) return rc;
+        L.st->n_extra_sorting += 1;
+        return md_step_forces(L, false);
+    }
     if (L.graphs) {
         const NcLoop::Key ka{L.s->pos[L.s->cur][0], L.s->force[L.s->cur][0], L.c->force[L.c->cur][0],
                              vel_due ? 1 : 0};
@@ -817,48 +830,8 @@ static int md_step(NcLoop &L, bool want_energy, bool vel_due)
         rc = issue_part_a(L, vel_due);
     }
     if (rc) return rc;
-    if (L.graphs && L.speculate && !want_energy) {
-        // queue the force part before reading the decision: while the host
-        // waits for it, the GPU has the forces to evaluate (or, on a step that
-        // re-sorts, an IF node that skips them)
-        RMPCD_CUDA_TRY(cudaEventRecord(L.ev_a, stream()));
-        rc = rmpcd_particles_switch_force(L.s);
-        if (!rc) rc = rmpcd_particles_switch_force(L.c);
-        if (rc) return rc;
-        const int before = L.full_rolls;
-        const bool fz[4] = {L.s->force_zero, L.s->force_old_zero, L.c->force_zero, L.c->force_old_zero};
-        const NcLoop::Key kb{L.s->pos[L.s->cur][0], L.s->force[L.s->cur][0], L.c->force[L.c->cur][0],
-                             before > 0 ? 1 : 0};
-        const int rs = replay_spec(L, kb);
-        bool resort = false;
-        rc = read_resort(L, L.ev_a, &resort);
-        if (rc) return rc;
-        if (!rs && !resort) {
-            L.full_rolls = before > 0 ? before - 1 : 0;
-            L.s->force_zero = false;
-            L.c->force_zero = false;
-            return RMPCD_OK;
-        }
-        // the queued part did nothing (or was not built): undo the host-side
-        // bookkeeping of its capture and the force switch, then go on as below
-        if (rs) L.speculate = false;
-        L.full_rolls = before;
-        L.s->force_zero = fz[0];
-        L.s->force_old_zero = fz[1];
-        L.c->force_zero = fz[2];
-        L.c->force_old_zero = fz[3];
-        rc = rmpcd_particles_switch_force(L.s);
-        if (!rc) rc = rmpcd_particles_switch_force(L.c);
-        if (rc) return rc;
-        if (resort) {
-            rc = catch_up_and_sort(L, false);
-            if (rc) return rc;
-            L.st->n_extra_sorting += 1;
-        }
-        return md_step_forces(L, want_energy);
-    }
     bool resort = false;
-    rc = read_resort(L, nullptr, &resort);
+    rc = read_resort(L, &resort);
     if (rc) return rc;
     if (resort) {
         rc = catch_up_and_sort(L, false);
@@ -931,7 +904,7 @@ extern "C" int rmpcd_ncolloids_run(rmpcd_particles *solvent, rmpcd_particles *co
     if (!Lp) {
         own.reset(new NcLoop);
         Lp = own.get();
-        const int rc = nc_alloc(*Lp, cells->S, solvent->N, colloids->N);
+        const int rc = nc_alloc(*Lp, cells->S, solvent->N);
         if (rc) return rc;
     }
     NcLoop &L = *Lp;
@@ -949,12 +922,11 @@ extern "C" int rmpcd_ncolloids_run(rmpcd_particles *solvent, rmpcd_particles *co
     L.full_rolls = 2;
     L.graphs = false;
     PhaseTimer timer("ncolloids_run");
-    if (colloids->N > 0)
-        RMPCD_CUDA_TRY(cudaMemcpyAsync(L.d_mass, L.vv_mass.data(), (size_t)colloids->N * sizeof(double),
-                                       cudaMemcpyHostToDevice, stream()));
     // the solvent is sorted on entry: its slots from the cell ranges
     k_fill_cellmap<<<grid_full((long long)cells->S * kLanesPerCell, 256), 256, 0, stream()>>>(
         cells->count, cells->start, cells->S, L.cellmap);
+    L.seq = 0;
+    ((volatile int *)L.h_ctl)[0] = 0;
     k_nc_set_since<<<1, 1, 0, stream()>>>(L.ctl, state->t - state->last_sort);
     RMPCD_CUDA_TRY(cudaMemsetAsync(solvent->d_max, 0, 8, stream()));
     int rc0 = list_md_cells(L);

@@ -65,8 +65,9 @@ __global__ void k_pair_forces(const double *cx, const double *cy, const double *
                               const R *sx, const R *sy, const R *sz, const int *sspec, int *sflags,
                               const int *list, const int *n, int Nmax, double L0, double L1, double L2,
                               LJDev lj, double *pf, double *pe, unsigned char *contrib, int *ncontrib,
-                              int *max_contrib)
+                              int *max_contrib, const int *gate)
 {
+    if (gate && *gate) return;
     const int i = blockIdx.y;
     const int ni = n[i];
     const double x[3] = {cx[i], cy[i], cz[i]};
@@ -81,8 +82,9 @@ __global__ void k_pair_forces(const double *cx, const double *cy, const double *
 template <typename R>
 __global__ void k_apply_single(const int *list, const int *n, int Nmax, const unsigned char *contrib,
                                const double *pf, const int *ncontrib, R *fx, R *fy, R *fz,
-                               unsigned long long *mkeys, int *m_count)
+                               unsigned long long *mkeys, int *m_count, const int *gate)
 {
+    if (gate && *gate) return;
     const int i = blockIdx.y;
     const int ni = n[i];
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ni; e += gridDim.x * blockDim.x)
@@ -92,8 +94,10 @@ __global__ void k_apply_single(const int *list, const int *n, int Nmax, const un
 template <typename R>
 __global__ void k_apply_multi(const int *list, const int *n, int C, int Nmax, const unsigned char *contrib,
                               const double *pf, const int *ncontrib, int *max_contrib, int serial,
-                              R *fx, R *fy, R *fz, const unsigned long long *mkeys, int *m_count)
+                              R *fx, R *fy, R *fz, const unsigned long long *mkeys, int *m_count,
+                              const int *gate)
 {
+    if (gate && *gate) return;
     // the largest contribution count, read by every thread before thread 0
     // clears it for the next evaluation
     const int mc = *max_contrib;
@@ -111,16 +115,18 @@ __global__ void k_apply_multi(const int *list, const int *n, int C, int Nmax, co
 // (kSum = false: only the contributing entries compacted into clist / cn)
 template <bool kSum>
 __global__ void k_colloid_sum(const int *n, int Nmax, const unsigned char *contrib, const double *pf,
-                              double *cfx, double *cfy, double *cfz, int *clist, int *cn)
+                              double *cfx, double *cfy, double *cfz, int *clist, int *cn, const int *gate)
 {
+    if (gate && *gate) return;
     colloid_sum_block<kSum>(blockIdx.x, n, Nmax, contrib, pf, cfx, cfy, cfz, clist, cn);
 }
 
 // the FP32 form: f1 by the fixed tree of colloid_tree_block
 __global__ void __launch_bounds__(kNlBlockThreads) k_colloid_tree(const int *n, int Nmax, const unsigned char *contrib,
                                                                   const double *pf, double *cfx, double *cfy,
-                                                                  double *cfz)
+                                                                  double *cfz, const int *gate)
 {
+    if (gate && *gate) return;
     colloid_tree_block(blockIdx.x, n, Nmax, contrib, pf, cfx, cfy, cfz);
 }
 
@@ -212,8 +218,9 @@ __global__ void __launch_bounds__(1024) k_energy(const int *cn, const int *clist
 }
 
 __global__ void k_reset_contrib(const int *list, const int *n, int Nmax, const unsigned char *contrib,
-                                int *ncontrib)
+                                int *ncontrib, const int *gate)
 {
+    if (gate && *gate) return;
     const int i = blockIdx.y;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n[i]; e += gridDim.x * blockDim.x) {
         size_t q = (size_t)i * Nmax + e;
@@ -224,16 +231,19 @@ __global__ void k_reset_contrib(const int *list, const int *n, int Nmax, const u
 // compute_force_n2, src/neighbor_list.f90:227-264: a thread per colloid for
 // a few colloids, a block per colloid for many
 __global__ void k_force_n2(const double *px, const double *py, const double *pz, const int *sp, int C,
-                           double L0, double L1, double L2, LJDev lj, double *fx, double *fy, double *fz)
+                           double L0, double L1, double L2, LJDev lj, double *fx, double *fy, double *fz,
+                           const int *gate)
 {
+    if (gate && *gate) return;
     for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < C; m += gridDim.x * blockDim.x)
         force_n2_one(m, px, py, pz, sp, C, L0, L1, L2, lj, fx, fy, fz);
 }
 
 __global__ void __launch_bounds__(kNlBlockThreads)
     k_force_n2_blocks(const double *px, const double *py, const double *pz, const int *sp, int C, double L0,
-                      double L1, double L2, LJDev lj, double *fx, double *fy, double *fz)
+                      double L1, double L2, LJDev lj, double *fx, double *fy, double *fz, const int *gate)
 {
+    if (gate && *gate) return;
     force_n2_block(blockIdx.x, px, py, pz, sp, C, L0, L1, L2, lj, fx, fy, fz);
 }
 
@@ -464,17 +474,18 @@ int rmpcd_compute_force(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist 
 namespace rmpcd {
 
 // the force kernels of compute_force_n2 (src/neighbor_list.f90:227-264) on st
-static void launch_force_n2(rmpcd_particles *ps, const double L[3], const rmpcd_lj *lj, cudaStream_t st)
+static void launch_force_n2(rmpcd_particles *ps, const double L[3], const rmpcd_lj *lj, cudaStream_t st,
+                            const int *gate = nullptr)
 {
     const int C = ps->N;
     PView<double> v = cur<double>(ps);
     LJDev ld = lj_dev(lj);
     if (C <= 32)
         k_force_n2<<<1, 32, 0, st>>>(v.pos.x, v.pos.y, v.pos.z, v.species, C, L[0], L[1], L[2], ld, v.force.x,
-                                     v.force.y, v.force.z);
+                                     v.force.y, v.force.z, gate);
     else
         k_force_n2_blocks<<<C, kNlBlockThreads, 0, st>>>(v.pos.x, v.pos.y, v.pos.z, v.species, C, L[0], L[1], L[2],
-                                                         ld, v.force.x, v.force.y, v.force.z);
+                                                         ld, v.force.x, v.force.y, v.force.z, gate);
 }
 
 int compute_force_impl(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist *nl, const double L[3],
@@ -488,6 +499,7 @@ int compute_force_impl(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist *
     PhaseTimer tm("neigh list force");
     cudaStream_t s = stream();
     int C = ps1->N;
+    const int *gate = n2 ? n2->gate : nullptr;
     if (roll_flags && ps2->N > 0) k_flag_roll<<<grid_for(ps2->N, 256), 256, 0, s>>>(ps2->flags[ps2->cur], ps2->N);
     int *max_contrib = nl->d_status;
     int *m_count = nl->d_status + 1;  // multi-contribution keys collected (reset by k_apply_multi)
@@ -514,13 +526,13 @@ int compute_force_impl(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist *
             k_pair_forces<float><<<grid, 256, 0, s>>>(cv.pos.x, cv.pos.y, cv.pos.z, cv.species, v.pos.x, v.pos.y,
                                                       v.pos.z, v.species, v.flags, nl->list, nl->n, nl->Nmax, L[0],
                                                       L[1], L[2], ld, nl->pair_f, nl->pair_e, nl->contrib,
-                                                      nl->ncontrib, max_contrib);
+                                                      nl->ncontrib, max_contrib, gate);
         } else {
             PView<double> v = cur<double>(ps2);
             k_pair_forces<double><<<grid, 256, 0, s>>>(cv.pos.x, cv.pos.y, cv.pos.z, cv.species, v.pos.x, v.pos.y,
                                                        v.pos.z, v.species, v.flags, nl->list, nl->n, nl->Nmax, L[0],
                                                        L[1], L[2], ld, nl->pair_f, nl->pair_e, nl->contrib,
-                                                       nl->ncontrib, max_contrib);
+                                                       nl->ncontrib, max_contrib, gate);
         }
         // the colloid sums (and with n2 the colloid-colloid forces after them)
         // only read the pair terms and write the colloid forces: with n2 they
@@ -536,34 +548,36 @@ int compute_force_impl(rmpcd_particles *ps1, rmpcd_particles *ps2, rmpcd_nlist *
         // FP32 form (whose energy still needs the compacted entries)
         if (ps2->precision == RMPCD_FP32) {
             k_colloid_tree<<<C, kNlBlockThreads, 0, sc>>>(nl->n, nl->Nmax, nl->contrib, nl->pair_f, cv.force.x,
-                                                          cv.force.y, cv.force.z);
+                                                          cv.force.y, cv.force.z, gate);
             if (energy)
                 k_colloid_sum<false><<<C, kNlThreads, 0, sc>>>(nl->n, nl->Nmax, nl->contrib, nl->pair_f, cv.force.x,
-                                                               cv.force.y, cv.force.z, clist, cn);
+                                                               cv.force.y, cv.force.z, clist, cn, gate);
         } else {
             k_colloid_sum<true><<<C, kNlThreads, 0, sc>>>(nl->n, nl->Nmax, nl->contrib, nl->pair_f, cv.force.x,
-                                                          cv.force.y, cv.force.z, clist, cn);
+                                                          cv.force.y, cv.force.z, clist, cn, gate);
         }
         if (fork) {
-            launch_force_n2(ps1, L, n2->lj_cc, sc);
+            launch_force_n2(ps1, L, n2->lj_cc, sc, gate);
             RMPCD_CUDA_TRY(cudaEventRecord(n2->ev_join, sc));
         }
         if (ps2->precision == RMPCD_FP32) {
             PView<float> v = cur<float>(ps2);
             k_apply_single<float><<<grid, 256, 0, s>>>(nl->list, nl->n, nl->Nmax, nl->contrib, nl->pair_f,
-                                                       nl->ncontrib, v.force.x, v.force.y, v.force.z, nl->mkeys, m_count);
+                                                       nl->ncontrib, v.force.x, v.force.y, v.force.z, nl->mkeys, m_count,
+                                                       gate);
             k_apply_multi<float><<<1, 1024, 0, s>>>(nl->list, nl->n, C, nl->Nmax, nl->contrib, nl->pair_f,
                                                    nl->ncontrib, max_contrib, serial, v.force.x, v.force.y, v.force.z, nl->mkeys,
-                                                   m_count);
+                                                   m_count, gate);
         } else {
             PView<double> v = cur<double>(ps2);
             k_apply_single<double><<<grid, 256, 0, s>>>(nl->list, nl->n, nl->Nmax, nl->contrib, nl->pair_f,
-                                                        nl->ncontrib, v.force.x, v.force.y, v.force.z, nl->mkeys, m_count);
+                                                        nl->ncontrib, v.force.x, v.force.y, v.force.z, nl->mkeys, m_count,
+                                                       gate);
             k_apply_multi<double><<<1, 1024, 0, s>>>(nl->list, nl->n, C, nl->Nmax, nl->contrib, nl->pair_f,
                                                     nl->ncontrib, max_contrib, serial, v.force.x, v.force.y, v.force.z, nl->mkeys,
-                                                   m_count);
+                                                   m_count, gate);
         }
-        k_reset_contrib<<<grid, 256, 0, s>>>(nl->list, nl->n, nl->Nmax, nl->contrib, nl->ncontrib);
+        k_reset_contrib<<<grid, 256, 0, s>>>(nl->list, nl->n, nl->Nmax, nl->contrib, nl->ncontrib, gate);
         if (energy) k_energy<<<1, 1024, 0, s>>>(cn, clist, C, nl->Nmax, nl->pair_e, nl->e_pre, e_out);
         if (fork) RMPCD_CUDA_TRY(cudaStreamWaitEvent(s, n2->ev_join, 0));
         RMPCD_CHECK_LAUNCH();

@@ -57,6 +57,7 @@ struct ForceN2Branch {
     const rmpcd_lj *lj_cc;      // colloid-colloid parameters of compute_force_n2
     cudaStream_t side;
     cudaEvent_t ev_fork, ev_join;
+    const int *gate;            // device word; non-zero: every kernel of the evaluation returns at once (or null)
 };
 // compute_force (src/neighbor_list.f90:159-225); roll_flags = false leaves
 // the PAST_MD/MD roll to the caller (which must then have done it).  n2 (no
