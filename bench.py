@@ -354,10 +354,10 @@ def run_dimer(rm, peak, peak_kind, local, dist=None, rank=0, world=1):
                          volume_correction=False, precision=prec)
         g.thermalise(1)
         rm.synchronize()
-        # the loop synchronises with the host once per MD step, so its wall
-        # clock carries host noise: best of three 2-interval runs
+        # the host reads each MD step's re-sort decision, so the loop's wall
+        # clock carries host noise: best of five 2-interval runs
         sec = float("inf")
-        for _ in range(3):
+        for _ in range(5):
             barrier(dist)
             t0 = time.perf_counter()
             g.thermalise(2)
@@ -366,7 +366,7 @@ def run_dimer(rm, peak, peak_kind, local, dist=None, rank=0, world=1):
         out[f"n_colloids_128_fp{prec}"] = {
             "value": world * g.N * DIMER_N_MD / sec, "us_per_md_step": round(sec * 1e6 / DIMER_N_MD, 2), "N": g.N,
             "colloids": 200, "n_extra_sorting": g.n_extra_sorting,
-            "path": "rmpcd_ncolloids_run (the program's calls issued in C; wall clock, best of 3 runs of 2 "
+            "path": "rmpcd_ncolloids_run (the program's calls issued in C; wall clock, best of 5 runs of 2 "
                     "thermostatted intervals)"}
         if prec == 64:
             t0 = time.perf_counter()

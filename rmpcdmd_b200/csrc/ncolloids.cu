@@ -301,8 +301,8 @@ __global__ void k_roll_clear(int *flags, Vec3<R> force, long long N, Vec3<double
 // The program's re-sort test (programs/n_colloids_pbc.f90:230-231) on the
 // device, in the host's double arithmetic: ctl[0] counts the MD steps since
 // the last sort (delta_t = dt * ctl[0]), ctl[1] receives the decision and
-// ctl[2] counts the tests; the host's mapped copy gets the decision, then the
-// count (h_ctl[1], h_ctl[0]), so a host that sees the count sees the decision.  The
+// ctl[2] counts the tests; the host's mapped word h_ctl[0] gets count * 2 +
+// decision in one store, so the host that sees the count sees its decision.  The
 // maxima are the squared displacements taken by the MD step's position pass
 // (solvent, floored at max_v * delta_t) and of the colloids.
 __device__ inline void nc_resort_test(unsigned long long *so_bits, double co_sq, int *ctl, int *h_ctl, double dt,
@@ -319,9 +319,7 @@ __device__ inline void nc_resort_test(unsigned long long *so_bits, double co_sq,
     ctl[1] = resort;
     const int seq = ctl[2] + 1;
     ctl[2] = seq;
-    ((volatile int *)h_ctl)[1] = resort;
-    __threadfence_system();
-    ((volatile int *)h_ctl)[0] = seq;
+    ((volatile int *)h_ctl)[0] = seq * 2 + resort;
     *so_bits = 0;  // cleared for the next MD step's position pass
 }
 
@@ -377,7 +375,7 @@ struct NcLoop {
     int *cellmap = nullptr;  // slot of every solvent particle (set by each sort)
     int *n_md = nullptr;     // their number (device)
     int *ctl = nullptr;      // device: MD steps since the last sort, re-sort decision
-    int *h_ctl = nullptr;    // page-locked, device-mapped copy of the decision (written by the kernel)
+    int *h_ctl = nullptr;    // page-locked, device-mapped word: test count * 2 + decision (written by the kernel)
     int *h_ctl_dev = nullptr;  // its device address
     // second stream of the force evaluation (colloid sums and colloid-colloid
     // forces beside the solvent force application)
@@ -650,7 +648,7 @@ static int read_resort(NcLoop &L, bool *resort)
 {
     const int rc = sync();
     if (rc) return rc;
-    *resort = ((volatile int *)L.h_ctl)[1] != 0;
+    *resort = (((volatile int *)L.h_ctl)[0] & 1) != 0;
     return RMPCD_OK;
 }
 
@@ -662,14 +660,15 @@ static int wait_resort(NcLoop &L, unsigned seq, bool *resort)
 {
     volatile int *h = (volatile int *)L.h_ctl;
     for (unsigned long it = 1;; it++) {
-        if ((unsigned)h[0] == seq) {
-            *resort = h[1] != 0;
+        const unsigned w = (unsigned)h[0];
+        if ((w >> 1) == seq) {
+            *resort = (w & 1u) != 0;
             return RMPCD_OK;
         }
         if ((it & 1023ul) == 0) {
             const cudaError_t e = cudaEventQuery(L.ev_step);
             if (e == cudaSuccess) {
-                if ((unsigned)h[0] == seq) continue;
+                if (((unsigned)h[0] >> 1) == seq) continue;
                 return fail(RMPCD_ERR_CUDA, "n_colloids step: re-sort decision %u missing after its step", seq);
             }
             if (e != cudaErrorNotReady) return fail(RMPCD_ERR_CUDA, "n_colloids step: %s", cudaGetErrorString(e));
