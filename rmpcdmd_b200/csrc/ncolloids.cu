@@ -81,11 +81,17 @@ __device__ inline void moved_pos(const PView<R> &v, long long i, int f, R dt, R 
     z = v.pos.z[i] + dt * v.vel.z[i] + dt_sq * fz;
 }
 
-// md_vel of one particle (src/md.f90:219-237 form)
+// md_vel of one particle (src/md.f90:219-237 form).  The FP32 form skips the
+// update of a particle without forces: its velocity keeps its value (a -0
+// component stays -0 where the reference's update stores +0, as in the
+// replica engine's FP32 step), and its 12 bytes are not written again.
 template <typename R>
 __device__ inline void stream_vel_gated(const PView<R> &v, long long i, int f, R dt)
 {
     if (!((f >> WALL_BIT) & 1)) {
+        if constexpr (sizeof(R) == 4) {
+            if (!(f & kForceFlags)) return;
+        }
         R fx = 0, fy = 0, fz = 0, ox = 0, oy = 0, oz = 0;
         if (f & kForceFlags) {
             fx = v.force.x[i];
@@ -374,7 +380,7 @@ struct NcLoop {
     int *md_list = nullptr;  // is_md slots
     int *cellmap = nullptr;  // slot of every solvent particle (set by each sort)
     int *n_md = nullptr;     // their number (device)
-    int *ctl = nullptr;      // device: MD steps since the last sort, re-sort decision
+    int *ctl = nullptr;      // device: MD steps since the last sort, re-sort decision, test count
     int *h_ctl = nullptr;    // page-locked, device-mapped word: test count * 2 + decision (written by the kernel)
     int *h_ctl_dev = nullptr;  // its device address
     // second stream of the force evaluation (colloid sums and colloid-colloid

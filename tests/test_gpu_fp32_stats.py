@@ -1,7 +1,8 @@
 """The FP32-solvent form against the plain FP64 form on the quantities the
 physics fixes (rmpcdmd_b200.validate): momentum conservation per MPCD
 interval, temperature, the velocity autocorrelation, and the FP32 bias on
-the dimer's propulsion velocity (paired with FP64 runs)."""
+the dimer's propulsion velocity and on the colloids' mean-squared
+displacement (paired with FP64 runs)."""
 import numpy as np
 import pytest
 
@@ -42,3 +43,15 @@ def test_dimer_propulsion_fp32_bias_is_below_one_percent():
     assert r["samples"] == 40
     assert r["delta_std"] < 1e-5  # the pair shares its noise
     assert abs(r["bias"]) + 3 * r["bias_err"] < 0.01 * V_PROP_SCALE
+
+
+def test_n_colloids_fp32_msd_bias():
+    """n_colloids_pbc, paired: an FP32 twin restarted from the FP64 state at
+    every interval boundary moves the colloids as the FP64 run does, to
+    rounding; the mean-squared displacement per interval differs by far less
+    than its own size."""
+    from rmpcdmd_b200.validate import paired_colloids_check
+
+    r = paired_colloids_check(L=24, n_colloids=8, n_intervals=4, skip=1)
+    assert r["displacement_diff_abs_max"] < 1e-4
+    assert abs(r["msd_bias"]) < 1e-3 * r["msd_per_interval_fp64"]
