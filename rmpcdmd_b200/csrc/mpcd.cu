@@ -26,64 +26,70 @@ __global__ void k_simple_mpcd(const int *__restrict__ count, const int *__restri
 // particle i with species > 0, (R)(rng::normal(seed, step, i, k) * t_factor)
 // for k = 0, 1, 2 into n[k][i].  Each deviate is the first accepted of the
 // attempts t = 0, 1, ... of rng::normal, so the values are rng::normal's.  A
-// warp's 32 particles (96 deviates) share its lanes: every lane tries one
-// attempt per round, and a rejected attempt queues the deviate's next attempt
-// for a later round, so no lane waits while another repeats a rejection (a
-// deviate drawn by one thread costs its warp the slowest lane's attempts).
+// warp takes kAtChunks chunks of 32 particles at a time and deals the
+// attempts of their deviates to its lanes: first every lane's attempt 0 of
+// its particles' deviates, then the attempts that rejections queue in a ring
+// in shared memory, 32 at a time, so no lane waits while another repeats a
+// rejection (a deviate drawn by one thread costs its warp the slowest lane's
+// attempts) and the last few rejections of a pass leave few lanes idle.
 constexpr int kAtThreads = 256;
-constexpr int kAtJobs = 96;  // deviates of one warp: 32 particles x 3
+constexpr int kAtChunks = 8;    // 32-particle chunks per warp pass
+constexpr int kAtQueue = 1024;  // ring of queued attempts per warp: at least 96 * kAtChunks
 
-__device__ inline unsigned short at_job(int p, int k, int t) { return (unsigned short)(p | (k << 5) | (t << 7)); }
+__device__ inline unsigned at_job(int p, int k, int t) { return (unsigned)p | ((unsigned)k << 8) | ((unsigned)t << 10); }
 
 template <typename R>
 __global__ void __launch_bounds__(kAtThreads) k_at_normals(const int *__restrict__ species, long long N, SrdParams q,
                                                            R *nx, R *ny, R *nz)
 {
-    __shared__ unsigned short jobs[kAtThreads / 32][2][kAtJobs];
+    static_assert(kAtChunks * 32 <= 256 && 96 * kAtChunks <= kAtQueue && (kAtQueue & (kAtQueue - 1)) == 0,
+                  "job fields and ring size");
+    __shared__ unsigned ring[kAtThreads / 32][kAtQueue];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned below = lanemask_lt();
+    unsigned *qr = ring[w];
     R *out[3] = {nx, ny, nz};
     const long long warps = (long long)gridDim.x * (kAtThreads / 32);
-    for (long long base = ((long long)blockIdx.x * (kAtThreads / 32) + w) * 32; base < N; base += warps * 32) {
-        unsigned short *cur = jobs[w][0], *next = jobs[w][1];
-        // round 0: every lane the attempt 0 of its own particle's deviates
-        const long long i = base + lane;
-        const bool act = i < N && species[i] > 0;
-        int nq = 0;
-        for (int k = 0; k < 3; k++) {
-            double z = 0;
-            const bool ok = act && rng::normal_attempt(q.seed, q.step, (uint32_t)i, (uint32_t)k, 0u, &z);
-            if (ok) out[k][i] = (R)(z * q.t_factor);
-            const unsigned rej = __ballot_sync(0xffffffffu, act && !ok);
-            if (act && !ok) cur[nq + __popc(rej & below)] = at_job(lane, k, 1);
-            nq += __popc(rej);
+    const long long span = 32LL * kAtChunks;
+    for (long long base = ((long long)blockIdx.x * (kAtThreads / 32) + w) * span; base < N; base += warps * span) {
+        // round 0: every lane the attempt 0 of its own particles' deviates
+        int tail = 0;
+        for (int c = 0; c < kAtChunks; c++) {
+            const long long i = base + c * 32 + lane;
+            const bool act = i < N && species[i] > 0;
+            for (int k = 0; k < 3; k++) {
+                double z = 0;
+                const bool ok = act && rng::normal_attempt(q.seed, q.step, (uint32_t)i, (uint32_t)k, 0u, &z);
+                if (ok) out[k][i] = (R)(z * q.t_factor);
+                const unsigned rej = __ballot_sync(0xffffffffu, act && !ok);
+                if (act && !ok) qr[(tail + __popc(rej & below)) & (kAtQueue - 1)] = at_job(c * 32 + lane, k, 1);
+                tail += __popc(rej);
+            }
         }
         __syncwarp();
-        // later rounds: the queued attempts, 32 at a time
-        while (nq > 0) {
-            int nn = 0;
-            for (int j0 = 0; j0 < nq; j0 += 32) {
-                const bool have = j0 + lane < nq;
-                const unsigned jb = have ? cur[j0 + lane] : 0u;
-                const int p = jb & 31, k = (jb >> 5) & 3, t = (int)(jb >> 7);
-                const long long ii = base + p;
-                double z = 0;
-                bool ok = false;
-                if (have) {
-                    // rng::normal gives 0 once its attempts are spent
-                    ok = t >= (int)rng::kNormalAttempts ||
-                         rng::normal_attempt(q.seed, q.step, (uint32_t)ii, (uint32_t)k, (uint32_t)t, &z);
-                    if (ok) out[k][ii] = (R)(z * q.t_factor);
-                }
-                const unsigned rej = __ballot_sync(0xffffffffu, have && !ok);
-                if (have && !ok) next[nn + __popc(rej & below)] = at_job(p, k, t + 1);
-                nn += __popc(rej);
+        // then the queued attempts, 32 at a time; a rejected one queues the
+        // deviate's next attempt behind the others (at most 96 * kAtChunks
+        // are queued at once, so the ring never overwrites an unread one)
+        int head = 0;
+        while (head < tail) {
+            const int n = min(32, tail - head);
+            const bool have = lane < n;
+            const unsigned jb = have ? qr[(head + lane) & (kAtQueue - 1)] : 0u;
+            head += n;
+            const int p = jb & 255, k = (jb >> 8) & 3, t = (int)(jb >> 10);
+            const long long ii = base + p;
+            double z = 0;
+            bool ok = false;
+            if (have) {
+                // rng::normal gives 0 once its attempts are spent
+                ok = t >= (int)rng::kNormalAttempts ||
+                     rng::normal_attempt(q.seed, q.step, (uint32_t)ii, (uint32_t)k, (uint32_t)t, &z);
+                if (ok) out[k][ii] = (R)(z * q.t_factor);
             }
+            const unsigned rej = __ballot_sync(0xffffffffu, have && !ok);
+            if (have && !ok) qr[(tail + __popc(rej & below)) & (kAtQueue - 1)] = at_job(p, k, t + 1);
+            tail += __popc(rej);
             __syncwarp();
-            unsigned short *tmp = cur;
-            cur = next;
-            next = tmp;
-            nq = nn;
         }
     }
 }
@@ -580,7 +586,7 @@ int rmpcd_simple_mpcd_step(rmpcd_particles *p, rmpcd_cells *c, rmpcd_rng *r, int
     if (thermostat && !q.gauss && p->N > 0) {
         // the normals first, into the sort target's velocity arrays (free
         // between sorts), then the cells
-        const int gn = grid_full(((long long)p->N + 31) / 32 * 32, kAtThreads);
+        const int gn = grid_full(((long long)p->N + 32 * kAtChunks - 1) / (32 * kAtChunks) * 32, kAtThreads);
         DISPATCH_R(p,
                    ({ PView<float> v = cur<float>(p), t = alt<float>(p);
                       k_at_normals<float><<<gn, kAtThreads, 0, s>>>(v.species, p->N, q, t.vel.x, t.vel.y, t.vel.z);
